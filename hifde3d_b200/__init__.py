@@ -1,0 +1,338 @@
+"""B200 implementation of HIFDE3D's hierarchical interpolative factorization.
+
+Python mirror of the reference's C++ API (arbenson/HIFDE3D include/Factor.hpp,
+include/setup_stencil.hpp) over the C ABI of libhif_b200.so
+(include/hif_b200.h). Names, argument meaning and call order follow the
+reference::
+
+    f = HIFFactor(N, P, epsilon)                 # HIFFactor<double>(N, P, eps)
+    SetupStencil(f, N, 1.0 / (N + 1), A, V)      # include/setup_stencil.hpp:6
+    f.Initialize(); f.Factor()                   # src/Factor.cpp:6, 41
+    f.Apply(u, apply_inverse=True)               # src/Factor.cpp:992 (in place)
+
+Vectors are float64 numpy arrays of NC^3 entries (NC = N + 1) in DOF order
+i + NC*j + NC^2*k, or (NC^3, nrhs) column blocks. Errors raise HIFError with the
+C status code. There is no CPU fallback: without the compiled library or a CUDA
+device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libhif_b200.so")
+_lib = None
+
+HIF_OK, HIF_ERR_ARG, HIF_ERR_CUDA, HIF_ERR_NOMEM, HIF_ERR_SINGULAR = 0, 1, 2, 3, 4
+HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET = 5, 6, 7
+PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
+OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB = 1, 2, 3
+TOP, BOTTOM, RIGHT, LEFT, FRONT, BACK = range(6)
+
+
+class HIFError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"hif status {code}: {msg}")
+        self.code = code
+
+
+_i, _d, _ll, _p = ctypes.c_int, ctypes.c_double, ctypes.c_longlong, ctypes.c_void_p
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+_llp = ctypes.POINTER(ctypes.c_longlong)
+
+_SIGNATURES = {
+    "hif_create": [_i, _i, _d, _i, ctypes.POINTER(_p)],
+    "hif_destroy": [_p],
+    "hif_set_stream": [_p, _p],
+    "hif_setup_stencil": [_p, _i, _d, _dp, _dp],
+    "hif_setup_stencil_device": [_p, _i, _d, _p, _p],
+    "hif_setup_stencil_faces": [_p, _i, _d, _dp, _dp, _dp, _dp],
+    "hif_initialize": [_p],
+    "hif_factor": [_p],
+    "hif_apply": [_p, _dp, _i, _ll, _i],
+    "hif_apply_device": [_p, _p, _i, _ll, _i],
+    "hif_spmv": [_p, _dp, _dp, _i, _ll, _i],
+    "hif_spmv_device": [_p, _p, _p, _i, _ll, _i],
+    "hif_solve_pcg": [_p, _dp, _dp, _i, _ll, _d, _i, _ip, _dp],
+    "hif_solve_pcg_device": [_p, _p, _p, _i, _ll, _d, _i, _ip, _dp],
+    "hif_num_levels": [_p, _ip],
+    "hif_num_blocks": [_p, _i, _i, _ip],
+    "hif_block_info": [_p, _i, _i, _i, _ip, _ip, _ip, _ip],
+    "hif_block_indices": [_p, _i, _i, _i, _ip, _ip, _ip],
+    "hif_block_matrix": [_p, _i, _i, _i, _i, _dp],
+    "hif_block_pivots": [_p, _i, _i, _ip, _dp],
+    "hif_set_option": [_p, _i, _ll],
+    "hif_set_replay_pivots": [_p, _i, _i, _ip, _ip],
+    "hif_factor_stats": [_p, _dp, _dp, _dp, _dp, _dp, _llp],
+    "hif_partition_cell": [_i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
+                           _ip, _ip, _ip, _ip],
+    "hif_partition_face": [_i, _i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
+                           _ip, _ip],
+}
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def lib():
+    """Load libhif_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise HIFError(HIF_ERR_NODEVICE,
+                           f"{_LIB_PATH} missing: run python -m hifde3d_b200.build")
+        L = ctypes.CDLL(_LIB_PATH)
+        for name, args in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.hif_last_error.restype = ctypes.c_char_p
+        L.hif_last_error.argtypes = []
+        _lib = L
+    return _lib
+
+
+def _check(code: int):
+    if code != HIF_OK:
+        raise HIFError(code, lib().hif_last_error().decode())
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(_ip)
+
+
+class Index3(tuple):
+    """Vec3T<int> (include/vec3t.hpp:197)."""
+
+    def __new__(cls, i, j, k):
+        return super().__new__(cls, (int(i), int(j), int(k)))
+
+
+class HIFFactor:
+    """``HIFFactor<double>`` (include/Factor.hpp:8-203) on one B200."""
+
+    def __init__(self, N: int, P: int, epsilon: float, partition: int = PARTITION_REFERENCE):
+        self._N, self._P, self._eps = int(N), int(P), float(epsilon)
+        self._h = _p()
+        _check(lib().hif_create(self._N, self._P, self._eps, int(partition),
+                                ctypes.byref(self._h)))
+        self.NC = self._N + 1
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().hif_destroy(self._h)
+            self._h = _p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- accessors (include/Factor.hpp:41-48) ----
+    def N(self) -> int:
+        return self._N
+
+    def P(self) -> int:
+        return self._P
+
+    def epsilon(self) -> float:
+        return self._eps
+
+    # ---- index maps (src/Factor.cpp:65-89) ----
+    def Tensor2LinearInd(self, ind) -> int:
+        i, j, k = ind
+        return i + self.NC * j + self.NC * self.NC * k
+
+    def Linear2TensorInd(self, ind: int) -> Index3:
+        NC = self.NC
+        return Index3(ind % NC, (ind // NC) % NC, ind // (NC * NC))
+
+    # ---- factor (src/Factor.cpp:6-63) ----
+    def Initialize(self):
+        _check(lib().hif_initialize(self._h))
+
+    def Factor(self):
+        _check(lib().hif_factor(self._h))
+
+    def set_option(self, option: int, value: int):
+        _check(lib().hif_set_option(self._h, int(option), int(value)))
+
+    def set_replay_pivots(self, level: int, orders):
+        """Test hook: prescribe each face's ID column order at ``level``."""
+        if not orders:
+            _check(lib().hif_set_replay_pivots(self._h, level, 0, None, None))
+            return
+        off = np.zeros(len(orders) + 1, np.int32)
+        off[1:] = np.cumsum([len(o) for o in orders])
+        flat = np.ascontiguousarray(np.concatenate(orders).astype(np.int32))
+        _check(lib().hif_set_replay_pivots(self._h, level, len(orders), _iptr(off), _iptr(flat)))
+
+    # ---- apply (src/Factor.cpp:992-1081) ----
+    def Apply(self, u: np.ndarray, apply_inverse: bool = False) -> np.ndarray:
+        """In place on ``u`` (float64, C-contiguous or (n, nrhs) Fortran order)."""
+        n3 = self.NC ** 3
+        if u.dtype != np.float64:
+            raise HIFError(HIF_ERR_ARG, "u must be float64")
+        if u.ndim == 1:
+            if u.size != n3 or not u.flags.c_contiguous:
+                raise HIFError(HIF_ERR_ARG, "u must have NC^3 contiguous entries")
+            _check(lib().hif_apply(self._h, _dptr(u), 1, n3, int(bool(apply_inverse))))
+            return u
+        if u.shape[0] != n3 or not u.flags.f_contiguous:
+            raise HIFError(HIF_ERR_ARG, "multi-RHS u must be (NC^3, nrhs) Fortran-ordered")
+        _check(lib().hif_apply(self._h, _dptr(u), u.shape[1], n3, int(bool(apply_inverse))))
+        return u
+
+    def apply_device(self, ptr: int, nrhs: int, ldu: int, apply_inverse: bool):
+        _check(lib().hif_apply_device(self._h, _p(ptr), nrhs, ldu, int(bool(apply_inverse))))
+
+    def spmv(self, x: np.ndarray, transpose: bool = True) -> np.ndarray:
+        """y = A^T x (``SpMV``, the reference walks columns) or y = A x."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        _check(lib().hif_spmv(self._h, _dptr(x), _dptr(y), 1, x.size, int(bool(transpose))))
+        return y
+
+    def solve_pcg(self, b: np.ndarray, tol: float = 1e-10, maxit: int = 200):
+        """PCG on A x = b preconditioned by the inverse apply. Returns (x, iters, relres)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b)
+        it = np.zeros(1, np.int32)
+        rr = np.zeros(1)
+        _check(lib().hif_solve_pcg(self._h, _dptr(b), _dptr(x), 1, b.size, tol, maxit,
+                                   _iptr(it), _dptr(rr)))
+        return x, int(it[0]), float(rr[0])
+
+    def solve_pcg_device(self, db: int, dx: int, nrhs: int, ld: int, tol: float, maxit: int):
+        it = np.zeros(nrhs, np.int32)
+        rr = np.zeros(nrhs)
+        _check(lib().hif_solve_pcg_device(self._h, _p(db), _p(dx), nrhs, ld, tol, maxit,
+                                          _iptr(it), _dptr(rr)))
+        return it, rr
+
+    # ---- introspection (schur_level_data / skel_level_data) ----
+    def num_levels(self) -> int:
+        v = ctypes.c_int()
+        _check(lib().hif_num_levels(self._h, ctypes.byref(v)))
+        return v.value
+
+    def num_blocks(self, level: int, kind: int) -> int:
+        v = ctypes.c_int()
+        _check(lib().hif_num_blocks(self._h, level, kind, ctypes.byref(v)))
+        return v.value
+
+    def block(self, level: int, kind: int, b: int, matrices: bool = False):
+        ng, nr, ns, face = (ctypes.c_int() for _ in range(4))
+        _check(lib().hif_block_info(self._h, level, kind, b, ctypes.byref(ng), ctypes.byref(nr),
+                                    ctypes.byref(ns), ctypes.byref(face)))
+        g = np.zeros(max(ng.value, 1), np.int32)
+        r = np.zeros(max(nr.value, 1), np.int32)
+        s = np.zeros(max(ns.value, 1), np.int32)
+        _check(lib().hif_block_indices(self._h, level, kind, b, _iptr(g), _iptr(r), _iptr(s)))
+        out = {"face": face.value, "global": g[:ng.value].astype(np.int64),
+               "red": r[:nr.value].astype(np.int64), "skel": s[:ns.value].astype(np.int64)}
+        if matrices:
+            R, K = nr.value, ns.value
+            shapes = {"A22": (R, R), "A22inv": (R, R), "X": (R, K)}
+            if kind == 1:
+                shapes["W"] = (K, R)
+            for which, name in enumerate(["A22", "A22inv", "X", "W"]):
+                if name not in shapes:
+                    continue
+                h, w = shapes[name]
+                buf = np.zeros(max(h * w, 1))
+                _check(lib().hif_block_matrix(self._h, level, kind, b, which, _dptr(buf)))
+                out[name] = buf[:h * w].reshape(w, h).T.copy()
+        return out
+
+    def schur_complement(self, level: int, kind: int, b: int) -> np.ndarray:
+        info = self.block(level, kind, b)
+        k = info["skel"].size
+        buf = np.zeros(max(k * k, 1))
+        _check(lib().hif_block_matrix(self._h, level, kind, b, 4, _dptr(buf)))
+        return buf[:k * k].reshape(k, k).T.copy()
+
+    def pivots(self, level: int, b: int):
+        info = self.block(level, 1, b)
+        n = info["global"].size
+        jp = np.zeros(max(n, 1), np.int32)
+        rd = np.zeros(max(n, 1))
+        _check(lib().hif_block_pivots(self._h, level, b, _iptr(jp), _dptr(rd)))
+        return jp[:n].astype(np.int64), rd[:n]
+
+    def factor_stats(self) -> dict:
+        vals = [ctypes.c_double() for _ in range(5)]
+        nb = ctypes.c_longlong()
+        _check(lib().hif_factor_stats(self._h, *[ctypes.byref(v) for v in vals], ctypes.byref(nb)))
+        keys = ["total_s", "gather_s", "elim_s", "id_s", "host_s"]
+        d = {k: v.value for k, v in zip(keys, vals)}
+        d["device_bytes"] = nb.value
+        return d
+
+
+def SetupStencil(factor: HIFFactor, N: int, h: float, A: np.ndarray, V: np.ndarray) -> None:
+    """``SetupStencil`` (include/setup_stencil.hpp:6-76). A, V: (N+2)^3 arrays indexed
+    [i, j, k] (NumTns order i fastest is handled here)."""
+    NC = N + 1
+    if A.shape != (NC + 1,) * 3 or V.shape != (NC + 1,) * 3:
+        raise HIFError(HIF_ERR_ARG, "A and V must be (N+2)^3")
+    a = np.ascontiguousarray(A.astype(np.float64).ravel(order="F"))
+    v = np.ascontiguousarray(V.astype(np.float64).ravel(order="F"))
+    _check(lib().hif_setup_stencil(factor._h, N, h, _dptr(a), _dptr(v)))
+
+
+def SetupStencilFaces(factor: HIFFactor, N: int, h: float, ax, ay, az, V) -> None:
+    """Symmetric flux-form operator; face arrays (N+2)^3 indexed [i, j, k]."""
+    arrs = [np.ascontiguousarray(np.asarray(x, np.float64).ravel(order="F")) for x in (ax, ay, az, V)]
+    NC = N + 1
+    for x in arrs:
+        if x.size != (NC + 1) ** 3:
+            raise HIFError(HIF_ERR_ARG, "face arrays must be (N+2)^3")
+    _check(lib().hif_setup_stencil_faces(factor._h, N, h, *[_dptr(x) for x in arrs]))
+
+
+def SpMV(factor: HIFFactor, x: np.ndarray, y: np.ndarray) -> None:
+    """``SpMV(sp_matrix, x, y)`` (src/Factor.cpp:1099-1113): y = A^T x."""
+    y[...] = factor.spmv(x, transpose=True)
+
+
+def RelativeErrorNorm2(x: np.ndarray, y: np.ndarray) -> float:
+    """``RelativeErrorNorm2`` (src/Factor.cpp:1083-1097): ||x - y|| / ||x||."""
+    return float(np.sqrt(np.sum(np.abs(x - y) ** 2) / np.sum(np.abs(x) ** 2)))
+
+
+def partition_cell(N: int, P: int, level: int, cell, mask: np.ndarray):
+    """Host partitioner (test hook): InteriorCellIndexData of one cell over a mask
+    (uint8, NC^3, DOF order). Returns (global, red, skel)."""
+    n3 = (N + 1) ** 3
+    m = np.ascontiguousarray(mask, np.uint8)
+    g = np.zeros(n3, np.int32)
+    r = np.zeros(n3, np.int32)
+    s = np.zeros(n3, np.int32)
+    cnt = np.zeros(3, np.int32)
+    _check(lib().hif_partition_cell(N, P, level, cell[0], cell[1], cell[2], 0,
+                                    m.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                    _iptr(g), _iptr(r), _iptr(s), _iptr(cnt)))
+    return g[:cnt[0]].astype(np.int64), r[:cnt[1]].astype(np.int64), s[:cnt[2]].astype(np.int64)
+
+
+def partition_face(N: int, P: int, level: int, cell, face: int, mask: np.ndarray):
+    """Host partitioner (test hook): SkelInteractionIndexData -> (rows, cols)."""
+    n3 = (N + 1) ** 3
+    m = np.ascontiguousarray(mask, np.uint8)
+    rows = np.zeros(n3 + 1, np.int32)
+    cols = np.zeros(n3 + 1, np.int32)
+    _check(lib().hif_partition_face(N, P, level, cell[0], cell[1], cell[2], face, 0,
+                                    m.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                    _iptr(rows), _iptr(cols)))
+    return rows[1:1 + rows[0]].astype(np.int64), cols[1:1 + cols[0]].astype(np.int64)

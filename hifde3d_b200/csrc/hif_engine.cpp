@@ -1,0 +1,1598 @@
+// Host engine of the B200 HIF factorization and the C ABI (include/hif_b200.h).
+//
+// Mirrors HIFFactor<double> of arbenson/HIFDE3D (include/Factor.hpp,
+// src/Factor.cpp). The reference keeps the remaining operator in one global
+// std::map sparse matrix, gathers every dense block from it and scatters every
+// Schur complement back (UpdateMatrixAndDOFs, src/Factor.cpp:262-311). Here the
+// remaining operator is never formed. It is the 7-point stencil (7 bands in
+// HBM) plus the live dense Schur-complement blocks ("sources") of the previous
+// phase; each phase assembles its dense blocks directly from those on the GPU:
+//
+//   after Schur(l):  operator = A0 + sum_c T_c, T_c on the face DOFs of cell c,
+//                    T_c = (sources inherited by c)(skel, skel) + S_c;
+//   skel(l):         face f between cells c (owner) and c': M and A_ff read
+//                    A0, T_c and T_c'; S_f becomes a source;
+//   Schur(l+1):      cell C reads A0 and the sources it owns (its 8 children's
+//                    T_c and the S_f of faces owned by its children); the
+//                    skeleton-skeleton part of what it read plus S_C is T_C.
+//
+// Every source is summed into exactly one later T, so the assembled blocks
+// equal the reference's DenseSubmatrix of its updated sparse matrix. Only the
+// partition and the small ID decisions cross PCIe; one host sync per phase.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hif_b200.h"
+#include "hif_kernels.cuh"
+#include "hif_partition.hpp"
+
+namespace hif {
+
+thread_local std::string g_last_error;
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+namespace {
+
+#define HIF_CK(call)                                                                      \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      throw ::hif::Error{e_ == cudaErrorMemoryAllocation ? HIF_ERR_NOMEM : HIF_ERR_CUDA,          \
+                  std::string(#call) + ": " + cudaGetErrorString(e_)};                    \
+    }                                                                                     \
+  } while (0)
+
+double wall() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+// Device allocation helpers on the engine stream (stream-ordered allocator).
+template <class T>
+T* dalloc(size_t count, cudaStream_t s) {
+  if (count == 0) count = 1;
+  void* p = nullptr;
+  HIF_CK(cudaMallocAsync(&p, count * sizeof(T), s));
+  return static_cast<T*>(p);
+}
+
+void dfree(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
+template <class T>
+T* upload(const std::vector<T>& v, cudaStream_t s) {
+  T* d = dalloc<T>(v.size(), s);
+  if (!v.empty()) HIF_CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+// Keeps device buffers of one phase alive until released together.
+struct BufList {
+  std::vector<void*> p;
+  template <class T>
+  T* add(T* x) {
+    p.push_back(x);
+    return x;
+  }
+  void release(cudaStream_t s) {
+    for (void* x : p) dfree(x, s);
+    p.clear();
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Factor data of one block (FactorData, include/data.hpp:84-110)
+// ---------------------------------------------------------------------------
+struct BlockInfo {
+  std::vector<int> global;    // global_inds (reference order)
+  std::vector<int> red_pos;   // redundant_inds
+  std::vector<int> skel_pos;  // skeleton_inds
+  int face = -1;
+  int cell = -1;  // cell index (ci * cpd + cj) * cpd + ck
+  int nbr = -1;   // skeletonization: neighbour cell index
+  int r() const { return (int)red_pos.size(); }
+  int s() const { return (int)skel_pos.size(); }
+  std::vector<int> jpvt;  // skeletonization: pivot order over global
+  std::vector<double> rdiag;
+  std::vector<double> S;  // kept Schur complement (option)
+};
+
+struct StepData {
+  int level = 0;
+  bool skel = false;
+  int cpd = 0;
+  std::vector<BlockInfo> blocks;
+  double* arena = nullptr;  // A22 | A22inv | X | W per block
+  std::vector<long long> o_a22, o_inv, o_x, o_w;
+  int* d_red = nullptr;
+  int* d_skel = nullptr;
+  std::vector<long long> o_red, o_skel;
+  long long n_red = 0, n_skel = 0;
+};
+
+// One launch of the apply sweep.
+struct ApplyLaunch {
+  int type = 0;  // 0 gemv, 1 reduce-scatter
+  GemvDesc* d_desc = nullptr;
+  int* d_toff = nullptr;
+  int nd = 0, tiles = 0;
+  int in_vec = 0, out_vec = 0;  // 0 = ua, 1 = ub
+  int* d_dof = nullptr;
+  int* d_off = nullptr;
+  int* d_slot = nullptr;
+  int ndof = 0;
+  double alpha = 0.0;
+};
+
+struct ApplyPlan {
+  std::vector<ApplyLaunch> launches;
+  BufList bufs;
+  long long contrib_slots = 0;
+};
+
+// Live Schur complement blocks feeding the next phase.
+struct Sources {
+  std::vector<SourceDesc> desc;
+  std::vector<int> owner;      // target cell (next Schur phase) that sums this source
+  std::vector<int> dof_src;    // 6 x NC^3 membership arrays (see GatherTarget)
+  std::vector<int> cell_src;   // cell index -> source id (T_c), -1 if none
+  BufList bufs;                // device memory holding the blocks
+};
+
+class Engine {
+ public:
+  int N, P, NC, partition;
+  double eps;
+  long long n3;
+  int L = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double* d_band = nullptr;
+  bool have_op = false, initialized = false, factored = false;
+  std::vector<uint8_t> rem;
+  std::vector<StepData> steps;
+  bool keep_schur = false, verbose = false;
+  long long budget_mb = 0;
+  std::map<int, std::vector<std::vector<int>>> replay;
+  double t_total = 0, t_gather = 0, t_elim = 0, t_id = 0, t_host = 0;
+  long long peak_bytes = 0, cur_bytes = 0;
+  int* d_status = nullptr;
+  // apply / solve workspace
+  double* d_ua = nullptr;
+  double* d_ub = nullptr;
+  double* d_contrib = nullptr;
+  int ws_nrhs = 0;
+  ApplyPlan plan_inv, plan_fwd;
+  bool plans_built = false;
+  // PCG workspace
+  double* d_pcg = nullptr;
+  int pcg_nrhs = 0;
+
+  Engine(int N_, int P_, double eps_, int part)
+      : N(N_), P(P_), NC(N_ + 1), partition(part), eps(eps_) {
+    n3 = (long long)NC * NC * NC;
+    HIF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own_stream = true;
+    d_status = dalloc<int>(4, stream);
+    HIF_CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), stream));
+    d_band = dalloc<double>(7 * n3, stream);
+    HIF_CK(cudaMemsetAsync(d_band, 0, 7 * n3 * sizeof(double), stream));
+  }
+
+  ~Engine() {
+    release_factor();
+    release_workspace();
+    dfree(d_band, stream);
+    dfree(d_status, stream);
+    cudaStreamSynchronize(stream);
+    if (own_stream) cudaStreamDestroy(stream);
+  }
+
+  void sync() { HIF_CK(cudaStreamSynchronize(stream)); }
+
+  void release_workspace() {
+    dfree(d_ua, stream);
+    dfree(d_ub, stream);
+    dfree(d_pcg, stream);
+    d_ua = d_ub = d_pcg = nullptr;
+    ws_nrhs = pcg_nrhs = 0;
+  }
+
+  void release_plans() {
+    plan_inv.bufs.release(stream);
+    plan_fwd.bufs.release(stream);
+    plan_inv.launches.clear();
+    plan_fwd.launches.clear();
+    plans_built = false;
+  }
+
+  void release_factor() {
+    release_plans();
+    dfree(d_contrib, stream);
+    d_contrib = nullptr;
+    contrib_cap = 0;
+    for (StepData& st : steps) {
+      dfree(st.arena, stream);
+      dfree(st.d_red, stream);
+      dfree(st.d_skel, stream);
+    }
+    steps.clear();
+    factored = false;
+  }
+
+  int levels_for() const {
+    if (partition == HIF_PARTITION_REFERENCE) {
+      // src/Factor.cpp:36: round(log2(NC / P)) + 1 with integer NC / P
+      return (int)std::lround(std::log2((double)(NC / P))) + 1;
+    }
+    int l = 0;
+    while ((long long)P << l < NC) ++l;
+    return l + 1;
+  }
+
+  int cells_per_dir(int level) const {
+    const int w = (1 << level) * P;
+    return partition == HIF_PARTITION_REFERENCE ? NC / w : (NC + w - 1) / w;
+  }
+
+  // ---- operator setup ----------------------------------------------------
+  void setup_node_device(const double* dA, const double* dV, double hstep) {
+    launch_setup_node(dA, dV, N, hstep, d_band, stream);
+    HIF_CK(cudaGetLastError());
+    have_op = true;
+  }
+
+  // ---- Initialize (src/Factor.cpp:6-39) -----------------------------------
+  void initialize() {
+    release_factor();
+    rem.assign(n3, 0);
+    for (int k = 1; k < NC; ++k)
+      for (int j = 1; j < NC; ++j)
+        for (int i = 1; i < NC; ++i) rem[i + (long long)NC * j + (long long)NC * NC * k] = 1;
+    L = levels_for();
+    initialized = true;
+  }
+
+  void track(long long bytes) {
+    cur_bytes += bytes;
+    peak_bytes = std::max(peak_bytes, cur_bytes);
+    if (budget_mb > 0 && cur_bytes > budget_mb * (1LL << 20))
+      throw Error{HIF_ERR_BUDGET, "device memory budget exceeded"};
+  }
+
+  // ---- dense elimination of a batch of blocks ---------------------------
+  // descs[b].B holds [A22 A21; A12 A11] (ld n); on return the compact
+  // A22^{-1}, X are written and B's trailing block holds A11 - A12 X.
+  void run_sweep(const std::vector<SweepDesc>& descs, BufList& tmp) {
+    std::vector<SweepDesc> small, large;
+    int max_small = 0;
+    for (const SweepDesc& d : descs) {
+      if (d.r <= 0) continue;
+      if (d.n <= kSmallSweepN) {
+        small.push_back(d);
+        max_small = std::max(max_small, d.n);
+      } else {
+        large.push_back(d);
+      }
+    }
+    if (!small.empty()) {
+      SweepDesc* dd = tmp.add(upload(small, stream));
+      launch_sweep_small(dd, (int)small.size(), max_small, d_status, stream);
+      HIF_CK(cudaGetLastError());
+    }
+    if (large.empty()) return;
+    const int nl = (int)large.size();
+    SweepDesc* dd = tmp.add(upload(large, stream));
+    double* dinv = tmp.add(dalloc<double>((size_t)nl * kSweepNB * kSweepNB, stream));
+    int maxr = 0;
+    for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
+    for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
+      std::vector<int> active;
+      std::vector<int> rowt, colt, toff(1, 0);
+      std::vector<GemmDesc> gd;
+      for (int b = 0; b < nl; ++b) {
+        const SweepDesc& d = large[b];
+        if (d.r <= k0) continue;
+        active.push_back(b);
+        const int k1 = std::min(d.r, k0 + kSweepNB);
+        auto tiles = [&](std::vector<int>& out, int lo, int hi) {
+          for (int x = lo; x < hi; x += kSweepNB) {
+            out.push_back(b);
+            out.push_back(x);
+            out.push_back(std::min(hi, x + kSweepNB));
+            out.push_back(0);
+          }
+        };
+        tiles(rowt, 0, k0);
+        tiles(rowt, k1, d.n);
+        tiles(colt, 0, k0);
+        tiles(colt, k1, d.r);
+        const int nbk = k1 - k0;
+        auto gemm = [&](int r0, int r1, int c0, int c1) {
+          if (r1 <= r0 || c1 <= c0) return;
+          GemmDesc g{};
+          g.C = d.B + r0 + (long long)c0 * d.n;
+          g.A = d.B + r0 + (long long)k0 * d.n;
+          g.B = d.B + k0 + (long long)c0 * d.n;
+          g.ldc = g.lda = g.ldb = d.n;
+          g.m = r1 - r0;
+          g.n = c1 - c0;
+          g.k = nbk;
+          g.alpha = -1.0;
+          g.beta = 1.0;
+          gd.push_back(g);
+          toff.push_back(toff.back() + dgemm_tiles(g.m, g.n));
+        };
+        gemm(0, k0, 0, k0);
+        gemm(0, k0, k1, d.n);
+        gemm(k1, d.r, 0, k0);
+        gemm(k1, d.r, k1, d.n);
+        gemm(d.r, d.n, k1, d.n);
+      }
+      BufList step;
+      int* dact = step.add(upload(active, stream));
+      int* drow = step.add(upload(rowt, stream));
+      int* dcol = step.add(upload(colt, stream));
+      GemmDesc* dg = step.add(upload(gd, stream));
+      int* dto = step.add(upload(toff, stream));
+      launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
+      launch_sweep_rowpanel(dd, drow, (int)rowt.size() / 4, k0, dinv, stream);
+      launch_dgemm(dg, dto, (int)gd.size(), toff.back(), stream);
+      launch_sweep_colpanel(dd, dcol, (int)colt.size() / 4, k0, dinv, stream);
+      launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
+      HIF_CK(cudaGetLastError());
+      step.release(stream);
+    }
+    // compact copies of A22^{-1} and X
+    std::vector<CopyDesc> cd;
+    std::vector<int> coff(1, 0);
+    for (const SweepDesc& d : large) {
+      CopyDesc a{d.B, d.a22inv, d.n, d.r, d.r, d.r};
+      cd.push_back(a);
+      coff.push_back(coff.back() + copy_tiles(d.r, d.r));
+      CopyDesc x{d.B + (long long)d.r * d.n, d.X, d.n, d.r, d.r, d.n - d.r};
+      cd.push_back(x);
+      coff.push_back(coff.back() + copy_tiles(d.r, d.n - d.r));
+    }
+    CopyDesc* dcd = tmp.add(upload(cd, stream));
+    int* dco = tmp.add(upload(coff, stream));
+    launch_copy(dcd, dco, (int)cd.size(), coff.back(), stream);
+    HIF_CK(cudaGetLastError());
+  }
+
+  void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
+              const SourceDesc* d_srcdesc, const int* d_dof_src, BufList& tmp) {
+    std::vector<int> toff(1, 0);
+    for (const GatherTarget& g : tg) toff.push_back(toff.back() + gather_tiles(g.m, g.n));
+    if (toff.back() == 0) return;
+    GatherTarget* dt = tmp.add(upload(tg, stream));
+    int* dto = tmp.add(upload(toff, stream));
+    launch_gather(dt, dto, (int)tg.size(), toff.back(), d_srcdesc, d_src_owner, d_dof_src,
+                  d_band, n3, NC, stream);
+    HIF_CK(cudaGetLastError());
+    (void)src;
+  }
+
+  // Upload the source tables of a phase; the membership arrays are shared by
+  // every gather of that phase.
+  void upload_sources(const Sources& s, BufList& tmp, SourceDesc** d_desc, int** d_owner,
+                      int** d_dof) {
+    *d_desc = tmp.add(upload(s.desc, stream));
+    *d_owner = tmp.add(upload(s.owner, stream));
+    *d_dof = tmp.add(upload(s.dof_src, stream));
+  }
+
+  void empty_sources(Sources& s, int ncells) {
+    s.desc.clear();
+    s.owner.clear();
+    s.dof_src.assign(6 * n3, -1);
+    s.cell_src.assign(ncells, -1);
+  }
+
+  // ---- Schur phase (LevelFactorSchur, src/Factor.cpp:184-213) ------------
+  void schur_phase(int level, Sources& in, Sources& out) {
+    double th = wall();
+    const int cpd = cells_per_dir(level);
+    const int w = (1 << level) * P;
+    StepData st;
+    st.level = level;
+    st.skel = false;
+    st.cpd = cpd;
+    Partitioner part{N, P, NC, rem.data()};
+    const int ncell = cpd * cpd * cpd;
+    st.blocks.resize(ncell);
+    for (int ci = 0; ci < cpd; ++ci)
+      for (int cj = 0; cj < cpd; ++cj)
+        for (int ck = 0; ck < cpd; ++ck) {
+          const int idx = (ci * cpd + cj) * cpd + ck;
+          const int c[3] = {ci, cj, ck};
+          BlockInfo& b = st.blocks[idx];
+          part.cell_index(level, c, b.global, b.red_pos, b.skel_pos);
+          b.cell = idx;
+        }
+    // sizes and device layout
+    std::vector<int> red_all, skel_all;
+    long long bsz = 0, asz = 0;
+    std::vector<long long> o_B(ncell);
+    st.o_a22.resize(ncell);
+    st.o_inv.resize(ncell);
+    st.o_x.resize(ncell);
+    st.o_w.assign(ncell, 0);
+    st.o_red.resize(ncell);
+    st.o_skel.resize(ncell);
+    std::vector<int> rows_all;
+    std::vector<long long> o_rows(ncell);
+    for (int b = 0; b < ncell; ++b) {
+      const BlockInfo& bi = st.blocks[b];
+      const long long n = bi.global.size(), r = bi.r(), s = bi.s();
+      o_B[b] = bsz;
+      bsz += n * n;
+      st.o_a22[b] = asz;
+      asz += r * r;
+      st.o_inv[b] = asz;
+      asz += r * r;
+      st.o_x[b] = asz;
+      asz += r * s;
+      st.o_red[b] = red_all.size();
+      st.o_skel[b] = skel_all.size();
+      o_rows[b] = rows_all.size();
+      for (int p : bi.red_pos) {
+        red_all.push_back(bi.global[p]);
+        rows_all.push_back(bi.global[p]);
+      }
+      for (int p : bi.skel_pos) {
+        skel_all.push_back(bi.global[p]);
+        rows_all.push_back(bi.global[p]);
+      }
+    }
+    st.n_red = red_all.size();
+    st.n_skel = skel_all.size();
+    t_host += wall() - th;
+
+    track((bsz + asz) * 8);
+    double* dB = dalloc<double>(bsz, stream);
+    st.arena = dalloc<double>(asz, stream);
+    st.d_red = upload(red_all, stream);
+    st.d_skel = upload(skel_all, stream);
+    BufList tmp;
+    int* drows = tmp.add(upload(rows_all, stream));
+
+    // gather every cell block
+    double tg0 = wall();
+    SourceDesc* d_sd;
+    int *d_own, *d_dof;
+    upload_sources(in, tmp, &d_sd, &d_own, &d_dof);
+    std::vector<GatherTarget> tg(ncell);
+    for (int b = 0; b < ncell; ++b) {
+      const BlockInfo& bi = st.blocks[b];
+      GatherTarget& g = tg[b];
+      g.out = dB + o_B[b];
+      g.ld = bi.global.size();
+      g.rows = g.cols = drows + o_rows[b];
+      g.a22_out = st.arena + st.o_a22[b];
+      g.m = g.n = (int)bi.global.size();
+      g.a0_skip = bi.r();  // the skeleton-skeleton stencil part stays in A0
+      g.r = bi.r();
+      g.mode = level == 0 ? 2 : 0;
+      g.owner = b;
+      g.allowA = g.allowB = -1;
+    }
+    gather(tg, in, d_own, d_sd, d_dof, tmp);
+    if (verbose) sync();
+    t_gather += wall() - tg0;
+
+    // sources consumed: free them once the gather has run (stream order)
+    in.bufs.release(stream);
+
+    // keep-Schur option: remember what was gathered on the skeleton block
+    std::vector<double> side_all;
+    if (keep_schur) {
+      sync();
+      for (int b = 0; b < ncell; ++b) {
+        BlockInfo& bi = st.blocks[b];
+        const int n = bi.global.size(), r = bi.r(), s = bi.s();
+        bi.S.assign((size_t)s * s, 0.0);
+        std::vector<double> full((size_t)n * n);
+        HIF_CK(cudaMemcpy(full.data(), dB + o_B[b], full.size() * 8, cudaMemcpyDeviceToHost));
+        for (int j = 0; j < s; ++j)
+          for (int i = 0; i < s; ++i) bi.S[i + (size_t)j * s] = -full[(r + i) + (size_t)(r + j) * n];
+      }
+    }
+
+    // eliminate
+    double te0 = wall();
+    std::vector<SweepDesc> sd;
+    for (int b = 0; b < ncell; ++b) {
+      const BlockInfo& bi = st.blocks[b];
+      SweepDesc d{};
+      d.B = dB + o_B[b];
+      d.a22inv = st.arena + st.o_inv[b];
+      d.X = st.arena + st.o_x[b];
+      d.n = bi.global.size();
+      d.r = bi.r();
+      sd.push_back(d);
+    }
+    run_sweep(sd, tmp);
+    if (verbose) sync();
+    t_elim += wall() - te0;
+
+    if (keep_schur) {
+      sync();
+      for (int b = 0; b < ncell; ++b) {
+        BlockInfo& bi = st.blocks[b];
+        const int n = bi.global.size(), r = bi.r(), s = bi.s();
+        std::vector<double> full((size_t)n * n);
+        HIF_CK(cudaMemcpy(full.data(), dB + o_B[b], full.size() * 8, cudaMemcpyDeviceToHost));
+        for (int j = 0; j < s; ++j)
+          for (int i = 0; i < s; ++i) bi.S[i + (size_t)j * s] += full[(r + i) + (size_t)(r + j) * n];
+      }
+    }
+
+    // new sources T_c = B(skel, skel); membership by low / high face of the cell
+    th = wall();
+    const int cpd_next = cells_per_dir(level + 1);
+    empty_sources(out, ncell);
+    for (int b = 0; b < ncell; ++b) {
+      const BlockInfo& bi = st.blocks[b];
+      const int s = bi.s(), r = bi.r(), n = bi.global.size();
+      if (s == 0) continue;
+      const int id = (int)out.desc.size();
+      out.desc.push_back(SourceDesc{dB + o_B[b] + r + (long long)r * n, (long long)n});
+      const int ci = b / (cpd * cpd), cj = (b / cpd) % cpd, ck = b % cpd;
+      const int parent = cpd_next > 0 ? ((ci / 2) * cpd_next + cj / 2) * cpd_next + ck / 2 : -1;
+      out.owner.push_back(parent);
+      out.cell_src[b] = id;
+      const int c[3] = {ci, cj, ck};
+      for (int t = 0; t < s; ++t) {
+        const int p = bi.global[bi.skel_pos[t]];
+        const int x[3] = {p % NC, (p / NC) % NC, p / (NC * NC)};
+        int slot = 1;  // high face
+        for (int a = 0; a < 3; ++a)
+          if (x[a] % w == 0 && x[a] == w * c[a]) slot = 0;  // low face
+        out.dof_src[(2 * slot) * n3 + p] = id;
+        out.dof_src[(2 * slot + 1) * n3 + p] = t;
+      }
+    }
+    out.bufs.add(dB);
+    // remove eliminated DOFs (UpdateRemainingDOFs, src/Factor.cpp:91-111)
+    for (int p : red_all) rem[p] = 0;
+    tmp.release(stream);
+    steps.push_back(std::move(st));
+    t_host += wall() - th;
+  }
+
+  // ---- skeletonization phase (LevelFactorSkel, src/Factor.cpp:232-260) -----
+  void skel_phase(int level, Sources& cells, Sources& out) {
+    double th = wall();
+    const int cpd = cells_per_dir(level);
+    StepData st;
+    st.level = level;
+    st.skel = true;
+    st.cpd = cpd;
+    Partitioner part{N, P, NC, rem.data()};
+    std::vector<std::vector<int>> rows_l;
+    std::vector<BlockInfo>& blocks = st.blocks;
+    std::vector<int> rws, cls;
+    for (int ci = 0; ci < cpd; ++ci)
+      for (int cj = 0; cj < cpd; ++cj)
+        for (int ck = 0; ck < cpd; ++ck) {
+          const int c[3] = {ci, cj, ck};
+          for (int face : {TOP, FRONT, LEFT}) {
+            int nb[3];
+            if (!part.skel_interaction(level, c, face, rws, cls, nb)) continue;
+            if (cls.empty()) continue;
+            BlockInfo b;
+            b.face = face;
+            b.global = cls;
+            b.cell = (ci * cpd + cj) * cpd + ck;
+            b.nbr = (nb[0] * cpd + nb[1]) * cpd + nb[2];
+            blocks.push_back(std::move(b));
+            rows_l.push_back(rws);
+          }
+        }
+    const int nf = (int)blocks.size();
+    // M blocks (rows x cols) and ID workspace
+    std::vector<int> idx_all;
+    std::vector<long long> o_rows(nf), o_cols(nf), o_M(nf), o_W(nf), o_i(nf);
+    long long msz = 0, wsz = 0, isz = 0;
+    int max_n = 0;
+    for (int f = 0; f < nf; ++f) {
+      const int m = rows_l[f].size(), n = blocks[f].global.size();
+      if (m < n) throw Error{HIF_ERR_STATE, "face with fewer interaction rows than columns"};
+      o_rows[f] = idx_all.size();
+      idx_all.insert(idx_all.end(), rows_l[f].begin(), rows_l[f].end());
+      o_cols[f] = idx_all.size();
+      idx_all.insert(idx_all.end(), blocks[f].global.begin(), blocks[f].global.end());
+      o_M[f] = msz;
+      msz += (long long)m * n;
+      o_W[f] = wsz;
+      wsz += (long long)n * n / 4 + n + 1;
+      o_i[f] = isz;
+      isz += n;
+      max_n = std::max(max_n, n);
+    }
+    t_host += wall() - th;
+
+    BufList tmp;
+    track((msz + wsz) * 8);
+    double* dM = tmp.add(dalloc<double>(msz, stream));
+    double* dWs = tmp.add(dalloc<double>(wsz, stream));
+    int* didx = tmp.add(upload(idx_all, stream));
+    int* d_jp = tmp.add(dalloc<int>(isz + 1, stream));
+    int* d_keep = tmp.add(dalloc<int>(isz + 1, stream));
+    int* d_rank = tmp.add(dalloc<int>(nf + 1, stream));
+    double* d_rd = tmp.add(dalloc<double>(isz + 1, stream));
+
+    double tg0 = wall();
+    SourceDesc* d_sd;
+    int *d_own, *d_dof;
+    upload_sources(cells, tmp, &d_sd, &d_own, &d_dof);
+    std::vector<GatherTarget> tg(nf);
+    for (int f = 0; f < nf; ++f) {
+      GatherTarget& g = tg[f];
+      g.out = dM + o_M[f];
+      g.m = rows_l[f].size();
+      g.n = blocks[f].global.size();
+      g.ld = g.m;
+      g.rows = didx + o_rows[f];
+      g.cols = didx + o_cols[f];
+      g.a22_out = nullptr;
+      g.a0_skip = INT_MAX;
+      g.r = 0;
+      g.mode = 1;
+      g.owner = -1;
+      g.allowA = cells.cell_src[blocks[f].cell];
+      g.allowB = cells.cell_src[blocks[f].nbr];
+    }
+    gather(tg, cells, d_own, d_sd, d_dof, tmp);
+    if (verbose) sync();
+    t_gather += wall() - tg0;
+
+    // interpolative decompositions
+    double ti0 = wall();
+    std::vector<int> orders;
+    std::vector<long long> o_ord(nf, -1);
+    auto rp = replay.find(level);
+    if (rp != replay.end()) {
+      if ((int)rp->second.size() != nf)
+        throw Error{HIF_ERR_ARG, "replay pivots: face count differs"};
+      for (int f = 0; f < nf; ++f) {
+        if ((int)rp->second[f].size() != (int)blocks[f].global.size())
+          throw Error{HIF_ERR_ARG, "replay pivots: face size differs"};
+        o_ord[f] = orders.size();
+        orders.insert(orders.end(), rp->second[f].begin(), rp->second[f].end());
+      }
+    }
+    int* d_ord = orders.empty() ? nullptr : tmp.add(upload(orders, stream));
+    std::vector<IdDesc> idd(nf);
+    for (int f = 0; f < nf; ++f) {
+      IdDesc& d = idd[f];
+      d.M = dM + o_M[f];
+      d.order = d_ord ? d_ord + o_ord[f] : nullptr;
+      d.jpvt = d_jp + o_i[f];
+      d.rdiag = d_rd + o_i[f];
+      d.keep = d_keep + o_i[f];
+      d.rank = d_rank + f;
+      d.W = dWs + o_W[f];
+      d.m = rows_l[f].size();
+      d.n = blocks[f].global.size();
+    }
+    IdDesc* d_idd = tmp.add(upload(idd, stream));
+    launch_id(d_idd, nf, max_n, eps, d_status, stream);
+    HIF_CK(cudaGetLastError());
+    std::vector<int> h_jp(isz + 1), h_keep(isz + 1);
+    std::vector<double> h_rd(isz + 1);
+    HIF_CK(cudaMemcpyAsync(h_jp.data(), d_jp, isz * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    HIF_CK(cudaMemcpyAsync(h_keep.data(), d_keep, isz * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    HIF_CK(cudaMemcpyAsync(h_rd.data(), d_rd, isz * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    sync();
+    t_id += wall() - ti0;
+
+    // skeleton / redundant sets (InterpDecomp.cpp:102-110), internal order
+    th = wall();
+    std::vector<int> red_all, skel_all, rows2;
+    std::vector<long long> o_B(nf), o_r2(nf);
+    long long bsz = 0, asz = 0;
+    st.o_a22.resize(nf);
+    st.o_inv.resize(nf);
+    st.o_x.resize(nf);
+    st.o_w.resize(nf);
+    st.o_red.resize(nf);
+    st.o_skel.resize(nf);
+    for (int f = 0; f < nf; ++f) {
+      BlockInfo& b = blocks[f];
+      const int n = b.global.size();
+      b.jpvt.assign(h_jp.begin() + o_i[f], h_jp.begin() + o_i[f] + n);
+      b.rdiag.assign(h_rd.begin() + o_i[f], h_rd.begin() + o_i[f] + n);
+      for (int i = 0; i < n; ++i) {
+        if (h_keep[o_i[f] + i]) b.skel_pos.push_back(b.jpvt[i]);
+        else b.red_pos.push_back(b.jpvt[i]);
+      }
+      const long long r = b.r(), k = b.s();
+      o_B[f] = bsz;
+      bsz += (long long)n * n;
+      st.o_a22[f] = asz;
+      asz += r * r;
+      st.o_inv[f] = asz;
+      asz += r * r;
+      st.o_x[f] = asz;
+      asz += r * k;
+      st.o_w[f] = asz;
+      asz += k * r;
+      st.o_red[f] = red_all.size();
+      st.o_skel[f] = skel_all.size();
+      o_r2[f] = rows2.size();
+      for (int p : b.red_pos) {
+        red_all.push_back(b.global[p]);
+        rows2.push_back(b.global[p]);
+      }
+      for (int p : b.skel_pos) {
+        skel_all.push_back(b.global[p]);
+        rows2.push_back(b.global[p]);
+      }
+    }
+    st.n_red = red_all.size();
+    st.n_skel = skel_all.size();
+    t_host += wall() - th;
+
+    track((bsz + asz) * 8);
+    double* dB = dalloc<double>(bsz, stream);
+    st.arena = dalloc<double>(asz, stream);
+    st.d_red = upload(red_all, stream);
+    st.d_skel = upload(skel_all, stream);
+    int* drows2 = tmp.add(upload(rows2, stream));
+
+    // A_ff in [red | skel] order (SchurAfterID, src/Factor.cpp:113-153)
+    tg0 = wall();
+    std::vector<GatherTarget> tg2;
+    std::vector<int> act;
+    for (int f = 0; f < nf; ++f) {
+      const BlockInfo& b = blocks[f];
+      if (b.r() == 0) continue;
+      act.push_back(f);
+      GatherTarget g{};
+      g.out = dB + o_B[f];
+      g.m = g.n = b.global.size();
+      g.ld = g.m;
+      g.rows = g.cols = drows2 + o_r2[f];
+      g.a22_out = nullptr;
+      g.a0_skip = INT_MAX;
+      g.r = 0;
+      g.mode = 1;
+      g.owner = -1;
+      g.allowA = cells.cell_src[b.cell];
+      g.allowB = cells.cell_src[b.nbr];
+      tg2.push_back(g);
+    }
+    gather(tg2, cells, d_own, d_sd, d_dof, tmp);
+    if (verbose) sync();
+    t_gather += wall() - tg0;
+
+    // rotation by the ID: B(red,:) -= W^T B(skel,:); B(:,red) -= B(:,skel) W; B(skel,skel) = 0
+    te_rot_and_sweep(st, act, dB, o_B, dWs, o_W, tmp);
+
+    // keep-Schur: S_f = B(skel, skel) after the sweep
+    if (keep_schur) {
+      sync();
+      for (int f : act) {
+        BlockInfo& b = blocks[f];
+        const int n = b.global.size(), r = b.r(), k = b.s();
+        std::vector<double> full((size_t)n * n);
+        HIF_CK(cudaMemcpy(full.data(), dB + o_B[f], full.size() * 8, cudaMemcpyDeviceToHost));
+        b.S.assign((size_t)k * k, 0.0);
+        for (int j = 0; j < k; ++j)
+          for (int i = 0; i < k; ++i) b.S[i + (size_t)j * k] = full[(r + i) + (size_t)(r + j) * n];
+      }
+    }
+
+    // new sources: S_f of faces that eliminated something
+    th = wall();
+    const int cpd_next = cells_per_dir(level + 1);
+    out.dof_src = std::move(cells.dof_src);  // cell memberships stay (T_c are still live)
+    out.desc = cells.desc;
+    out.owner = cells.owner;
+    out.cell_src = cells.cell_src;
+    for (int f : act) {
+      const BlockInfo& b = blocks[f];
+      const int r = b.r(), k = b.s(), n = b.global.size();
+      if (k == 0) continue;
+      const int id = (int)out.desc.size();
+      out.desc.push_back(SourceDesc{dB + o_B[f] + r + (long long)r * n, (long long)n});
+      const int ci = b.cell / (cpd * cpd), cj = (b.cell / cpd) % cpd, ck = b.cell % cpd;
+      out.owner.push_back(((ci / 2) * cpd_next + cj / 2) * cpd_next + ck / 2);
+      for (int t = 0; t < k; ++t) {
+        const int p = b.global[b.skel_pos[t]];
+        out.dof_src[4 * n3 + p] = id;
+        out.dof_src[5 * n3 + p] = t;
+      }
+    }
+    // T_c buffers move to the output set; add this phase's B
+    out.bufs.p = cells.bufs.p;
+    cells.bufs.p.clear();
+    out.bufs.add(dB);
+    for (int p : red_all) rem[p] = 0;
+    tmp.release(stream);
+    steps.push_back(std::move(st));
+    t_host += wall() - th;
+  }
+
+  void te_rot_and_sweep(StepData& st, const std::vector<int>& act, double* dB,
+                        const std::vector<long long>& o_B, double* dWs,
+                        const std::vector<long long>& o_W, BufList& tmp) {
+    double te0 = wall();
+    std::vector<GemmDesc> g1, g2, g3;
+    std::vector<int> t1(1, 0), t2(1, 0), t3(1, 0);
+    std::vector<CopyDesc> cw, ca;
+    std::vector<int> tw(1, 0), ta(1, 0);
+    for (int f : act) {
+      const BlockInfo& b = st.blocks[f];
+      const int n = b.global.size(), r = b.r(), k = b.s();
+      double* B = dB + o_B[f];
+      const double* W = dWs + o_W[f];
+      if (k > 0) {
+        GemmDesc a{};
+        a.C = B;
+        a.A = W;
+        a.B = B + r;
+        a.ldc = n;
+        a.lda = k;
+        a.ldb = n;
+        a.m = r;
+        a.n = n;
+        a.k = k;
+        a.transA = 1;
+        a.alpha = -1.0;
+        a.beta = 1.0;
+        g1.push_back(a);
+        t1.push_back(t1.back() + dgemm_tiles(a.m, a.n));
+        GemmDesc c{};
+        c.C = B;
+        c.A = B + (long long)r * n;
+        c.B = W;
+        c.ldc = n;
+        c.lda = n;
+        c.ldb = k;
+        c.m = n;
+        c.n = r;
+        c.k = k;
+        c.alpha = -1.0;
+        c.beta = 1.0;
+        g2.push_back(c);
+        t2.push_back(t2.back() + dgemm_tiles(c.m, c.n));
+        GemmDesc z{};
+        z.C = B + r + (long long)r * n;
+        z.A = z.B = B;
+        z.ldc = n;
+        z.lda = z.ldb = n;
+        z.m = k;
+        z.n = k;
+        z.k = 0;
+        z.alpha = 0.0;
+        z.beta = 0.0;
+        g3.push_back(z);
+        t3.push_back(t3.back() + dgemm_tiles(k, k));
+        cw.push_back(CopyDesc{W, st.arena + st.o_w[f], k, k, k, r});
+        tw.push_back(tw.back() + copy_tiles(k, r));
+      }
+      ca.push_back(CopyDesc{B, st.arena + st.o_a22[f], n, r, r, r});
+      ta.push_back(ta.back() + copy_tiles(r, r));
+    }
+    auto run_gemm = [&](std::vector<GemmDesc>& g, std::vector<int>& t) {
+      if (g.empty()) return;
+      GemmDesc* d = tmp.add(upload(g, stream));
+      int* to = tmp.add(upload(t, stream));
+      launch_dgemm(d, to, (int)g.size(), t.back(), stream);
+      HIF_CK(cudaGetLastError());
+    };
+    auto run_copy = [&](std::vector<CopyDesc>& c, std::vector<int>& t) {
+      if (c.empty()) return;
+      CopyDesc* d = tmp.add(upload(c, stream));
+      int* to = tmp.add(upload(t, stream));
+      launch_copy(d, to, (int)c.size(), t.back(), stream);
+      HIF_CK(cudaGetLastError());
+    };
+    run_gemm(g1, t1);
+    run_gemm(g2, t2);
+    run_gemm(g3, t3);
+    run_copy(cw, tw);
+    run_copy(ca, ta);
+    std::vector<SweepDesc> sd;
+    for (int f : act) {
+      const BlockInfo& b = st.blocks[f];
+      SweepDesc d{};
+      d.B = dB + o_B[f];
+      d.a22inv = st.arena + st.o_inv[f];
+      d.X = st.arena + st.o_x[f];
+      d.n = b.global.size();
+      d.r = b.r();
+      sd.push_back(d);
+    }
+    run_sweep(sd, tmp);
+    if (verbose) sync();
+    t_elim += wall() - te0;
+  }
+
+  // ---- Factor (src/Factor.cpp:41-63) --------------------------------------
+  void factor() {
+    if (!have_op) throw Error{HIF_ERR_STATE, "no operator: call hif_setup_stencil first"};
+    if (partition == HIF_PARTITION_CLIPPED && NC % P != 0)
+      throw Error{HIF_ERR_ARG, "clipped partition needs (N+1) divisible by P"};
+    initialize();
+    t_total = t_gather = t_elim = t_id = t_host = 0;
+    cur_bytes = peak_bytes = 0;
+    HIF_CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), stream));
+    const double t0 = wall();
+    Sources a, b;
+    empty_sources(a, 0);
+    for (int level = 0; level < L; ++level) {
+      const double tl = wall();
+      schur_phase(level, a, b);
+      if (level < L - 1) {
+        skel_phase(level, b, a);
+      } else {
+        b.bufs.release(stream);
+      }
+      if (verbose) {
+        sync();
+        std::fprintf(stderr, "[hif] level %d: %.3f ms\n", level, 1e3 * (wall() - tl));
+      }
+    }
+    sync();
+    t_total = wall() - t0;
+    int st = 0;
+    HIF_CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    factored = true;
+    if (st & kStatusTinyPivot) throw Error{HIF_ERR_SINGULAR, "zero or non-finite pivot"};
+  }
+
+  // ---- Apply (src/Factor.cpp:992-1081) ------------------------------------
+  // Builds the launch list of one sweep. Matrices: X (r x s, ld r),
+  // W (k x r, ld k), A22 / A22^{-1} (r x r, ld r).
+  void add_gemv(ApplyPlan& plan, const StepData& st, int which, int trans, bool in_red,
+                bool out_red, double alpha, int mode, int in_vec, int out_vec) {
+    std::vector<GemvDesc> dd;
+    std::vector<int> toff(1, 0);
+    for (size_t b = 0; b < st.blocks.size(); ++b) {
+      const BlockInfo& bi = st.blocks[b];
+      const int r = bi.r(), s = bi.s();
+      if (r == 0 || (which < 2 && s == 0)) continue;
+      GemvDesc g{};
+      if (which == 0) {  // X: r x s
+        g.M = st.arena + st.o_x[b];
+        g.ld = r;
+        g.m = r;
+        g.n = s;
+      } else if (which == 1) {  // W: k x r
+        g.M = st.arena + st.o_w[b];
+        g.ld = s;
+        g.m = s;
+        g.n = r;
+      } else {  // 2: A22, 3: A22^{-1}
+        g.M = st.arena + (which == 2 ? st.o_a22[b] : st.o_inv[b]);
+        g.ld = r;
+        g.m = r;
+        g.n = r;
+      }
+      g.in_idx = in_red ? st.d_red + st.o_red[b] : st.d_skel + st.o_skel[b];
+      g.out_idx = out_red ? st.d_red + st.o_red[b] : st.d_skel + st.o_skel[b];
+      g.trans = trans;
+      g.alpha = alpha;
+      g.mode = mode;
+      g.contrib = (mode == 1) ? d_contrib + st.o_skel[b] : nullptr;
+      dd.push_back(g);
+      toff.push_back(toff.back() + gemv_tiles(g.m, g.n, trans));
+    }
+    if (dd.empty()) return;
+    ApplyLaunch l;
+    l.type = 0;
+    l.nd = dd.size();
+    l.tiles = toff.back();
+    l.in_vec = in_vec;
+    l.out_vec = out_vec;
+    l.d_toff = plan.bufs.add(upload(toff, stream));
+    l.d_desc = plan.bufs.add(upload(dd, stream));
+    plan.launches.push_back(l);
+  }
+
+  void add_reduce(ApplyPlan& plan, const StepData& st, double alpha, int vec) {
+    // every skeleton DOF of the level: its contribution slots in block order
+    std::map<int, std::vector<int>> by_dof;
+    std::vector<int> order;
+    for (size_t b = 0; b < st.blocks.size(); ++b) {
+      const BlockInfo& bi = st.blocks[b];
+      if (bi.r() == 0) continue;
+      for (int t = 0; t < bi.s(); ++t) {
+        const int p = bi.global[bi.skel_pos[t]];
+        auto it = by_dof.find(p);
+        if (it == by_dof.end()) {
+          order.push_back(p);
+          by_dof[p] = {};
+        }
+        by_dof[p].push_back((int)(st.o_skel[b] + t));
+      }
+    }
+    if (order.empty()) return;
+    std::vector<int> dof, off(1, 0), slot;
+    for (int p : order) {
+      dof.push_back(p);
+      for (int s : by_dof[p]) slot.push_back(s);
+      off.push_back((int)slot.size());
+    }
+    ApplyLaunch l;
+    l.type = 1;
+    l.d_dof = plan.bufs.add(upload(dof, stream));
+    l.d_off = plan.bufs.add(upload(off, stream));
+    l.d_slot = plan.bufs.add(upload(slot, stream));
+    l.ndof = dof.size();
+    l.alpha = alpha;
+    l.out_vec = vec;
+    plan.launches.push_back(l);
+  }
+
+  // Contribution buffer: max over phases of the skeleton slots, times the
+  // right-hand-side capacity; GEMV descriptors point into it directly.
+  long long contrib_ld = 1;
+  int contrib_cap = 0;
+
+  void build_plans(int nrhs_cap) {
+    release_plans();
+    long long max_slots = 1;
+    for (const StepData& st : steps) max_slots = std::max(max_slots, st.n_skel);
+    contrib_ld = max_slots;
+    dfree(d_contrib, stream);
+    d_contrib = dalloc<double>(max_slots * nrhs_cap, stream);
+    contrib_cap = nrhs_cap;
+    plan_inv.contrib_slots = plan_fwd.contrib_slots = max_slots;
+    // index steps by (level, kind)
+    std::vector<const StepData*> sch(L, nullptr), skl(L, nullptr);
+    for (const StepData& st : steps) (st.skel ? skl : sch)[st.level] = &st;
+    // inverse
+    {
+      ApplyPlan& p = plan_inv;
+      for (int l = 0; l < L - 1; ++l) {
+        if (sch[l]) {
+          add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 0, 0);
+          add_reduce(p, *sch[l], -1.0, 0);
+        }
+        if (skl[l]) {
+          add_gemv(p, *skl[l], 1, 1, false, true, -1.0, 0, 0, 0);
+          add_gemv(p, *skl[l], 0, 1, true, false, -1.0, 0, 0, 0);
+        }
+      }
+      for (int l = 0; l < L; ++l) {
+        if (sch[l]) add_gemv(p, *sch[l], 3, 0, true, true, 1.0, 2, 0, 1);
+        if (skl[l]) add_gemv(p, *skl[l], 3, 0, true, true, 1.0, 2, 0, 1);
+      }
+      for (int l = L - 2; l >= 0; --l) {
+        if (skl[l]) {
+          add_gemv(p, *skl[l], 0, 0, false, true, -1.0, 0, 1, 1);
+          add_gemv(p, *skl[l], 1, 0, true, false, -1.0, 0, 1, 1);
+        }
+        if (sch[l]) add_gemv(p, *sch[l], 0, 0, false, true, -1.0, 0, 1, 1);
+      }
+    }
+    // forward (F u)
+    {
+      ApplyPlan& p = plan_fwd;
+      for (int l = 0; l < L - 1; ++l) {
+        if (sch[l]) add_gemv(p, *sch[l], 0, 0, false, true, 1.0, 0, 0, 0);
+        if (skl[l]) {
+          add_gemv(p, *skl[l], 1, 0, true, false, 1.0, 0, 0, 0);
+          add_gemv(p, *skl[l], 0, 0, false, true, 1.0, 0, 0, 0);
+        }
+      }
+      for (int l = 0; l < L; ++l) {
+        if (sch[l]) add_gemv(p, *sch[l], 2, 0, true, true, 1.0, 2, 0, 1);
+        if (skl[l]) add_gemv(p, *skl[l], 2, 0, true, true, 1.0, 2, 0, 1);
+      }
+      for (int l = L - 2; l >= 0; --l) {
+        if (skl[l]) {
+          add_gemv(p, *skl[l], 0, 1, true, false, 1.0, 0, 1, 1);
+          add_gemv(p, *skl[l], 1, 1, false, true, 1.0, 0, 1, 1);
+        }
+        if (sch[l]) {
+          add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 1, 1);
+          add_reduce(p, *sch[l], 1.0, 1);
+        }
+      }
+    }
+    plans_built = true;
+  }
+
+  void ensure_workspace(int nrhs) {
+    if (!plans_built || contrib_cap < nrhs) build_plans(std::max(nrhs, contrib_cap));
+    if (ws_nrhs >= nrhs && d_ua) return;
+    dfree(d_ua, stream);
+    dfree(d_ub, stream);
+    d_ua = dalloc<double>(n3 * nrhs, stream);
+    d_ub = dalloc<double>(n3 * nrhs, stream);
+    ws_nrhs = nrhs;
+  }
+
+  void run_plan(ApplyPlan& plan, int nrhs) {
+    double* vec[2] = {d_ua, d_ub};
+    for (ApplyLaunch& l : plan.launches) {
+      if (l.type == 0) {
+        launch_gemv(l.d_desc, l.d_toff, l.nd, l.tiles, vec[l.in_vec], vec[l.out_vec], nrhs, n3,
+                    contrib_ld, stream);
+      } else {
+        launch_reduce_scatter(l.d_dof, l.d_off, l.d_slot, d_contrib, l.ndof, contrib_ld,
+                              l.alpha, vec[l.out_vec], nrhs, n3, stream);
+      }
+      HIF_CK(cudaGetLastError());
+    }
+  }
+
+  void apply_device(double* du, int nrhs, long long ldu, bool inverse) {
+    if (!factored) throw Error{HIF_ERR_STATE, "Apply before Factor"};
+    if (nrhs <= 0 || ldu < n3) throw Error{HIF_ERR_ARG, "bad nrhs / ldu"};
+    ensure_workspace(nrhs);
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(d_ua + c * n3, du + c * ldu, n3 * 8, cudaMemcpyDeviceToDevice,
+                             stream));
+    launch_zero_boundary(d_ua, NC, nrhs, n3, stream);
+    HIF_CK(cudaMemsetAsync(d_ub, 0, n3 * nrhs * 8, stream));
+    run_plan(inverse ? plan_inv : plan_fwd, nrhs);
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(du + c * ldu, d_ub + c * n3, n3 * 8, cudaMemcpyDeviceToDevice,
+                             stream));
+  }
+
+  // ---- PCG with the inverse apply as preconditioner -----------------------
+  void solve_pcg_device(const double* db, double* dx, int nrhs, long long ld, double tol,
+                        int maxit, int* iters, double* relres) {
+    if (!factored) throw Error{HIF_ERR_STATE, "solve before Factor"};
+    if (nrhs <= 0 || ld < n3) throw Error{HIF_ERR_ARG, "bad nrhs / ld"};
+    if (pcg_nrhs < nrhs) {
+      dfree(d_pcg, stream);
+      d_pcg = dalloc<double>(5 * n3 * nrhs + 8 * nrhs + (size_t)kDotBlocks * nrhs, stream);
+      pcg_nrhs = nrhs;
+    }
+    double* r = d_pcg;
+    double* z = r + n3 * nrhs;
+    double* p = z + n3 * nrhs;
+    double* q = p + n3 * nrhs;
+    double* x = q + n3 * nrhs;
+    double* sc = x + n3 * nrhs;  // rz, rz_new, pq, rr, bb
+    double* rz = sc;
+    double* rz_new = sc + nrhs;
+    double* pq = sc + 2 * nrhs;
+    double* rr = sc + 3 * nrhs;
+    double* bb = sc + 4 * nrhs;
+    double* part = sc + 8 * nrhs;
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(r + c * n3, db + c * ld, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+    launch_zero_boundary(r, NC, nrhs, n3, stream);
+    HIF_CK(cudaMemsetAsync(x, 0, n3 * nrhs * 8, stream));
+    launch_dot(r, r, n3, nrhs, n3, part, bb, stream);
+    // z = M r
+    auto precond = [&](double* in, double* outv) {
+      if (outv != in)
+        HIF_CK(cudaMemcpyAsync(outv, in, n3 * nrhs * 8, cudaMemcpyDeviceToDevice, stream));
+      apply_device(outv, nrhs, n3, true);
+    };
+    precond(r, z);
+    HIF_CK(cudaMemcpyAsync(p, z, n3 * nrhs * 8, cudaMemcpyDeviceToDevice, stream));
+    launch_dot(r, z, n3, nrhs, n3, part, rz, stream);
+    std::vector<double> h_bb(nrhs), h_rr(nrhs);
+    HIF_CK(cudaMemcpyAsync(h_bb.data(), bb, nrhs * 8, cudaMemcpyDeviceToHost, stream));
+    sync();
+    std::vector<int> done(nrhs, 0);
+    for (int c = 0; c < nrhs; ++c) {
+      iters[c] = 0;
+      relres[c] = h_bb[c] > 0 ? 1.0 : 0.0;
+      if (h_bb[c] == 0) done[c] = 1;
+    }
+    for (int it = 1; it <= maxit; ++it) {
+      bool all = true;
+      for (int c = 0; c < nrhs; ++c) all = all && done[c];
+      if (all) break;
+      launch_stencil_apply(d_band, NC, p, q, nrhs, n3, 0, stream);
+      launch_dot(p, q, n3, nrhs, n3, part, pq, stream);
+      launch_pcg_update_xr(x, r, p, q, rz, pq, n3, nrhs, n3, stream);
+      launch_dot(r, r, n3, nrhs, n3, part, rr, stream);
+      HIF_CK(cudaMemcpyAsync(h_rr.data(), rr, nrhs * 8, cudaMemcpyDeviceToHost, stream));
+      sync();
+      bool all_now = true;
+      for (int c = 0; c < nrhs; ++c) {
+        if (done[c]) continue;
+        relres[c] = std::sqrt(h_rr[c] / h_bb[c]);
+        iters[c] = it;
+        if (relres[c] <= tol) done[c] = 1;
+        all_now = all_now && done[c];
+      }
+      if (all_now) break;
+      precond(r, z);
+      launch_dot(r, z, n3, nrhs, n3, part, rz_new, stream);
+      launch_pcg_update_p(p, z, rz_new, rz, n3, nrhs, n3, stream);
+      HIF_CK(cudaMemcpyAsync(rz, rz_new, nrhs * 8, cudaMemcpyDeviceToDevice, stream));
+      HIF_CK(cudaGetLastError());
+    }
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(dx + c * ld, x + c * n3, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+    sync();
+  }
+};
+
+}  // namespace hif
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+struct hif_factor_s {
+  std::unique_ptr<hif::Engine> e;
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return HIF_OK;
+  } catch (const hif::Error& e) {
+    hif::g_last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    hif::g_last_error = "host allocation failed";
+    return HIF_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    hif::g_last_error = e.what();
+    return HIF_ERR_CUDA;
+  }
+}
+
+hif::StepData* find_step(hif_handle h, int level, int kind) {
+  for (hif::StepData& s : h->e->steps)
+    if (s.level == level && (int)s.skel == kind) return &s;
+  return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hif_last_error(void) { return hif::g_last_error.c_str(); }
+
+int hif_create(int N, int P, double epsilon, int partition, hif_handle* out) {
+  if (!out || N < 1 || P < 1 || !(epsilon > 0) ||
+      (partition != HIF_PARTITION_REFERENCE && partition != HIF_PARTITION_CLIPPED)) {
+    hif::g_last_error = "hif_create: invalid argument";
+    return HIF_ERR_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    hif::g_last_error = "no CUDA device";
+    return HIF_ERR_NODEVICE;
+  }
+  return guarded([&] {
+    auto* h = new hif_factor_s;
+    try {
+      h->e.reset(new hif::Engine(N, P, epsilon, partition));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int hif_destroy(hif_handle h) {
+  if (!h) return HIF_ERR_ARG;
+  return guarded([&] { delete h; });
+}
+
+int hif_set_stream(hif_handle h, void* stream) {
+  if (!h) return HIF_ERR_ARG;
+  return guarded([&] {
+    h->e->sync();
+    if (stream == nullptr) return;
+    h->e->stream = static_cast<cudaStream_t>(stream);
+  });
+}
+
+int hif_setup_stencil_device(hif_handle h, int N, double hstep, const double* dA,
+                             const double* dV) {
+  if (!h || !dA || !dV || N != h->e->N || !(hstep > 0)) return HIF_ERR_ARG;
+  return guarded([&] { h->e->setup_node_device(dA, dV, hstep); });
+}
+
+int hif_setup_stencil(hif_handle h, int N, double hstep, const double* A, const double* V) {
+  if (!h || !A || !V || N != h->e->N || !(hstep > 0)) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Engine& e = *h->e;
+    const long long nt = (long long)(N + 2) * (N + 2) * (N + 2);
+    std::vector<double> a(A, A + nt), v(V, V + nt);
+    double* dA = hif::upload(a, e.stream);
+    double* dV = hif::upload(v, e.stream);
+    e.setup_node_device(dA, dV, hstep);
+    hif::dfree(dA, e.stream);
+    hif::dfree(dV, e.stream);
+    e.sync();
+  });
+}
+
+int hif_setup_stencil_faces(hif_handle h, int N, double hstep, const double* ax,
+                            const double* ay, const double* az, const double* V) {
+  if (!h || !ax || !ay || !az || !V || N != h->e->N || !(hstep > 0)) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Engine& e = *h->e;
+    const long long nt = (long long)(N + 2) * (N + 2) * (N + 2);
+    std::vector<double> hx(ax, ax + nt), hy(ay, ay + nt), hz(az, az + nt), hv(V, V + nt);
+    double* dx = hif::upload(hx, e.stream);
+    double* dy = hif::upload(hy, e.stream);
+    double* dz = hif::upload(hz, e.stream);
+    double* dv = hif::upload(hv, e.stream);
+    hif::launch_setup_faces(dx, dy, dz, dv, N, hstep, e.d_band, e.stream);
+    HIF_CK(cudaGetLastError());
+    hif::dfree(dx, e.stream);
+    hif::dfree(dy, e.stream);
+    hif::dfree(dz, e.stream);
+    hif::dfree(dv, e.stream);
+    e.have_op = true;
+    e.sync();
+  });
+}
+
+int hif_initialize(hif_handle h) {
+  if (!h) return HIF_ERR_ARG;
+  return guarded([&] { h->e->initialize(); });
+}
+
+int hif_factor(hif_handle h) {
+  if (!h) return HIF_ERR_ARG;
+  return guarded([&] { h->e->factor(); });
+}
+
+int hif_apply_device(hif_handle h, double* du, int nrhs, long long ldu, int apply_inverse) {
+  if (!h || !du) return HIF_ERR_ARG;
+  return guarded([&] { h->e->apply_device(du, nrhs, ldu, apply_inverse != 0); });
+}
+
+int hif_apply(hif_handle h, double* u, int nrhs, long long ldu, int apply_inverse) {
+  if (!h || !u || nrhs <= 0) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Engine& e = *h->e;
+    if (ldu < e.n3) throw hif::Error{HIF_ERR_ARG, "ldu < (N+1)^3"};
+    double* d = hif::dalloc<double>(e.n3 * nrhs, e.stream);
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(d + c * e.n3, u + c * ldu, e.n3 * 8, cudaMemcpyHostToDevice, e.stream));
+    e.apply_device(d, nrhs, e.n3, apply_inverse != 0);
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(u + c * ldu, d + c * e.n3, e.n3 * 8, cudaMemcpyDeviceToHost, e.stream));
+    hif::dfree(d, e.stream);
+    e.sync();
+  });
+}
+
+int hif_spmv_device(hif_handle h, const double* dx, double* dy, int nrhs, long long ld,
+                    int transpose) {
+  if (!h || !dx || !dy || nrhs <= 0) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Engine& e = *h->e;
+    if (!e.have_op) throw hif::Error{HIF_ERR_STATE, "no operator"};
+    if (ld < e.n3) throw hif::Error{HIF_ERR_ARG, "ld < (N+1)^3"};
+    hif::launch_stencil_apply(e.d_band, e.NC, dx, dy, nrhs, ld, transpose, e.stream);
+    HIF_CK(cudaGetLastError());
+  });
+}
+
+int hif_spmv(hif_handle h, const double* x, double* y, int nrhs, long long ld, int transpose) {
+  if (!h || !x || !y || nrhs <= 0) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Engine& e = *h->e;
+    if (!e.have_op) throw hif::Error{HIF_ERR_STATE, "no operator"};
+    if (ld < e.n3) throw hif::Error{HIF_ERR_ARG, "ld < (N+1)^3"};
+    double* dx = hif::dalloc<double>(e.n3 * nrhs, e.stream);
+    double* dy = hif::dalloc<double>(e.n3 * nrhs, e.stream);
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(dx + c * e.n3, x + c * ld, e.n3 * 8, cudaMemcpyHostToDevice, e.stream));
+    hif::launch_stencil_apply(e.d_band, e.NC, dx, dy, nrhs, e.n3, transpose, e.stream);
+    HIF_CK(cudaGetLastError());
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(y + c * ld, dy + c * e.n3, e.n3 * 8, cudaMemcpyDeviceToHost, e.stream));
+    hif::dfree(dx, e.stream);
+    hif::dfree(dy, e.stream);
+    e.sync();
+  });
+}
+
+int hif_solve_pcg_device(hif_handle h, const double* db, double* dx, int nrhs, long long ld,
+                         double tol, int maxit, int* iters, double* relres) {
+  if (!h || !db || !dx || !iters || !relres || nrhs <= 0 || maxit < 0) return HIF_ERR_ARG;
+  return guarded([&] { h->e->solve_pcg_device(db, dx, nrhs, ld, tol, maxit, iters, relres); });
+}
+
+int hif_solve_pcg(hif_handle h, const double* b, double* x, int nrhs, long long ld, double tol,
+                  int maxit, int* iters, double* relres) {
+  if (!h || !b || !x || !iters || !relres || nrhs <= 0 || maxit < 0) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Engine& e = *h->e;
+    if (ld < e.n3) throw hif::Error{HIF_ERR_ARG, "ld < (N+1)^3"};
+    double* db = hif::dalloc<double>(e.n3 * nrhs, e.stream);
+    double* dx = hif::dalloc<double>(e.n3 * nrhs, e.stream);
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(db + c * e.n3, b + c * ld, e.n3 * 8, cudaMemcpyHostToDevice, e.stream));
+    e.solve_pcg_device(db, dx, nrhs, e.n3, tol, maxit, iters, relres);
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(x + c * ld, dx + c * e.n3, e.n3 * 8, cudaMemcpyDeviceToHost, e.stream));
+    hif::dfree(db, e.stream);
+    hif::dfree(dx, e.stream);
+    e.sync();
+  });
+}
+
+int hif_num_levels(hif_handle h, int* levels) {
+  if (!h || !levels) return HIF_ERR_ARG;
+  *levels = h->e->initialized ? h->e->L : h->e->levels_for();
+  return HIF_OK;
+}
+
+int hif_num_blocks(hif_handle h, int level, int kind, int* nblocks) {
+  if (!h || !nblocks) return HIF_ERR_ARG;
+  hif::StepData* s = find_step(h, level, kind);
+  *nblocks = s ? (int)s->blocks.size() : 0;
+  return HIF_OK;
+}
+
+int hif_block_info(hif_handle h, int level, int kind, int b, int* ng, int* nr, int* ns,
+                   int* face) {
+  if (!h) return HIF_ERR_ARG;
+  hif::StepData* s = find_step(h, level, kind);
+  if (!s || b < 0 || b >= (int)s->blocks.size()) return HIF_ERR_ARG;
+  const hif::BlockInfo& bi = s->blocks[b];
+  if (ng) *ng = bi.global.size();
+  if (nr) *nr = bi.r();
+  if (ns) *ns = bi.s();
+  if (face) *face = bi.face;
+  return HIF_OK;
+}
+
+int hif_block_indices(hif_handle h, int level, int kind, int b, int* g, int* r, int* s_) {
+  if (!h) return HIF_ERR_ARG;
+  hif::StepData* s = find_step(h, level, kind);
+  if (!s || b < 0 || b >= (int)s->blocks.size()) return HIF_ERR_ARG;
+  const hif::BlockInfo& bi = s->blocks[b];
+  if (g) std::copy(bi.global.begin(), bi.global.end(), g);
+  if (r) std::copy(bi.red_pos.begin(), bi.red_pos.end(), r);
+  if (s_) std::copy(bi.skel_pos.begin(), bi.skel_pos.end(), s_);
+  return HIF_OK;
+}
+
+int hif_block_matrix(hif_handle h, int level, int kind, int b, int which, double* out) {
+  if (!h || !out) return HIF_ERR_ARG;
+  hif::StepData* s = find_step(h, level, kind);
+  if (!s || b < 0 || b >= (int)s->blocks.size()) return HIF_ERR_ARG;
+  return guarded([&] {
+    const hif::BlockInfo& bi = s->blocks[b];
+    const long long r = bi.r(), k = bi.s();
+    long long off = 0, cnt = 0;
+    switch (which) {
+      case 0: off = s->o_a22[b]; cnt = r * r; break;
+      case 1: off = s->o_inv[b]; cnt = r * r; break;
+      case 2: off = s->o_x[b]; cnt = r * k; break;
+      case 3:
+        if (!s->skel) throw hif::Error{HIF_ERR_ARG, "W exists for skeletonization blocks only"};
+        off = s->o_w[b];
+        cnt = k * r;
+        break;
+      case 4:
+        if (!h->e->keep_schur) throw hif::Error{HIF_ERR_STATE, "enable HIF_OPT_KEEP_SCHUR"};
+        if (r == 0) {
+          std::fill(out, out + k * k, 0.0);
+        } else {
+          std::copy(bi.S.begin(), bi.S.end(), out);
+        }
+        return;
+      default:
+        throw hif::Error{HIF_ERR_ARG, "which"};
+    }
+    if (cnt == 0) return;
+    h->e->sync();
+    HIF_CK(cudaMemcpy(out, s->arena + off, cnt * 8, cudaMemcpyDeviceToHost));
+  });
+}
+
+int hif_block_pivots(hif_handle h, int level, int b, int* jpvt, double* rdiag) {
+  if (!h) return HIF_ERR_ARG;
+  hif::StepData* s = find_step(h, level, 1);
+  if (!s || b < 0 || b >= (int)s->blocks.size()) return HIF_ERR_ARG;
+  const hif::BlockInfo& bi = s->blocks[b];
+  if (jpvt) std::copy(bi.jpvt.begin(), bi.jpvt.end(), jpvt);
+  if (rdiag) std::copy(bi.rdiag.begin(), bi.rdiag.end(), rdiag);
+  return HIF_OK;
+}
+
+int hif_set_option(hif_handle h, int option, long long value) {
+  if (!h) return HIF_ERR_ARG;
+  switch (option) {
+    case HIF_OPT_KEEP_SCHUR: h->e->keep_schur = value != 0; return HIF_OK;
+    case HIF_OPT_VERBOSE: h->e->verbose = value != 0; return HIF_OK;
+    case HIF_OPT_MEM_BUDGET_MB: h->e->budget_mb = value; return HIF_OK;
+  }
+  return HIF_ERR_ARG;
+}
+
+int hif_set_replay_pivots(hif_handle h, int level, int nfaces, const int* offsets,
+                          const int* orders) {
+  if (!h || level < 0 || nfaces < 0) return HIF_ERR_ARG;
+  if (nfaces == 0) {
+    h->e->replay.erase(level);
+    return HIF_OK;
+  }
+  if (!offsets || !orders) return HIF_ERR_ARG;
+  std::vector<std::vector<int>> v(nfaces);
+  for (int f = 0; f < nfaces; ++f) v[f].assign(orders + offsets[f], orders + offsets[f + 1]);
+  h->e->replay[level] = std::move(v);
+  return HIF_OK;
+}
+
+int hif_factor_stats(hif_handle h, double* total_s, double* gather_s, double* elim_s,
+                     double* id_s, double* host_s, long long* device_bytes) {
+  if (!h) return HIF_ERR_ARG;
+  hif::Engine& e = *h->e;
+  if (total_s) *total_s = e.t_total;
+  if (gather_s) *gather_s = e.t_gather;
+  if (elim_s) *elim_s = e.t_elim;
+  if (id_s) *id_s = e.t_id;
+  if (host_s) *host_s = e.t_host;
+  if (device_bytes) *device_bytes = e.peak_bytes;
+  return HIF_OK;
+}
+
+int hif_partition_cell(int N, int P, int level, int ci, int cj, int ck, int reserved,
+                       const unsigned char* mask, int* g, int* r, int* s_, int* counts) {
+  if (N < 1 || P < 1 || level < 0 || !mask || !g || !r || !s_ || !counts || reserved != 0)
+    return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Partitioner part{N, P, N + 1, mask};
+    const int c[3] = {ci, cj, ck};
+    std::vector<int> gg, rr, ss;
+    part.cell_index(level, c, gg, rr, ss);
+    std::copy(gg.begin(), gg.end(), g);
+    std::copy(rr.begin(), rr.end(), r);
+    std::copy(ss.begin(), ss.end(), s_);
+    counts[0] = gg.size();
+    counts[1] = rr.size();
+    counts[2] = ss.size();
+  });
+}
+
+int hif_partition_face(int N, int P, int level, int ci, int cj, int ck, int face, int reserved,
+                       const unsigned char* mask, int* rows, int* cols) {
+  if (N < 1 || P < 1 || level < 0 || !mask || !rows || !cols || reserved != 0) return HIF_ERR_ARG;
+  if (face != hif::TOP && face != hif::LEFT && face != hif::FRONT) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Partitioner part{N, P, N + 1, mask};
+    const int c[3] = {ci, cj, ck};
+    std::vector<int> rw, cl;
+    int nb[3];
+    if (!part.skel_interaction(level, c, face, rw, cl, nb)) {
+      rw.clear();
+      cl.clear();
+    }
+    rows[0] = rw.size();
+    cols[0] = cl.size();
+    std::copy(rw.begin(), rw.end(), rows + 1);
+    std::copy(cl.begin(), cl.end(), cols + 1);
+  });
+}
+
+}  // extern "C"

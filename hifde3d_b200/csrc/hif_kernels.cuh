@@ -1,0 +1,185 @@
+// Device kernels of the HIF factor / apply path (sm_100a, FP64).
+//
+// Every launcher takes device-resident descriptor arrays and a stream; the
+// host engine (hif_engine.cpp) builds the descriptors per level phase.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace hif {
+
+// ---------------------------------------------------------------------------
+// Status bits written by kernels (OR-ed into a device word per phase).
+// ---------------------------------------------------------------------------
+enum StatusBits : int {
+  kStatusTinyPivot = 1,   // |pivot| <= 1e-300 or not finite in an elimination
+  kStatusNonFinite = 2,   // NaN / Inf met in an output
+  kStatusIdZero = 4,      // ID of an all-zero face block (every column redundant)
+};
+
+// A DOF's membership in one dense source block: source id and position.
+struct CoverEntry {
+  int src;  // < 0: unused slot
+  int pos;
+};
+constexpr int kCover = 3;
+
+// One dense "source" of the remaining operator (a Schur complement block).
+struct SourceDesc {
+  const double* ptr;
+  long long ld;
+};
+
+// Assembly target: out(i, j) = A0(rows[i], cols[j]) + sum over the sources s
+// that hold both DOFs rows[i] and cols[j] and are admitted for this target,
+// of s(pos(rows[i]), pos(cols[j])).
+//
+// Source membership comes from per-DOF arrays (6 x NC^3 ints): for DOF p,
+// dof_src[(2c) NC^3 + p] / dof_src[(2c+1) NC^3 + p] are (source, position)
+// for slot c in {0: cell having p on its low face, 1: cell having p on its
+// high face, 2: skeletonized face containing p}; source < 0 means none.
+struct GatherTarget {
+  double* out;
+  long long ld;
+  const int* rows;
+  const int* cols;
+  double* a22_out;  // optional copy of out[0:r, 0:r] (ld r)
+  int m, n;
+  int a0_skip;      // no stencil term where i >= a0_skip && j >= a0_skip
+  int r;
+  int mode;         // 0: sources with src_owner[s] == owner; 1: s in {allowA, allowB}; 2: none
+  int owner;
+  int allowA, allowB;
+};
+
+// C(m x n) = beta * C + alpha * op(A) * op(B); column-major.
+struct GemmDesc {
+  double* C;
+  const double* A;
+  const double* B;
+  long long ldc, lda, ldb;
+  int m, n, k;
+  int transA, transB;
+  double alpha, beta;
+};
+
+// Dense elimination block: B (n x n, ld n) in assembly order [red | skel].
+struct SweepDesc {
+  double* B;
+  double* a22inv;  // r x r, ld r  (compact copy written at the end)
+  double* X;       // r x s, ld r
+  int n, r;
+};
+
+// Interpolative decomposition of M (m x n, ld m) for one face.
+struct IdDesc {
+  double* M;
+  const int* order;  // optional prescribed column order (replay), else null
+  int* jpvt;         // n: 0-based pivot order
+  double* rdiag;     // n: diagonal of R
+  int* keep;         // n: 1 if |R_ii| > eps |R_00|
+  int* rank;         // 1
+  double* W;         // k x (n-k), ld k (written after the rank is known)
+  int m, n;
+};
+
+// Apply: y = op(M) x[in] with x, y gathered / scattered through DOF lists.
+struct GemvDesc {
+  const double* M;
+  long long ld;
+  const int* in_idx;
+  const int* out_idx;   // mode 0 / 2
+  double* contrib;      // mode 1: contribution slots (length = rows of op(M))
+  int m, n;             // M is m x n
+  int trans;            // 0: y = M x (len m), 1: y = M^T x (len n)
+  double alpha;
+  int mode;             // 0: u_out[out] += alpha y; 1: contrib = y; 2: u_out[out] = alpha y
+};
+
+struct CopyDesc {
+  const double* src;
+  double* dst;
+  long long lds, ldd;
+  int m, n;
+};
+
+// ---------------------------------------------------------------------------
+// Launchers. Descriptor arrays live in device memory; tile_off (device) is
+// the prefix sum of per-descriptor tile counts, total = tile_off[count].
+// ---------------------------------------------------------------------------
+void launch_gather(const GatherTarget* d_tg, const int* d_tile_off, int ntg, int total_tiles,
+                   const SourceDesc* d_src, const int* d_src_owner, const int* d_dof_src,
+                   const double* d_band, long long ncell3, int NC, cudaStream_t s);
+int gather_tiles(int m, int n);
+
+void launch_dgemm(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                  cudaStream_t s);
+int dgemm_tiles(int m, int n);
+
+// In-shared-memory Gauss-Jordan sweep of the first r pivots (n <= kSmallSweepN).
+constexpr int kSmallSweepN = 160;
+void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_status,
+                        cudaStream_t s);
+
+// Blocked sweep, one pivot block [k0, k0+nbk) of every active block.
+constexpr int kSweepNB = 64;
+void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
+                       double* d_dinv, int* d_status, cudaStream_t s);
+// Panel tile maps hold 4 ints per tile: {descriptor, lo, hi, unused}; the
+// row panel covers columns [lo, hi) of pivot rows, the column panel rows
+// [lo, hi) of pivot columns. d_dinv holds kSweepNB^2 doubles per descriptor.
+void launch_sweep_rowpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
+                           const double* d_dinv, cudaStream_t s);
+void launch_sweep_colpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
+                           const double* d_dinv, cudaStream_t s);
+void launch_sweep_setdiag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
+                          const double* d_dinv, cudaStream_t s);
+
+// Column-pivoted Householder QR + rank + interpolation matrix, one CTA per face.
+// W is written to IdDesc::W, which must hold at least n*n/4 + n doubles.
+void launch_id(const IdDesc* d_desc, int nd, int max_n, double eps, int* d_status,
+               cudaStream_t s);
+
+void launch_copy(const CopyDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                 cudaStream_t s);
+int copy_tiles(int m, int n);
+
+// contrib_ld: stride between right-hand sides in the contribution buffer.
+void launch_gemv(const GemvDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                 const double* u_in, double* u_out, int nrhs, long long ldu,
+                 long long contrib_ld, cudaStream_t s);
+int gemv_tiles(int m, int n, int trans);
+
+// u[dof[d]] += alpha * sum_{t in [off[d], off[d+1])} contrib[slot[t]], in order.
+void launch_reduce_scatter(const int* d_dof, const int* d_off, const int* d_slot,
+                           const double* d_contrib, int ndof, long long contrib_ld,
+                           double alpha, double* u, int nrhs, long long ldu, cudaStream_t s);
+
+// Operators and vectors.
+void launch_setup_node(const double* d_A, const double* d_V, int N, double h, double* d_band,
+                       cudaStream_t s);
+void launch_setup_faces(const double* d_ax, const double* d_ay, const double* d_az,
+                        const double* d_V, int N, double h, double* d_band, cudaStream_t s);
+void launch_stencil_apply(const double* d_band, int NC, const double* x, double* y, int nrhs,
+                          long long ldx, int transpose, cudaStream_t s);
+void launch_zero_boundary(double* u, int NC, int nrhs, long long ldu, cudaStream_t s);
+void launch_copy_vec(const double* x, double* y, long long n, cudaStream_t s);
+
+// Deterministic dot products: out[c] = sum_i x[i + c ld] y[i + c ld] (per rhs c).
+void launch_dot(const double* x, const double* y, long long n, int nrhs, long long ld,
+                double* d_partial, double* d_out, cudaStream_t s);
+constexpr int kDotBlocks = 296;
+
+// PCG vector updates (all per rhs column c, scalars from device arrays):
+//   x += a p; r -= a q with a = rz / pq
+void launch_pcg_update_xr(double* x, double* r, const double* p, const double* q,
+                          const double* rz, const double* pq, long long n, int nrhs,
+                          long long ld, cudaStream_t s);
+//   p = z + (rz_new / rz_old) p
+void launch_pcg_update_p(double* p, const double* z, const double* rz_new,
+                         const double* rz_old, long long n, int nrhs, long long ld,
+                         cudaStream_t s);
+
+}  // namespace hif

@@ -1,0 +1,144 @@
+/*
+ * hif_b200.h -- C ABI of the B200 implementation of HIFDE3D's hierarchical
+ * interpolative factorization (HIF) for 3D 7-point elliptic operators.
+ *
+ * The reference (arbenson/HIFDE3D) exposes a C++ template API; each entry
+ * point below replaces one call of it for Scalar = double. All functions
+ * return an int status (HIF_OK = 0). Handles are not thread-safe; one handle
+ * drives one CUDA device (the device current at hif_create) and one stream.
+ *
+ * Host-pointer entry points copy their inputs to the GPU and their results
+ * back; *_device entry points take device pointers on that device and do not
+ * synchronise the stream unless stated.
+ *
+ * Vector layout everywhere: NC^3 entries (NC = N + 1), DOF id
+ * i + NC*j + NC^2*k for i, j, k in [0, N]; entries with i, j or k equal to 0 are
+ * the Dirichlet planes and are ignored / zeroed (src/Factor.cpp:79-89,977-990).
+ * Several right-hand sides are stored column-major with leading dimension ldu.
+ */
+#ifndef HIF_B200_H_
+#define HIF_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hif_factor_s* hif_handle;
+
+enum hif_status {
+  HIF_OK = 0,
+  HIF_ERR_ARG = 1,        /* invalid argument */
+  HIF_ERR_CUDA = 2,       /* CUDA runtime error (message: hif_last_error) */
+  HIF_ERR_NOMEM = 3,      /* device allocation failed */
+  HIF_ERR_SINGULAR = 4,   /* zero / non-finite pivot in an elimination */
+  HIF_ERR_STATE = 5,      /* call out of order (e.g. Apply before Factor) */
+  HIF_ERR_NODEVICE = 6,   /* no CUDA device / kernels not loadable */
+  HIF_ERR_BUDGET = 7      /* would exceed the handle's memory budget */
+};
+
+enum hif_partition {
+  HIF_PARTITION_REFERENCE = 0, /* cells_per_dir = NC / width (src/Factor.cpp:52-53) */
+  HIF_PARTITION_CLIPPED = 1    /* ceil(NC / width), last cell clipped at N */
+};
+
+/* HIFFactor<double>(int N, int P, double epsilon) -- include/Factor.hpp:12-13. */
+int hif_create(int N, int P, double epsilon, int partition, hif_handle* out);
+/* ~HIFFactor -- include/Factor.hpp:15. */
+int hif_destroy(hif_handle h);
+
+/* Stream used by every call on this handle (a cudaStream_t; 0 = the handle's own). */
+int hif_set_stream(hif_handle h, void* stream);
+
+/* SetupStencil(factor, N, h, A, V) -- include/setup_stencil.hpp:6-76.
+ * A, V: (N+2)^3 float64 tensors in NumTns order (i fastest, include/numtns.hpp:99). */
+int hif_setup_stencil(hif_handle h, int N, double hstep, const double* A, const double* V);
+int hif_setup_stencil_device(hif_handle h, int N, double hstep, const double* dA,
+                             const double* dV);
+/* Symmetric flux form -div(a grad u) + V u with face coefficients (no reference
+ * counterpart; the reference's node form is non-symmetric for variable a).
+ * ax(i,j,k) couples (i,j,k)-(i+1,j,k); ay, az likewise; all (N+2)^3, i fastest. */
+int hif_setup_stencil_faces(hif_handle h, int N, double hstep, const double* ax,
+                            const double* ay, const double* az, const double* V);
+
+/* HIFFactor::Initialize -- src/Factor.cpp:6-39. */
+int hif_initialize(hif_handle h);
+/* HIFFactor::Factor -- src/Factor.cpp:41-63. */
+int hif_factor(hif_handle h);
+
+/* HIFFactor::Apply(u, apply_inverse) -- src/Factor.cpp:992-1081, in place. */
+int hif_apply(hif_handle h, double* u, int nrhs, long long ldu, int apply_inverse);
+int hif_apply_device(hif_handle h, double* du, int nrhs, long long ldu, int apply_inverse);
+
+/* SpMV(sp_matrix, x, y) -- src/Factor.cpp:1099-1113: y = A^T x (the reference walks
+ * columns); transpose = 0 gives y = A x. The operator is the one set up, kept intact
+ * by hif_factor (the reference consumes its sparse matrix). */
+int hif_spmv(hif_handle h, const double* x, double* y, int nrhs, long long ld, int transpose);
+int hif_spmv_device(hif_handle h, const double* dx, double* dy, int nrhs, long long ld,
+                    int transpose);
+
+/* Preconditioned CG on A x = b with the factor's inverse apply as preconditioner and
+ * an FP64 residual on the operator (the reference has no iterative solver; its driver
+ * only reports e_a / e_s, tests/HIFDE3D/main.cpp:121-134). x is an output (x0 = 0).
+ * iters, relres: per right-hand side. */
+int hif_solve_pcg(hif_handle h, const double* b, double* x, int nrhs, long long ld,
+                  double tol, int maxit, int* iters, double* relres);
+int hif_solve_pcg_device(hif_handle h, const double* db, double* dx, int nrhs, long long ld,
+                         double tol, int maxit, int* iters, double* relres);
+
+/* ---- introspection (schur_level_data / skel_level_data, include/Factor.hpp:50-51,
+ *      declared but not defined by the reference) --------------------------------- */
+int hif_num_levels(hif_handle h, int* levels);
+/* kind: 0 = Schur (cell interiors), 1 = skeletonization (faces). */
+int hif_num_blocks(hif_handle h, int level, int kind, int* nblocks);
+/* Sizes of block b: |global_inds|, |redundant_inds|, |skeleton_inds| and the face
+ * (data.hpp enum, -1 for Schur blocks). */
+int hif_block_info(hif_handle h, int level, int kind, int b, int* ng, int* nr, int* ns,
+                   int* face);
+/* Index data exactly as the reference's IndexData (include/data.hpp:11-62). */
+int hif_block_indices(hif_handle h, int level, int kind, int b, int* global_inds,
+                      int* redundant_inds, int* skeleton_inds);
+/* which: 0 A_22, 1 A_22^{-1}, 2 X = A_22^{-1} A_21, 3 W (skeletonization only),
+ * 4 Schur complement S (only with HIF_OPT_KEEP_SCHUR). Column-major, rows / columns
+ * ordered as redundant_inds / skeleton_inds. */
+int hif_block_matrix(hif_handle h, int level, int kind, int b, int which, double* out);
+/* Pivot order (0-based, n entries) and R diagonal of a skeletonized face's ID. */
+int hif_block_pivots(hif_handle h, int level, int b, int* jpvt, double* rdiag);
+
+enum hif_option {
+  HIF_OPT_KEEP_SCHUR = 1,    /* keep every Schur complement for hif_block_matrix(which=4) */
+  HIF_OPT_VERBOSE = 2,       /* per-phase timings on stderr */
+  HIF_OPT_MEM_BUDGET_MB = 3  /* refuse factorizations whose device memory exceeds this */
+};
+int hif_set_option(hif_handle h, int option, long long value);
+
+/* Test hook: prescribe the ID column order of every face of one level (replay of
+ * another implementation's pivot decisions). offsets: nfaces+1 prefix offsets into
+ * orders. Pass nfaces = 0 to clear. */
+int hif_set_replay_pivots(hif_handle h, int level, int nfaces, const int* offsets,
+                          const int* orders);
+
+/* Timings of the last hif_factor in seconds: total, and per phase kind (gather,
+ * elimination, ID, host partition). */
+int hif_factor_stats(hif_handle h, double* total_s, double* gather_s, double* elim_s,
+                     double* id_s, double* host_s, long long* device_bytes);
+
+/* ---- host-only test hooks of the partitioner (no GPU needed) ---------------------
+ * Index data over a caller-given remaining-DOF mask (NC^3 bytes, DOF order).
+ * hif_partition_cell: InteriorCellIndexData (src/Factor.cpp:359-392); counts[3] =
+ * {|global|, |red|, |skel|}. hif_partition_face: SkelInteractionIndexData
+ * (src/Factor.cpp:645-755) for face TOP / LEFT / FRONT; rows[0], cols[0] hold the
+ * counts, entries follow. Output arrays must hold NC^3 (+1) ints. reserved: 0. */
+int hif_partition_cell(int N, int P, int level, int ci, int cj, int ck, int reserved,
+                       const unsigned char* mask, int* global_inds, int* redundant_inds,
+                       int* skeleton_inds, int* counts);
+int hif_partition_face(int N, int P, int level, int ci, int cj, int ck, int face,
+                       int reserved, const unsigned char* mask, int* rows, int* cols);
+
+/* Message of the last error on this thread. */
+const char* hif_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIF_B200_H_ */
