@@ -1,0 +1,394 @@
+"""Benchmark of the HIF hot path on B200: factor + FP64-residual PCG solve.
+
+One step = assemble the face-coefficient operator from HBM-resident coefficient
+arrays, hif_factor (every level: assembly, eliminations, IDs) and one PCG solve
+to relative residual 1e-10 with the factor's inverse apply as preconditioner,
+at n = 128 (N = 127, 2,048,383 DOFs), a = exp(GRF) at faces (correlation 1/16,
+sigma 1, seed 2), eps = 1e-6, FP64. The metric's unit is whole-job
+(factor + solve) steps per second; factor seconds, solves per second and PCG
+iterations are reported alongside.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--n 128]
+
+Multi-GPU: replicas (each rank factors and solves its own operator; the path has
+no exchange step), timing is the max over ranks.
+
+--impl reference times the reference's own CPU build (oracle/_ref, built from
+arbenson/HIFDE3D's sources) on this host's cores over a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("factor s + solves/sec at N=128^3, resid<=1e-10: mixed vs FP64 GPU; "
+          "serving p50/p99 ms")
+REF_PROBE = os.path.join(ROOT, "oracle", "_ref", "hif_ref_probe")
+
+
+def dofs(n: int) -> int:
+    return (n - 1) ** 3
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU build on this host
+# ---------------------------------------------------------------------------
+def reference_sample(n_sample: int, threads: int, workdir: str):
+    """Reference Factor() + one Apply(u, true) at n_sample with a = exp(GRF) at nodes.
+
+    Returns seconds. The reference has no face-coefficient operator; its node form
+    with the same field sampled at nodes has the same block structure and cost."""
+    from hifde3d_b200 import synth
+    N = n_sample - 1
+    NC = N + 1
+    g = synth.gaussian_random_field(NC, 2, 1.0 / 16, 1.0)
+    idx = (2 * np.arange(NC + 1)) % g.shape[0]
+    A = np.exp(g[np.ix_(idx, idx, idx)])
+    V = np.zeros_like(A)
+    fa, fv = os.path.join(workdir, "A.bin"), os.path.join(workdir, "V.bin")
+    A.ravel(order="F").astype("<f8").tofile(fa)
+    V.ravel(order="F").astype("<f8").tofile(fv)
+    env = dict(os.environ, OPENBLAS_NUM_THREADS=str(threads), OMP_NUM_THREADS=str(threads))
+    t0 = time.perf_counter()
+    out = subprocess.run([REF_PROBE, "time", str(N), "4", "1e-6", "-1", fa, fv], env=env,
+                         capture_output=True, text=True, check=True).stdout
+    wall = time.perf_counter() - t0
+    rec = json.loads(out.strip().splitlines()[-1])
+    return rec["factor_s"] + max(rec["apply_inv_s"], 0.0), wall, rec
+
+
+def reference_units(sample_s: float, n_sample: int, n: int) -> float:
+    """Steps per second at size n from a sample at n_sample, scaling the sample's
+    time linearly in DOFs. The reference's update phase grows faster than linearly
+    (about 50x per doubling of n measured from 32 to 64), so this overstates the
+    reference's speed: a conservative stand-in."""
+    return 1.0 / (sample_s * dofs(n) / dofs(n_sample))
+
+
+def run_reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return
+    steps, warm = args.steps, args.warmup
+    n_sample = 32 if (steps + warm) * 15 <= 240 else 16
+    threads = os.cpu_count() or 1
+    if not os.path.exists(REF_PROBE):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/hif_ref_probe not built (make -C oracle)"}))
+        return
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        for i in range(warm + steps):
+            s, _, _ = reference_sample(n_sample, threads, td)
+            if i >= warm:
+                times.append(s)
+    t = float(np.mean(times))
+    value = reference_units(t, n_sample, args.n)
+    sample = (f"reference Factor() + Apply(u, true) at n={n_sample} ({dofs(n_sample)} DOFs), "
+              f"node operator a=exp(GRF) at nodes, eps=1e-6, OpenBLAS {threads} threads; "
+              f"scaled to n={args.n} linearly in DOFs (a lower bound on the reference's time)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value,
+        "unit": f"factor+solve steps/s at n={args.n}", "n_gpus": world, "steps": steps,
+        "warmup": warm, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"hif factor+pcg n={args.n} (sampled at n={n_sample})"},
+        "cpu_baseline": {"value": value, "unit": f"factor+solve steps/s at n={args.n}",
+                         "cores": threads, "kind": "reference", "sample": sample,
+                         "measured_sample_s": t},
+        "e2e": {"value": value, "unit": f"factor+solve steps/s at n={args.n}",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def fp64_gemm_peak(torch, dev):
+    """cuBLAS DGEMM 8192^3 burst rate in TFLOP/s (the FP64 roofline denominator)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def run_ours(args, rank: int, world: int):
+    import torch
+    import torch.distributed as dist
+
+    import hifde3d_b200 as hb
+    from hifde3d_b200 import synth
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    N, NC = n - 1, n
+    eps = args.eps
+
+    # synthetic operator (per-rank seed for replicas) and right-hand side
+    ax, ay, az = synth.face_coefficients_grf(N, 2 + rank, 1.0 / 16, 1.0)
+    V = np.zeros((NC + 1,) * 3)
+    b = synth.dof_vector(N, rank)
+    host = [np.ascontiguousarray(x.ravel(order="F")) for x in (ax, ay, az, V)]
+    dcoef = [torch.from_numpy(x).to(dev) for x in host]
+    db = torch.from_numpy(b).to(dev)
+    dx = torch.zeros_like(db)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+
+    peak_fp64 = fp64_gemm_peak(torch, dev) if rank == 0 else None
+
+    f = hb.HIFFactor(N, 4, eps)
+    stream = torch.cuda.Stream(device=dev)
+    hb.set_stream(f, stream.cuda_stream)
+    h = 1.0 / NC
+
+    def step():
+        hb.SetupStencilFacesDevice(f, N, h, *[t.data_ptr() for t in dcoef])
+        f.Factor()
+        it, rr = f.solve_pcg_device(db.data_ptr(), dx.data_ptr(), 1, NC ** 3, 1e-10, 100)
+        return int(it[0]), float(rr[0])
+
+    # warm-up
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # timed region: K steps, profiled launch by launch (CUDA events on the stream)
+    f.set_option(hb.OPT_PROFILE, 1)
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    iters, rel, fac = [], [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        it, rr = step()
+        iters.append(it)
+        rel.append(rr)
+        fac.append(f.factor_stats()["total_s"])
+    t_end.record(stream)
+    t_end.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms_total = t_start.elapsed_time(t_end)
+    kst = f.kernel_stats()
+    f.set_option(hb.OPT_PROFILE, 0)
+
+    # solve-only throughput with the resident factor
+    solve_ms = []
+    for _ in range(max(3, args.steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f.solve_pcg_device(db.data_ptr(), dx.data_ptr(), 1, NC ** 3, 1e-10, 100)
+        e1.record(stream)
+        e1.synchronize()
+        solve_ms.append(e0.elapsed_time(e1))
+
+    # end to end through the public API with host buffers
+    xh = np.zeros_like(b)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        hb.SetupStencilFaces(f, N, h, ax, ay, az, V)
+        f.Factor()
+        xh, it_e2e, rr_e2e = f.solve_pcg(b, 1e-10, 100)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    h2d = 4 * (NC + 1) ** 3 * 8 + NC ** 3 * 8
+    d2h = NC ** 3 * 8
+
+    # max over ranks
+    ms_step = ms_total / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step, e2e_s = float(t[0]), float(t[1])
+    if rank != 0:
+        f.close()
+        return
+
+    # roofline of the dominant kernel class
+    dom = max(kst, key=lambda k: kst[k]["ms"])
+    k = kst[dom]
+    per_launch_ms = k["ms"] / max(k["launches"], 1)
+    traffic = None
+    tf_path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(tf_path):
+        with open(tf_path) as fh:
+            traffic = json.load(fh).get(dom)
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        with open(pk_path) as fh:
+            peaks = json.load(fh)
+    if k["flops"] > 0:
+        achieved = k["flops"] / max(k["launches"], 1) / (per_launch_ms * 1e-3) / 1e12
+        roof = {"bound": "fp64", "kernel_class": dom, "achieved": achieved, "peak": peak_fp64,
+                "unit": "TFLOP/s", "frac": achieved / peak_fp64 if peak_fp64 else None,
+                "traffic": traffic, "launches": k["launches"],
+                "avg_launch_ms": per_launch_ms,
+                "peak_source": "cuBLAS DGEMM 8192^3 burst measured in this run (FP64 has no "
+                               "entry in MEASURED_PEAKS.json)"}
+    else:
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        achieved = k["bytes"] / max(k["launches"], 1) / (per_launch_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel_class": dom, "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "launches": k["launches"], "avg_launch_ms": per_launch_ms,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"}
+    share = {kk: round(v["ms"] / max(sum(x["ms"] for x in kst.values()), 1e-9), 4)
+             for kk, v in kst.items() if v["launches"]}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline and os.path.exists(REF_PROBE):
+        with tempfile.TemporaryDirectory() as td:
+            s, _, _ = reference_sample(32, 1, td)
+        cpu = {"value": reference_units(s, 32, n), "unit": f"factor+solve steps/s at n={n}",
+               "cores": 1, "kind": "reference",
+               "sample": (f"reference Factor() + Apply(u, true) at n=32 "
+                          f"({dofs(32)} DOFs) on 1 core took {s:.2f} s; scaled to n={n} "
+                          "linearly in DOFs (a lower bound on the reference's time)")}
+
+    value = world * 1e3 / ms_step
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": f"factor+solve steps/s at n={n}",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"hif factor + pcg(1e-10), n={n} (N={N}, {dofs(n)} DOFs), "
+                               f"face a=exp(GRF ell=1/16 sigma=1), eps={eps}, P=4, FP64",
+                   "parallelism": f"replicas x{world}", "l2_flush": "256 MB write per step",
+                   "inputs": "coefficients and rhs resident in HBM"},
+        "factor_s": float(np.mean(fac)),
+        "solve_ms": float(np.median(solve_ms)),
+        "solves_per_s": 1e3 / float(np.median(solve_ms)),
+        "pcg_iters": iters[-1],
+        "pcg_relres": rel[-1],
+        "clocks": clk,
+        "e2e": {"value": world / e2e_s, "unit": f"factor+solve steps/s at n={n}",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "pcg_iters": it_e2e, "pcg_relres": rr_e2e},
+        "roofline": roof,
+        "kernel_share": share,
+        "gpu_launches": int(sum(v["launches"] for v in kst.values()) / args.steps),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    f.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--eps", type=float, default=1e-6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

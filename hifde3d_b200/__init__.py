@@ -29,7 +29,9 @@ _lib = None
 HIF_OK, HIF_ERR_ARG, HIF_ERR_CUDA, HIF_ERR_NOMEM, HIF_ERR_SINGULAR = 0, 1, 2, 3, 4
 HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET = 5, 6, 7
 PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
-OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB = 1, 2, 3
+OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE = 1, 2, 3, 4
+KCLASS_NAMES = ["gather", "gemm", "sweep_small", "sweep_panel", "id", "gemv", "copy", "vector",
+                "qr"]
 TOP, BOTTOM, RIGHT, LEFT, FRONT, BACK = range(6)
 
 
@@ -51,6 +53,7 @@ _SIGNATURES = {
     "hif_setup_stencil": [_p, _i, _d, _dp, _dp],
     "hif_setup_stencil_device": [_p, _i, _d, _p, _p],
     "hif_setup_stencil_faces": [_p, _i, _d, _dp, _dp, _dp, _dp],
+    "hif_setup_stencil_faces_device": [_p, _i, _d, _p, _p, _p, _p],
     "hif_initialize": [_p],
     "hif_factor": [_p],
     "hif_apply": [_p, _dp, _i, _ll, _i],
@@ -68,6 +71,7 @@ _SIGNATURES = {
     "hif_set_option": [_p, _i, _ll],
     "hif_set_replay_pivots": [_p, _i, _i, _ip, _ip],
     "hif_factor_stats": [_p, _dp, _dp, _dp, _dp, _dp, _llp],
+    "hif_kernel_stats": [_p, _i, _llp, _dp, _dp, _dp],
     "hif_partition_cell": [_i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
                            _ip, _ip, _ip, _ip],
     "hif_partition_face": [_i, _i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
@@ -270,6 +274,17 @@ class HIFFactor:
         _check(lib().hif_block_pivots(self._h, level, b, _iptr(jp), _dptr(rd)))
         return jp[:n].astype(np.int64), rd[:n]
 
+    def kernel_stats(self) -> dict:
+        """Per kernel class: launches, ms, algorithmic flops and bytes (needs OPT_PROFILE)."""
+        out = {}
+        for c, name in enumerate(KCLASS_NAMES):
+            n = ctypes.c_longlong()
+            ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+            _check(lib().hif_kernel_stats(self._h, c, ctypes.byref(n), ctypes.byref(ms),
+                                          ctypes.byref(fl), ctypes.byref(by)))
+            out[name] = {"launches": n.value, "ms": ms.value, "flops": fl.value, "bytes": by.value}
+        return out
+
     def factor_stats(self) -> dict:
         vals = [ctypes.c_double() for _ in range(5)]
         nb = ctypes.c_longlong()
@@ -299,6 +314,17 @@ def SetupStencilFaces(factor: HIFFactor, N: int, h: float, ax, ay, az, V) -> Non
         if x.size != (NC + 1) ** 3:
             raise HIFError(HIF_ERR_ARG, "face arrays must be (N+2)^3")
     _check(lib().hif_setup_stencil_faces(factor._h, N, h, *[_dptr(x) for x in arrs]))
+
+
+def SetupStencilFacesDevice(factor: HIFFactor, N: int, h: float, dax: int, day: int, daz: int,
+                            dV: int) -> None:
+    """Face-coefficient operator from device pointers ((N+2)^3 float64 each, i fastest)."""
+    _check(lib().hif_setup_stencil_faces_device(factor._h, N, h, _p(dax), _p(day), _p(daz),
+                                                _p(dV)))
+
+
+def set_stream(factor: HIFFactor, stream_ptr: int) -> None:
+    _check(lib().hif_set_stream(factor._h, _p(stream_ptr)))
 
 
 def SpMV(factor: HIFFactor, x: np.ndarray, y: np.ndarray) -> None:

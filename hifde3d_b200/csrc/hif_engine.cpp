@@ -129,6 +129,7 @@ struct StepData {
 
 // One launch of the apply sweep.
 struct ApplyLaunch {
+  double bytes = 0;  // matrix bytes streamed per right-hand-side group
   int type = 0;  // 0 gemv, 1 reduce-scatter
   GemvDesc* d_desc = nullptr;
   int* d_toff = nullptr;
@@ -162,8 +163,8 @@ class Engine {
   double eps;
   long long n3;
   int L = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
+  cudaStream_t stream = nullptr;      // stream every launch goes to
+  cudaStream_t own_stream = nullptr;  // created by the handle
   double* d_band = nullptr;
   bool have_op = false, initialized = false, factored = false;
   std::vector<uint8_t> rem;
@@ -171,9 +172,72 @@ class Engine {
   bool keep_schur = false, verbose = false;
   long long budget_mb = 0;
   std::map<int, std::vector<std::vector<int>>> replay;
-  double t_total = 0, t_gather = 0, t_elim = 0, t_id = 0, t_host = 0;
+  double t_total = 0, t_gather = 0, t_elim = 0, t_id = 0, t_host = 0, t_plan = 0;
   long long peak_bytes = 0, cur_bytes = 0;
   int* d_status = nullptr;
+
+  // ---- per-kernel-class timing (HIF_OPT_PROFILE): CUDA events on the engine
+  // stream around each launch, with the launch's algorithmic flops / bytes.
+  struct KStat {
+    long long launches = 0;
+    double ms = 0, flops = 0, bytes = 0;
+  };
+  struct Pending {
+    int cls;
+    cudaEvent_t a, b;
+    double flops, bytes;
+    int nlaunch;
+  };
+  bool profile = false;
+  KStat kstat[HIF_KCLASS_COUNT];
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> ev_pool;
+
+  cudaEvent_t get_event() {
+    if (!ev_pool.empty()) {
+      cudaEvent_t e = ev_pool.back();
+      ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    HIF_CK(cudaEventCreate(&e));
+    return e;
+  }
+
+  template <class F>
+  void timed(int cls, double flops, double bytes, F&& launch, int nlaunch = 1) {
+    if (!profile) {
+      launch();
+      return;
+    }
+    Pending pd{cls, get_event(), get_event(), flops, bytes, nlaunch};
+    HIF_CK(cudaEventRecord(pd.a, stream));
+    launch();
+    HIF_CK(cudaEventRecord(pd.b, stream));
+    pending.push_back(pd);
+  }
+
+  void resolve_profile() {
+    for (Pending& pd : pending) {
+      HIF_CK(cudaEventSynchronize(pd.b));
+      float ms = 0;
+      HIF_CK(cudaEventElapsedTime(&ms, pd.a, pd.b));
+      KStat& k = kstat[pd.cls];
+      k.launches += pd.nlaunch;
+      k.ms += ms;
+      k.flops += pd.flops;
+      k.bytes += pd.bytes;
+      ev_pool.push_back(pd.a);
+      ev_pool.push_back(pd.b);
+    }
+    pending.clear();
+  }
+
+  void reset_profile() {
+    resolve_profile();
+    for (KStat& k : kstat) k = KStat{};
+  }
+
   // apply / solve workspace
   double* d_ua = nullptr;
   double* d_ub = nullptr;
@@ -188,8 +252,8 @@ class Engine {
   Engine(int N_, int P_, double eps_, int part)
       : N(N_), P(P_), NC(N_ + 1), partition(part), eps(eps_) {
     n3 = (long long)NC * NC * NC;
-    HIF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    own_stream = true;
+    HIF_CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    stream = own_stream;
     d_status = dalloc<int>(4, stream);
     HIF_CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), stream));
     d_band = dalloc<double>(7 * n3, stream);
@@ -197,15 +261,23 @@ class Engine {
   }
 
   ~Engine() {
+    sync_quiet();
+    for (Pending& pd : pending) {
+      cudaEventDestroy(pd.a);
+      cudaEventDestroy(pd.b);
+    }
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     release_factor();
     release_workspace();
     dfree(d_band, stream);
     dfree(d_status, stream);
     cudaStreamSynchronize(stream);
-    if (own_stream) cudaStreamDestroy(stream);
+    cudaStreamSynchronize(own_stream);
+    cudaStreamDestroy(own_stream);
   }
 
   void sync() { HIF_CK(cudaStreamSynchronize(stream)); }
+  void sync_quiet() { cudaStreamSynchronize(stream); }
 
   void release_workspace() {
     dfree(d_ua, stream);
@@ -294,7 +366,15 @@ class Engine {
     }
     if (!small.empty()) {
       SweepDesc* dd = tmp.add(upload(small, stream));
-      launch_sweep_small(dd, (int)small.size(), max_small, d_status, stream);
+      double fl = 0, by = 0;
+      for (const SweepDesc& d : small) {
+        const double r = d.r, sk = d.n - d.r;
+        fl += 2 * r * r * r + 2 * r * r * sk + 2 * r * sk * sk;
+        by += 8.0 * d.n * d.n + 8.0 * (r * r + r * sk + sk * sk);
+      }
+      timed(HIF_KCLASS_SWEEP_SMALL, fl, by, [&] {
+        launch_sweep_small(dd, (int)small.size(), max_small, d_status, stream);
+      });
       HIF_CK(cudaGetLastError());
     }
     if (large.empty()) return;
@@ -352,11 +432,17 @@ class Engine {
       int* dcol = step.add(upload(colt, stream));
       GemmDesc* dg = step.add(upload(gd, stream));
       int* dto = step.add(upload(toff, stream));
-      launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
-      launch_sweep_rowpanel(dd, drow, (int)rowt.size() / 4, k0, dinv, stream);
-      launch_dgemm(dg, dto, (int)gd.size(), toff.back(), stream);
-      launch_sweep_colpanel(dd, dcol, (int)colt.size() / 4, k0, dinv, stream);
-      launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
+      double gfl = 0;
+      for (const GemmDesc& g : gd) gfl += 2.0 * g.m * g.n * g.k;
+      timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+        launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
+        launch_sweep_rowpanel(dd, drow, (int)rowt.size() / 4, k0, dinv, stream);
+      }, 2);
+      timed(HIF_KCLASS_GEMM, gfl, 0, [&] { launch_dgemm(dg, dto, (int)gd.size(), toff.back(), stream); });
+      timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+        launch_sweep_colpanel(dd, dcol, (int)colt.size() / 4, k0, dinv, stream);
+        launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
+      }, 2);
       HIF_CK(cudaGetLastError());
       step.release(stream);
     }
@@ -373,19 +459,25 @@ class Engine {
     }
     CopyDesc* dcd = tmp.add(upload(cd, stream));
     int* dco = tmp.add(upload(coff, stream));
-    launch_copy(dcd, dco, (int)cd.size(), coff.back(), stream);
+    timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dcd, dco, (int)cd.size(), coff.back(), stream); });
     HIF_CK(cudaGetLastError());
   }
 
   void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
               const SourceDesc* d_srcdesc, const int* d_dof_src, BufList& tmp) {
     std::vector<int> toff(1, 0);
-    for (const GatherTarget& g : tg) toff.push_back(toff.back() + gather_tiles(g.m, g.n));
+    double by = 0;
+    for (const GatherTarget& g : tg) {
+      toff.push_back(toff.back() + gather_tiles(g.m, g.n));
+      by += 8.0 * g.m * g.n;
+    }
     if (toff.back() == 0) return;
     GatherTarget* dt = tmp.add(upload(tg, stream));
     int* dto = tmp.add(upload(toff, stream));
-    launch_gather(dt, dto, (int)tg.size(), toff.back(), d_srcdesc, d_src_owner, d_dof_src,
-                  d_band, n3, NC, stream);
+    timed(HIF_KCLASS_GATHER, 0, by, [&] {
+      launch_gather(dt, dto, (int)tg.size(), toff.back(), d_srcdesc, d_src_owner, d_dof_src,
+                    d_band, n3, NC, stream);
+    });
     HIF_CK(cudaGetLastError());
     (void)src;
   }
@@ -695,7 +787,9 @@ class Engine {
       d.n = blocks[f].global.size();
     }
     IdDesc* d_idd = tmp.add(upload(idd, stream));
-    launch_id(d_idd, nf, max_n, eps, d_status, stream);
+    double idfl = 0;
+    for (const IdDesc& d : idd) idfl += 4.0 * d.m * d.n * d.n - 4.0 / 3.0 * d.n * d.n * (double)d.n;
+    timed(HIF_KCLASS_ID, idfl, 0, [&] { launch_id(d_idd, nf, max_n, eps, d_status, stream); });
     HIF_CK(cudaGetLastError());
     std::vector<int> h_jp(isz + 1), h_keep(isz + 1);
     std::vector<double> h_rd(isz + 1);
@@ -898,14 +992,16 @@ class Engine {
       if (g.empty()) return;
       GemmDesc* d = tmp.add(upload(g, stream));
       int* to = tmp.add(upload(t, stream));
-      launch_dgemm(d, to, (int)g.size(), t.back(), stream);
+      double fl = 0;
+      for (const GemmDesc& x : g) fl += 2.0 * x.m * x.n * x.k;
+      timed(HIF_KCLASS_GEMM, fl, 0, [&] { launch_dgemm(d, to, (int)g.size(), t.back(), stream); });
       HIF_CK(cudaGetLastError());
     };
     auto run_copy = [&](std::vector<CopyDesc>& c, std::vector<int>& t) {
       if (c.empty()) return;
       CopyDesc* d = tmp.add(upload(c, stream));
       int* to = tmp.add(upload(t, stream));
-      launch_copy(d, to, (int)c.size(), t.back(), stream);
+      timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(d, to, (int)c.size(), t.back(), stream); });
       HIF_CK(cudaGetLastError());
     };
     run_gemm(g1, t1);
@@ -960,6 +1056,12 @@ class Engine {
     HIF_CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
     factored = true;
     if (st & kStatusTinyPivot) throw Error{HIF_ERR_SINGULAR, "zero or non-finite pivot"};
+    // the apply sweeps are part of the factorization's output: build them now
+    const double tp = wall();
+    ensure_workspace(1);
+    sync();
+    t_plan = wall() - tp;
+    if (profile) resolve_profile();
   }
 
   // ---- Apply (src/Factor.cpp:992-1081) ------------------------------------
@@ -969,6 +1071,7 @@ class Engine {
                 bool out_red, double alpha, int mode, int in_vec, int out_vec) {
     std::vector<GemvDesc> dd;
     std::vector<int> toff(1, 0);
+    double mbytes = 0;
     for (size_t b = 0; b < st.blocks.size(); ++b) {
       const BlockInfo& bi = st.blocks[b];
       const int r = bi.r(), s = bi.s();
@@ -996,12 +1099,14 @@ class Engine {
       g.alpha = alpha;
       g.mode = mode;
       g.contrib = (mode == 1) ? d_contrib + st.o_skel[b] : nullptr;
+      mbytes += 8.0 * g.m * g.n;
       dd.push_back(g);
       toff.push_back(toff.back() + gemv_tiles(g.m, g.n, trans));
     }
     if (dd.empty()) return;
     ApplyLaunch l;
     l.type = 0;
+    l.bytes = mbytes;
     l.nd = dd.size();
     l.tiles = toff.back();
     l.in_vec = in_vec;
@@ -1012,28 +1117,32 @@ class Engine {
   }
 
   void add_reduce(ApplyPlan& plan, const StepData& st, double alpha, int vec) {
-    // every skeleton DOF of the level: its contribution slots in block order
-    std::map<int, std::vector<int>> by_dof;
-    std::vector<int> order;
+    // every skeleton DOF of the level with its contribution slots, in block order
+    std::vector<int> head(n3, -1), dof, cnt;
     for (size_t b = 0; b < st.blocks.size(); ++b) {
       const BlockInfo& bi = st.blocks[b];
       if (bi.r() == 0) continue;
       for (int t = 0; t < bi.s(); ++t) {
         const int p = bi.global[bi.skel_pos[t]];
-        auto it = by_dof.find(p);
-        if (it == by_dof.end()) {
-          order.push_back(p);
-          by_dof[p] = {};
+        if (head[p] < 0) {
+          head[p] = (int)dof.size();
+          dof.push_back(p);
+          cnt.push_back(0);
         }
-        by_dof[p].push_back((int)(st.o_skel[b] + t));
+        ++cnt[head[p]];
       }
     }
-    if (order.empty()) return;
-    std::vector<int> dof, off(1, 0), slot;
-    for (int p : order) {
-      dof.push_back(p);
-      for (int s : by_dof[p]) slot.push_back(s);
-      off.push_back((int)slot.size());
+    if (dof.empty()) return;
+    std::vector<int> off(dof.size() + 1, 0);
+    for (size_t d = 0; d < dof.size(); ++d) off[d + 1] = off[d] + cnt[d];
+    std::vector<int> slot(off.back()), cur(off.begin(), off.end() - 1);
+    for (size_t b = 0; b < st.blocks.size(); ++b) {
+      const BlockInfo& bi = st.blocks[b];
+      if (bi.r() == 0) continue;
+      for (int t = 0; t < bi.s(); ++t) {
+        const int p = bi.global[bi.skel_pos[t]];
+        slot[cur[head[p]]++] = (int)(st.o_skel[b] + t);
+      }
     }
     ApplyLaunch l;
     l.type = 1;
@@ -1130,11 +1239,16 @@ class Engine {
     double* vec[2] = {d_ua, d_ub};
     for (ApplyLaunch& l : plan.launches) {
       if (l.type == 0) {
-        launch_gemv(l.d_desc, l.d_toff, l.nd, l.tiles, vec[l.in_vec], vec[l.out_vec], nrhs, n3,
-                    contrib_ld, stream);
+        const double by = l.bytes * ((nrhs + 3) / 4);
+        timed(HIF_KCLASS_GEMV, 2.0 * l.bytes / 8 * nrhs, by, [&] {
+          launch_gemv(l.d_desc, l.d_toff, l.nd, l.tiles, vec[l.in_vec], vec[l.out_vec], nrhs, n3,
+                      contrib_ld, stream);
+        });
       } else {
-        launch_reduce_scatter(l.d_dof, l.d_off, l.d_slot, d_contrib, l.ndof, contrib_ld,
-                              l.alpha, vec[l.out_vec], nrhs, n3, stream);
+        timed(HIF_KCLASS_VECTOR, 0, 0, [&] {
+          launch_reduce_scatter(l.d_dof, l.d_off, l.d_slot, d_contrib, l.ndof, contrib_ld,
+                                l.alpha, vec[l.out_vec], nrhs, n3, stream);
+        });
       }
       HIF_CK(cudaGetLastError());
     }
@@ -1147,7 +1261,8 @@ class Engine {
     for (int c = 0; c < nrhs; ++c)
       HIF_CK(cudaMemcpyAsync(d_ua + c * n3, du + c * ldu, n3 * 8, cudaMemcpyDeviceToDevice,
                              stream));
-    launch_zero_boundary(d_ua, NC, nrhs, n3, stream);
+    timed(HIF_KCLASS_VECTOR, 0, 8.0 * n3 * nrhs,
+          [&] { launch_zero_boundary(d_ua, NC, nrhs, n3, stream); });
     HIF_CK(cudaMemsetAsync(d_ub, 0, n3 * nrhs * 8, stream));
     run_plan(inverse ? plan_inv : plan_fwd, nrhs);
     for (int c = 0; c < nrhs; ++c)
@@ -1179,9 +1294,10 @@ class Engine {
     double* part = sc + 8 * nrhs;
     for (int c = 0; c < nrhs; ++c)
       HIF_CK(cudaMemcpyAsync(r + c * n3, db + c * ld, n3 * 8, cudaMemcpyDeviceToDevice, stream));
-    launch_zero_boundary(r, NC, nrhs, n3, stream);
+    const double vb = 8.0 * n3 * nrhs;
+    timed(HIF_KCLASS_VECTOR, 0, vb, [&] { launch_zero_boundary(r, NC, nrhs, n3, stream); });
     HIF_CK(cudaMemsetAsync(x, 0, n3 * nrhs * 8, stream));
-    launch_dot(r, r, n3, nrhs, n3, part, bb, stream);
+    timed(HIF_KCLASS_VECTOR, 0, vb, [&] { launch_dot(r, r, n3, nrhs, n3, part, bb, stream); }, 2);
     // z = M r
     auto precond = [&](double* in, double* outv) {
       if (outv != in)
@@ -1190,7 +1306,7 @@ class Engine {
     };
     precond(r, z);
     HIF_CK(cudaMemcpyAsync(p, z, n3 * nrhs * 8, cudaMemcpyDeviceToDevice, stream));
-    launch_dot(r, z, n3, nrhs, n3, part, rz, stream);
+    timed(HIF_KCLASS_VECTOR, 0, 2 * vb, [&] { launch_dot(r, z, n3, nrhs, n3, part, rz, stream); }, 2);
     std::vector<double> h_bb(nrhs), h_rr(nrhs);
     HIF_CK(cudaMemcpyAsync(h_bb.data(), bb, nrhs * 8, cudaMemcpyDeviceToHost, stream));
     sync();
@@ -1204,10 +1320,12 @@ class Engine {
       bool all = true;
       for (int c = 0; c < nrhs; ++c) all = all && done[c];
       if (all) break;
-      launch_stencil_apply(d_band, NC, p, q, nrhs, n3, 0, stream);
-      launch_dot(p, q, n3, nrhs, n3, part, pq, stream);
-      launch_pcg_update_xr(x, r, p, q, rz, pq, n3, nrhs, n3, stream);
-      launch_dot(r, r, n3, nrhs, n3, part, rr, stream);
+      timed(HIF_KCLASS_VECTOR, 13.0 * n3 * nrhs, 9 * vb,
+            [&] { launch_stencil_apply(d_band, NC, p, q, nrhs, n3, 0, stream); });
+      timed(HIF_KCLASS_VECTOR, 0, 2 * vb, [&] { launch_dot(p, q, n3, nrhs, n3, part, pq, stream); }, 2);
+      timed(HIF_KCLASS_VECTOR, 0, 6 * vb,
+            [&] { launch_pcg_update_xr(x, r, p, q, rz, pq, n3, nrhs, n3, stream); });
+      timed(HIF_KCLASS_VECTOR, 0, vb, [&] { launch_dot(r, r, n3, nrhs, n3, part, rr, stream); }, 2);
       HIF_CK(cudaMemcpyAsync(h_rr.data(), rr, nrhs * 8, cudaMemcpyDeviceToHost, stream));
       sync();
       bool all_now = true;
@@ -1220,8 +1338,10 @@ class Engine {
       }
       if (all_now) break;
       precond(r, z);
-      launch_dot(r, z, n3, nrhs, n3, part, rz_new, stream);
-      launch_pcg_update_p(p, z, rz_new, rz, n3, nrhs, n3, stream);
+      timed(HIF_KCLASS_VECTOR, 0, 2 * vb,
+            [&] { launch_dot(r, z, n3, nrhs, n3, part, rz_new, stream); }, 2);
+      timed(HIF_KCLASS_VECTOR, 0, 3 * vb,
+            [&] { launch_pcg_update_p(p, z, rz_new, rz, n3, nrhs, n3, stream); });
       HIF_CK(cudaMemcpyAsync(rz, rz_new, nrhs * 8, cudaMemcpyDeviceToDevice, stream));
       HIF_CK(cudaGetLastError());
     }
@@ -1303,8 +1423,7 @@ int hif_set_stream(hif_handle h, void* stream) {
   if (!h) return HIF_ERR_ARG;
   return guarded([&] {
     h->e->sync();
-    if (stream == nullptr) return;
-    h->e->stream = static_cast<cudaStream_t>(stream);
+    h->e->stream = stream ? static_cast<cudaStream_t>(stream) : h->e->own_stream;
   });
 }
 
@@ -1348,6 +1467,19 @@ int hif_setup_stencil_faces(hif_handle h, int N, double hstep, const double* ax,
     hif::dfree(dv, e.stream);
     e.have_op = true;
     e.sync();
+  });
+}
+
+int hif_setup_stencil_faces_device(hif_handle h, int N, double hstep, const double* dax,
+                                   const double* day, const double* daz, const double* dV) {
+  if (!h || !dax || !day || !daz || !dV || N != h->e->N || !(hstep > 0)) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Engine& e = *h->e;
+    e.timed(HIF_KCLASS_VECTOR, 0, 11.0 * 8 * e.n3, [&] {
+      hif::launch_setup_faces(dax, day, daz, dV, N, hstep, e.d_band, e.stream);
+    });
+    HIF_CK(cudaGetLastError());
+    e.have_op = true;
   });
 }
 
@@ -1526,6 +1658,11 @@ int hif_set_option(hif_handle h, int option, long long value) {
     case HIF_OPT_KEEP_SCHUR: h->e->keep_schur = value != 0; return HIF_OK;
     case HIF_OPT_VERBOSE: h->e->verbose = value != 0; return HIF_OK;
     case HIF_OPT_MEM_BUDGET_MB: h->e->budget_mb = value; return HIF_OK;
+    case HIF_OPT_PROFILE:
+      return guarded([&] {
+        h->e->reset_profile();
+        h->e->profile = value != 0;
+      });
   }
   return HIF_ERR_ARG;
 }
@@ -1548,13 +1685,27 @@ int hif_factor_stats(hif_handle h, double* total_s, double* gather_s, double* el
                      double* id_s, double* host_s, long long* device_bytes) {
   if (!h) return HIF_ERR_ARG;
   hif::Engine& e = *h->e;
-  if (total_s) *total_s = e.t_total;
+  if (total_s) *total_s = e.t_total + e.t_plan;
   if (gather_s) *gather_s = e.t_gather;
   if (elim_s) *elim_s = e.t_elim;
   if (id_s) *id_s = e.t_id;
   if (host_s) *host_s = e.t_host;
   if (device_bytes) *device_bytes = e.peak_bytes;
   return HIF_OK;
+}
+
+int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, double* flops,
+                     double* bytes) {
+  if (!h || kclass < 0 || kclass >= HIF_KCLASS_COUNT) return HIF_ERR_ARG;
+  return guarded([&] {
+    h->e->sync();
+    h->e->resolve_profile();
+    const hif::Engine::KStat& k = h->e->kstat[kclass];
+    if (launches) *launches = k.launches;
+    if (ms) *ms = k.ms;
+    if (flops) *flops = k.flops;
+    if (bytes) *bytes = k.bytes;
+  });
 }
 
 int hif_partition_cell(int N, int P, int level, int ci, int cj, int ck, int reserved,

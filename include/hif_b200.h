@@ -59,6 +59,8 @@ int hif_setup_stencil_device(hif_handle h, int N, double hstep, const double* dA
  * ax(i,j,k) couples (i,j,k)-(i+1,j,k); ay, az likewise; all (N+2)^3, i fastest. */
 int hif_setup_stencil_faces(hif_handle h, int N, double hstep, const double* ax,
                             const double* ay, const double* az, const double* V);
+int hif_setup_stencil_faces_device(hif_handle h, int N, double hstep, const double* dax,
+                                   const double* day, const double* daz, const double* dV);
 
 /* HIFFactor::Initialize -- src/Factor.cpp:6-39. */
 int hif_initialize(hif_handle h);
@@ -107,7 +109,8 @@ int hif_block_pivots(hif_handle h, int level, int b, int* jpvt, double* rdiag);
 enum hif_option {
   HIF_OPT_KEEP_SCHUR = 1,    /* keep every Schur complement for hif_block_matrix(which=4) */
   HIF_OPT_VERBOSE = 2,       /* per-phase timings on stderr */
-  HIF_OPT_MEM_BUDGET_MB = 3  /* refuse factorizations whose device memory exceeds this */
+  HIF_OPT_MEM_BUDGET_MB = 3, /* refuse factorizations whose device memory exceeds this */
+  HIF_OPT_PROFILE = 4        /* time every launch with CUDA events (resets the counters) */
 };
 int hif_set_option(hif_handle h, int option, long long value);
 
@@ -133,6 +136,24 @@ int hif_partition_cell(int N, int P, int level, int ci, int cj, int ck, int rese
                        int* skeleton_inds, int* counts);
 int hif_partition_face(int N, int P, int level, int ci, int cj, int ck, int face,
                        int reserved, const unsigned char* mask, int* rows, int* cols);
+
+/* Kernel classes of hif_kernel_stats. */
+enum hif_kernel_class {
+  HIF_KCLASS_GATHER = 0,      /* block assembly from the stencil + Schur complement blocks */
+  HIF_KCLASS_GEMM = 1,        /* batched FP64 GEMM (elimination updates, ID rotations) */
+  HIF_KCLASS_SWEEP_SMALL = 2, /* whole-block elimination in shared memory */
+  HIF_KCLASS_SWEEP_PANEL = 3, /* pivot-block inverse and panels of the blocked elimination */
+  HIF_KCLASS_ID = 4,          /* pivoted-QR interpolative decomposition */
+  HIF_KCLASS_GEMV = 5,        /* apply sweeps */
+  HIF_KCLASS_COPY = 6,        /* compact copies of factor blocks */
+  HIF_KCLASS_VECTOR = 7,      /* reductions / vector updates of the apply */
+  HIF_KCLASS_QR = 8,          /* blocked Householder row compression of face blocks */
+  HIF_KCLASS_COUNT = 9
+};
+/* Accumulated launches, milliseconds (CUDA events on the handle's stream), algorithmic
+ * flops and bytes of one kernel class since HIF_OPT_PROFILE was last set. */
+int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, double* flops,
+                     double* bytes);
 
 /* Message of the last error on this thread. */
 const char* hif_last_error(void);
