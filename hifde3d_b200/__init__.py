@@ -72,6 +72,11 @@ _SIGNATURES = {
     "hif_set_replay_pivots": [_p, _i, _i, _ip, _ip],
     "hif_factor_stats": [_p, _dp, _dp, _dp, _dp, _dp, _llp],
     "hif_kernel_stats": [_p, _i, _llp, _dp, _dp, _dp],
+    "hif_schur": [_dp, _i, _ll, _ip, _i, _ip, _i, _dp, _dp, _dp, _dp],
+    "hif_schur_device": [_p, _i, _i, _p, _p, _p],
+    "hif_interp_decomp": [_dp, _i, _i, _ll, _d, _dp, _ip, _ip, _ip],
+    "hif_pivoted_qr": [_dp, _i, _i, _ll, _ip],
+    "hif_triangular_solve": [_dp, _i, _ll, _dp, _i, _ll],
     "hif_partition_cell": [_i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
                            _ip, _ip, _ip, _ip],
     "hif_partition_face": [_i, _i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
@@ -335,6 +340,55 @@ def SpMV(factor: HIFFactor, x: np.ndarray, y: np.ndarray) -> None:
 def RelativeErrorNorm2(x: np.ndarray, y: np.ndarray) -> float:
     """``RelativeErrorNorm2`` (src/Factor.cpp:1083-1097): ||x - y|| / ||x||."""
     return float(np.sqrt(np.sum(np.abs(x - y) ** 2) / np.sum(np.abs(x) ** 2)))
+
+
+def Schur(matrix: np.ndarray, red, skel):
+    """``Schur`` (include/Schur.hpp:72-100) on the GPU: returns (A22, A22inv, X, S)."""
+    M = np.asfortranarray(matrix, dtype=np.float64)
+    r = np.ascontiguousarray(red, np.int32)
+    s = np.ascontiguousarray(skel, np.int32)
+    nr, ns = r.size, s.size
+    out = [np.zeros((max(nr, 1), max(nr, 1)), order="F"), np.zeros((max(nr, 1), max(nr, 1)), order="F"),
+           np.zeros((max(nr, 1), max(ns, 1)), order="F"), np.zeros((max(ns, 1), max(ns, 1)), order="F")]
+    _check(lib().hif_schur(_dptr(M), M.shape[0], M.shape[0], _iptr(r), nr, _iptr(s), ns,
+                           *[_dptr(o) for o in out]))
+    A22, inv, X, S = out
+    return A22[:nr, :nr], inv[:nr, :nr], X[:nr, :ns], S[:ns, :ns]
+
+
+def InterpDecomp(M: np.ndarray, eps: float):
+    """``InterpDecomp`` (src/InterpDecomp.cpp:86-138) on the GPU.
+
+    Returns (W, skeleton_cols, redundant_cols); M is not modified (the C entry point
+    overwrites its argument as the reference does; this wrapper passes a copy)."""
+    A = np.array(M, dtype=np.float64, order="F", copy=True)
+    m, n = A.shape
+    W = np.zeros(n * n // 4 + n + 1)
+    sk = np.zeros(n, np.int32)
+    rd = np.zeros(n, np.int32)
+    k = ctypes.c_int()
+    _check(lib().hif_interp_decomp(_dptr(A), m, n, m, float(eps), _dptr(W), _iptr(sk), _iptr(rd),
+                                   ctypes.byref(k)))
+    k = k.value
+    return (W[:k * (n - k)].reshape(n - k, k).T.copy(), sk[:k].astype(np.int64),
+            rd[:n - k].astype(np.int64))
+
+
+def PivotedQR(A: np.ndarray):
+    """``PivotedQRWrapper`` (src/InterpDecomp.cpp:198-211): returns (R-array, jpvt)."""
+    X = np.array(A, dtype=np.float64, order="F", copy=True)
+    jp = np.zeros(X.shape[1], np.int32)
+    _check(lib().hif_pivoted_qr(_dptr(X), X.shape[0], X.shape[1], X.shape[0], _iptr(jp)))
+    return X, jp.astype(np.int64)
+
+
+def TriangularSolve(R: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """``TriangularSolveWrapper`` (src/InterpDecomp.cpp:213-231): returns R^{-1} B."""
+    Rf = np.asfortranarray(R, dtype=np.float64)
+    Bf = np.array(B, dtype=np.float64, order="F", copy=True)
+    k, nb = Bf.shape
+    _check(lib().hif_triangular_solve(_dptr(Rf), k, Rf.shape[0], _dptr(Bf), nb, k))
+    return Bf
 
 
 def partition_cell(N: int, P: int, level: int, cell, mask: np.ndarray):

@@ -157,6 +157,125 @@ struct Sources {
   BufList bufs;                // device memory holding the blocks
 };
 
+// Dense elimination of a batch of blocks: descs[b].B holds [A22 A21; A12 A11]
+// (ld n); on return the compact A22^{-1}, X are written and B's trailing block
+// holds A11 - A12 X. Blocks up to kSmallSweepN are eliminated whole in shared
+// memory; larger ones by 64-wide pivot blocks with batched GEMM updates.
+// `timed(kernel class, flops, bytes, launch, launches)` wraps every launch.
+template <class Timed>
+void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t stream,
+                int* d_status, Timed&& timed) {
+  std::vector<SweepDesc> small, large;
+  int max_small = 0;
+  for (const SweepDesc& d : descs) {
+    if (d.r <= 0) continue;
+    if (d.n <= kSmallSweepN) {
+      small.push_back(d);
+      max_small = std::max(max_small, d.n);
+    } else {
+      large.push_back(d);
+    }
+  }
+  if (!small.empty()) {
+    SweepDesc* dd = tmp.add(upload(small, stream));
+    double fl = 0, by = 0;
+    for (const SweepDesc& d : small) {
+      const double r = d.r, sk = d.n - d.r;
+      fl += 2 * r * r * r + 2 * r * r * sk + 2 * r * sk * sk;
+      by += 8.0 * d.n * d.n + 8.0 * (r * r + r * sk + sk * sk);
+    }
+    timed(HIF_KCLASS_SWEEP_SMALL, fl, by, [&] {
+      launch_sweep_small(dd, (int)small.size(), max_small, d_status, stream);
+    });
+    HIF_CK(cudaGetLastError());
+  }
+  if (large.empty()) return;
+  const int nl = (int)large.size();
+  SweepDesc* dd = tmp.add(upload(large, stream));
+  double* dinv = tmp.add(dalloc<double>((size_t)nl * kSweepNB * kSweepNB, stream));
+  int maxr = 0;
+  for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
+  for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
+    std::vector<int> active;
+    std::vector<int> rowt, colt, toff(1, 0);
+    std::vector<GemmDesc> gd;
+    for (int b = 0; b < nl; ++b) {
+      const SweepDesc& d = large[b];
+      if (d.r <= k0) continue;
+      active.push_back(b);
+      const int k1 = std::min(d.r, k0 + kSweepNB);
+      auto tiles = [&](std::vector<int>& out, int lo, int hi) {
+        for (int x = lo; x < hi; x += kSweepNB) {
+          out.push_back(b);
+          out.push_back(x);
+          out.push_back(std::min(hi, x + kSweepNB));
+          out.push_back(0);
+        }
+      };
+      tiles(rowt, 0, k0);
+      tiles(rowt, k1, d.n);
+      tiles(colt, 0, k0);
+      tiles(colt, k1, d.r);
+      const int nbk = k1 - k0;
+      auto gemm = [&](int r0, int r1, int c0, int c1) {
+        if (r1 <= r0 || c1 <= c0) return;
+        GemmDesc g{};
+        g.C = d.B + r0 + (long long)c0 * d.n;
+        g.A = d.B + r0 + (long long)k0 * d.n;
+        g.B = d.B + k0 + (long long)c0 * d.n;
+        g.ldc = g.lda = g.ldb = d.n;
+        g.m = r1 - r0;
+        g.n = c1 - c0;
+        g.k = nbk;
+        g.alpha = -1.0;
+        g.beta = 1.0;
+        gd.push_back(g);
+        toff.push_back(toff.back() + dgemm_tiles(g.m, g.n));
+      };
+      gemm(0, k0, 0, k0);
+      gemm(0, k0, k1, d.n);
+      gemm(k1, d.r, 0, k0);
+      gemm(k1, d.r, k1, d.n);
+      gemm(d.r, d.n, k1, d.n);
+    }
+    BufList step;
+    int* dact = step.add(upload(active, stream));
+    int* drow = step.add(upload(rowt, stream));
+    int* dcol = step.add(upload(colt, stream));
+    GemmDesc* dg = step.add(upload(gd, stream));
+    int* dto = step.add(upload(toff, stream));
+    double gfl = 0;
+    for (const GemmDesc& g : gd) gfl += 2.0 * g.m * g.n * g.k;
+    timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+      launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
+      launch_sweep_rowpanel(dd, drow, (int)rowt.size() / 4, k0, dinv, stream);
+    }, 2);
+    timed(HIF_KCLASS_GEMM, gfl, 0, [&] { launch_dgemm(dg, dto, (int)gd.size(), toff.back(), stream); });
+    timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+      launch_sweep_colpanel(dd, dcol, (int)colt.size() / 4, k0, dinv, stream);
+      launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
+    }, 2);
+    HIF_CK(cudaGetLastError());
+    step.release(stream);
+  }
+  // compact copies of A22^{-1} and X
+  std::vector<CopyDesc> cd;
+  std::vector<int> coff(1, 0);
+  for (const SweepDesc& d : large) {
+    CopyDesc a{d.B, d.a22inv, d.n, d.r, d.r, d.r};
+    cd.push_back(a);
+    coff.push_back(coff.back() + copy_tiles(d.r, d.r));
+    CopyDesc x{d.B + (long long)d.r * d.n, d.X, d.n, d.r, d.r, d.n - d.r};
+    cd.push_back(x);
+    coff.push_back(coff.back() + copy_tiles(d.r, d.n - d.r));
+  }
+  CopyDesc* dcd = tmp.add(upload(cd, stream));
+  int* dco = tmp.add(upload(coff, stream));
+  timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dcd, dco, (int)cd.size(), coff.back(), stream); });
+  HIF_CK(cudaGetLastError());
+}
+
+
 class Engine {
  public:
   int N, P, NC, partition;
@@ -353,114 +472,8 @@ class Engine {
   // descs[b].B holds [A22 A21; A12 A11] (ld n); on return the compact
   // A22^{-1}, X are written and B's trailing block holds A11 - A12 X.
   void run_sweep(const std::vector<SweepDesc>& descs, BufList& tmp) {
-    std::vector<SweepDesc> small, large;
-    int max_small = 0;
-    for (const SweepDesc& d : descs) {
-      if (d.r <= 0) continue;
-      if (d.n <= kSmallSweepN) {
-        small.push_back(d);
-        max_small = std::max(max_small, d.n);
-      } else {
-        large.push_back(d);
-      }
-    }
-    if (!small.empty()) {
-      SweepDesc* dd = tmp.add(upload(small, stream));
-      double fl = 0, by = 0;
-      for (const SweepDesc& d : small) {
-        const double r = d.r, sk = d.n - d.r;
-        fl += 2 * r * r * r + 2 * r * r * sk + 2 * r * sk * sk;
-        by += 8.0 * d.n * d.n + 8.0 * (r * r + r * sk + sk * sk);
-      }
-      timed(HIF_KCLASS_SWEEP_SMALL, fl, by, [&] {
-        launch_sweep_small(dd, (int)small.size(), max_small, d_status, stream);
-      });
-      HIF_CK(cudaGetLastError());
-    }
-    if (large.empty()) return;
-    const int nl = (int)large.size();
-    SweepDesc* dd = tmp.add(upload(large, stream));
-    double* dinv = tmp.add(dalloc<double>((size_t)nl * kSweepNB * kSweepNB, stream));
-    int maxr = 0;
-    for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
-    for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
-      std::vector<int> active;
-      std::vector<int> rowt, colt, toff(1, 0);
-      std::vector<GemmDesc> gd;
-      for (int b = 0; b < nl; ++b) {
-        const SweepDesc& d = large[b];
-        if (d.r <= k0) continue;
-        active.push_back(b);
-        const int k1 = std::min(d.r, k0 + kSweepNB);
-        auto tiles = [&](std::vector<int>& out, int lo, int hi) {
-          for (int x = lo; x < hi; x += kSweepNB) {
-            out.push_back(b);
-            out.push_back(x);
-            out.push_back(std::min(hi, x + kSweepNB));
-            out.push_back(0);
-          }
-        };
-        tiles(rowt, 0, k0);
-        tiles(rowt, k1, d.n);
-        tiles(colt, 0, k0);
-        tiles(colt, k1, d.r);
-        const int nbk = k1 - k0;
-        auto gemm = [&](int r0, int r1, int c0, int c1) {
-          if (r1 <= r0 || c1 <= c0) return;
-          GemmDesc g{};
-          g.C = d.B + r0 + (long long)c0 * d.n;
-          g.A = d.B + r0 + (long long)k0 * d.n;
-          g.B = d.B + k0 + (long long)c0 * d.n;
-          g.ldc = g.lda = g.ldb = d.n;
-          g.m = r1 - r0;
-          g.n = c1 - c0;
-          g.k = nbk;
-          g.alpha = -1.0;
-          g.beta = 1.0;
-          gd.push_back(g);
-          toff.push_back(toff.back() + dgemm_tiles(g.m, g.n));
-        };
-        gemm(0, k0, 0, k0);
-        gemm(0, k0, k1, d.n);
-        gemm(k1, d.r, 0, k0);
-        gemm(k1, d.r, k1, d.n);
-        gemm(d.r, d.n, k1, d.n);
-      }
-      BufList step;
-      int* dact = step.add(upload(active, stream));
-      int* drow = step.add(upload(rowt, stream));
-      int* dcol = step.add(upload(colt, stream));
-      GemmDesc* dg = step.add(upload(gd, stream));
-      int* dto = step.add(upload(toff, stream));
-      double gfl = 0;
-      for (const GemmDesc& g : gd) gfl += 2.0 * g.m * g.n * g.k;
-      timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
-        launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
-        launch_sweep_rowpanel(dd, drow, (int)rowt.size() / 4, k0, dinv, stream);
-      }, 2);
-      timed(HIF_KCLASS_GEMM, gfl, 0, [&] { launch_dgemm(dg, dto, (int)gd.size(), toff.back(), stream); });
-      timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
-        launch_sweep_colpanel(dd, dcol, (int)colt.size() / 4, k0, dinv, stream);
-        launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
-      }, 2);
-      HIF_CK(cudaGetLastError());
-      step.release(stream);
-    }
-    // compact copies of A22^{-1} and X
-    std::vector<CopyDesc> cd;
-    std::vector<int> coff(1, 0);
-    for (const SweepDesc& d : large) {
-      CopyDesc a{d.B, d.a22inv, d.n, d.r, d.r, d.r};
-      cd.push_back(a);
-      coff.push_back(coff.back() + copy_tiles(d.r, d.r));
-      CopyDesc x{d.B + (long long)d.r * d.n, d.X, d.n, d.r, d.r, d.n - d.r};
-      cd.push_back(x);
-      coff.push_back(coff.back() + copy_tiles(d.r, d.n - d.r));
-    }
-    CopyDesc* dcd = tmp.add(upload(cd, stream));
-    int* dco = tmp.add(upload(coff, stream));
-    timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dcd, dco, (int)cd.size(), coff.back(), stream); });
-    HIF_CK(cudaGetLastError());
+    sweep_blocks(descs, tmp, stream, d_status,
+                 [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); });
   }
 
   void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
@@ -1692,6 +1705,210 @@ int hif_factor_stats(hif_handle h, double* total_s, double* gather_s, double* el
   if (host_s) *host_s = e.t_host;
   if (device_bytes) *device_bytes = e.peak_bytes;
   return HIF_OK;
+}
+
+// ---- the reference's free functions -------------------------------------------
+namespace {
+
+struct FreeCtx {
+  cudaStream_t stream = cudaStreamPerThread;
+  int* d_status = nullptr;
+  hif::BufList bufs;
+  FreeCtx() {
+    d_status = bufs.add(hif::dalloc<int>(4, stream));
+    HIF_CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), stream));
+  }
+  ~FreeCtx() {
+    bufs.release(stream);
+    cudaStreamSynchronize(stream);
+  }
+  int status() {
+    int st = 0;
+    HIF_CK(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    HIF_CK(cudaStreamSynchronize(stream));
+    return st;
+  }
+};
+
+int check_device() {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    hif::g_last_error = "no CUDA device";
+    return HIF_ERR_NODEVICE;
+  }
+  return HIF_OK;
+}
+
+// Eliminate the redundant DOFs of one device block given in [red | skel] order:
+// writes A22^{-1} (r x r), X (r x s) and S = -A12 X (s x s), all ld = rows.
+void schur_on_device(FreeCtx& c, const double* dB, int n, int r, double* dA22inv, double* dX,
+                     double* dS) {
+  const int s = n - r;
+  double* W = c.bufs.add(hif::dalloc<double>((size_t)n * n, c.stream));
+  HIF_CK(cudaMemcpyAsync(W, dB, (size_t)n * n * 8, cudaMemcpyDeviceToDevice, c.stream));
+  if (s > 0) {  // S = -A12 X: eliminate with the skeleton block zeroed
+    HIF_CK(cudaMemset2DAsync(W + r + (long long)r * n, (size_t)n * 8, 0, (size_t)s * 8, s, c.stream));
+  }
+  std::vector<hif::SweepDesc> sd(1);
+  sd[0].B = W;
+  sd[0].a22inv = dA22inv;
+  sd[0].X = dX;
+  sd[0].n = n;
+  sd[0].r = r;
+  hif::sweep_blocks(sd, c.bufs, c.stream, c.d_status,
+                    [&](int, double, double, auto&& f, int = 1) { f(); });
+  HIF_CK(cudaGetLastError());
+  if (s > 0)
+    HIF_CK(cudaMemcpy2DAsync(dS, (size_t)s * 8, W + r + (long long)r * n, (size_t)n * 8,
+                             (size_t)s * 8, s, cudaMemcpyDeviceToDevice, c.stream));
+}
+
+}  // namespace
+
+int hif_schur_device(const double* dB, int n, int r, double* dA22inv, double* dX, double* dS) {
+  if (!dB || n < 0 || r < 0 || r > n || (r > 0 && (!dA22inv || (r < n && !dX))) ||
+      (r < n && !dS))
+    return HIF_ERR_ARG;
+  if (int e = check_device()) return e;
+  return guarded([&] {
+    FreeCtx c;
+    if (r == 0) {
+      if (n > 0) HIF_CK(cudaMemsetAsync(dS, 0, (size_t)n * n * 8, c.stream));
+    } else {
+      schur_on_device(c, dB, n, r, dA22inv, dX, dS);
+    }
+    if (c.status() & hif::kStatusTinyPivot) throw hif::Error{HIF_ERR_SINGULAR, "zero pivot"};
+  });
+}
+
+int hif_schur(const double* matrix, int m, long long ld, const int* red, int nr, const int* skel,
+              int ns, double* A22, double* A22inv, double* X, double* S) {
+  if (!matrix || m < 0 || ld < m || nr < 0 || ns < 0 || nr + ns > m || (nr && !red) ||
+      (ns && !skel))
+    return HIF_ERR_ARG;
+  if (int e = check_device()) return e;
+  return guarded([&] {
+    const int n = nr + ns;
+    std::vector<int> ord(red, red + nr);
+    ord.insert(ord.end(), skel, skel + ns);
+    for (int p : ord)
+      if (p < 0 || p >= m) throw hif::Error{HIF_ERR_ARG, "index out of range"};
+    std::vector<double> B((size_t)n * n);
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) B[i + (size_t)j * n] = matrix[ord[i] + (long long)ord[j] * ld];
+    if (A22)
+      for (int j = 0; j < nr; ++j)
+        for (int i = 0; i < nr; ++i) A22[i + (size_t)j * nr] = B[i + (size_t)j * n];
+    FreeCtx c;
+    double* dB = c.bufs.add(hif::upload(B, c.stream));
+    double* dInv = c.bufs.add(hif::dalloc<double>((size_t)nr * nr, c.stream));
+    double* dX = c.bufs.add(hif::dalloc<double>((size_t)nr * ns, c.stream));
+    double* dS = c.bufs.add(hif::dalloc<double>((size_t)ns * ns, c.stream));
+    if (nr == 0) {
+      HIF_CK(cudaMemsetAsync(dS, 0, (size_t)ns * ns * 8, c.stream));
+    } else {
+      schur_on_device(c, dB, n, nr, dInv, dX, dS);
+    }
+    if (A22inv) HIF_CK(cudaMemcpyAsync(A22inv, dInv, (size_t)nr * nr * 8, cudaMemcpyDeviceToHost, c.stream));
+    if (X) HIF_CK(cudaMemcpyAsync(X, dX, (size_t)nr * ns * 8, cudaMemcpyDeviceToHost, c.stream));
+    if (S) HIF_CK(cudaMemcpyAsync(S, dS, (size_t)ns * ns * 8, cudaMemcpyDeviceToHost, c.stream));
+    if (c.status() & hif::kStatusTinyPivot) throw hif::Error{HIF_ERR_SINGULAR, "zero pivot"};
+  });
+}
+
+namespace {
+
+// Pivoted QR + rank test + W of one host matrix on the device (the ID kernel).
+// M is overwritten with the factorization (R on and above the diagonal).
+void id_host(double* M, int m, int n, long long ldm, double eps, std::vector<int>& jpvt,
+             std::vector<int>& keep, int& k, double* W) {
+  FreeCtx c;
+  double* dM = c.bufs.add(hif::dalloc<double>((size_t)m * n, c.stream));
+  HIF_CK(cudaMemcpy2DAsync(dM, (size_t)m * 8, M, (size_t)ldm * 8, (size_t)m * 8, n,
+                           cudaMemcpyHostToDevice, c.stream));
+  int* dint = c.bufs.add(hif::dalloc<int>(2 * (size_t)n + 1, c.stream));
+  double* drd = c.bufs.add(hif::dalloc<double>(n, c.stream));
+  double* dW = c.bufs.add(hif::dalloc<double>((size_t)n * n / 4 + n + 1, c.stream));
+  std::vector<hif::IdDesc> idd(1);
+  idd[0].M = dM;
+  idd[0].order = nullptr;
+  idd[0].jpvt = dint;
+  idd[0].keep = dint + n;
+  idd[0].rank = dint + 2 * n;
+  idd[0].rdiag = drd;
+  idd[0].W = dW;
+  idd[0].m = m;
+  idd[0].n = n;
+  hif::IdDesc* d_idd = c.bufs.add(hif::upload(idd, c.stream));
+  hif::launch_id(d_idd, 1, n, eps, c.d_status, c.stream);
+  HIF_CK(cudaGetLastError());
+  std::vector<int> hi(2 * n + 1);
+  HIF_CK(cudaMemcpyAsync(hi.data(), dint, (2 * (size_t)n + 1) * sizeof(int),
+                         cudaMemcpyDeviceToHost, c.stream));
+  HIF_CK(cudaMemcpy2DAsync(M, (size_t)ldm * 8, dM, (size_t)m * 8, (size_t)m * 8, n,
+                           cudaMemcpyDeviceToHost, c.stream));
+  HIF_CK(cudaStreamSynchronize(c.stream));
+  jpvt.assign(hi.begin(), hi.begin() + n);
+  keep.assign(hi.begin() + n, hi.begin() + 2 * n);
+  k = hi[2 * n];
+  if (W && k > 0 && k < n)
+    HIF_CK(cudaMemcpyAsync(W, dW, (size_t)k * (n - k) * 8, cudaMemcpyDeviceToHost, c.stream));
+  HIF_CK(cudaStreamSynchronize(c.stream));
+}
+
+}  // namespace
+
+int hif_interp_decomp(double* M, int m, int n, long long ldm, double eps, double* W,
+                      int* skeleton_cols, int* redundant_cols, int* rank) {
+  if (!M || m < 1 || n < 1 || m < n || ldm < m || !(eps >= 0) || !rank) return HIF_ERR_ARG;
+  if (int e = check_device()) return e;
+  return guarded([&] {
+    std::vector<int> jp, keep;
+    int k = 0;
+    id_host(M, m, n, ldm, eps, jp, keep, k, W);
+    *rank = k;
+    int a = 0, b = 0;
+    for (int i = 0; i < n; ++i) {
+      if (keep[i]) {
+        if (skeleton_cols) skeleton_cols[a] = jp[i];
+        ++a;
+      } else {
+        if (redundant_cols) redundant_cols[b] = jp[i];
+        ++b;
+      }
+    }
+  });
+}
+
+int hif_pivoted_qr(double* A, int m, int n, long long lda, int* jpvt) {
+  if (!A || !jpvt || m < 1 || n < 1 || m < n || lda < m) return HIF_ERR_ARG;
+  if (int e = check_device()) return e;
+  return guarded([&] {
+    std::vector<int> jp, keep;
+    int k = 0;
+    id_host(A, m, n, lda, 0.0, jp, keep, k, nullptr);
+    std::copy(jp.begin(), jp.end(), jpvt);
+  });
+}
+
+int hif_triangular_solve(const double* R, int k, long long ldr, double* B, int nb, long long ldb) {
+  if (!R || !B || k < 0 || nb < 0 || ldr < k || ldb < k) return HIF_ERR_ARG;
+  if (k == 0 || nb == 0) return HIF_OK;
+  if (int e = check_device()) return e;
+  return guarded([&] {
+    FreeCtx c;
+    double* dR = c.bufs.add(hif::dalloc<double>((size_t)k * k, c.stream));
+    double* dB = c.bufs.add(hif::dalloc<double>((size_t)k * nb, c.stream));
+    HIF_CK(cudaMemcpy2DAsync(dR, (size_t)k * 8, R, (size_t)ldr * 8, (size_t)k * 8, k,
+                             cudaMemcpyHostToDevice, c.stream));
+    HIF_CK(cudaMemcpy2DAsync(dB, (size_t)k * 8, B, (size_t)ldb * 8, (size_t)k * 8, nb,
+                             cudaMemcpyHostToDevice, c.stream));
+    hif::launch_trsm_upper(dR, k, k, dB, k, nb, c.stream);
+    HIF_CK(cudaGetLastError());
+    HIF_CK(cudaMemcpy2DAsync(B, (size_t)ldb * 8, dB, (size_t)k * 8, (size_t)k * 8, nb,
+                             cudaMemcpyDeviceToHost, c.stream));
+    HIF_CK(cudaStreamSynchronize(c.stream));
+  });
 }
 
 int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, double* flops,

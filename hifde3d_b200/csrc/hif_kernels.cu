@@ -741,6 +741,24 @@ void launch_copy(const CopyDesc* d_desc, const int* d_tile_off, int nd, int tota
   k_copy<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
 }
 
+__global__ void k_trsm_upper(const double* __restrict__ R, long long ldr, int k,
+                             double* __restrict__ B, long long ldb, int nb) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nb) return;
+  double* x = B + (long long)c * ldb;
+  for (int a = k - 1; a >= 0; --a) {
+    const double xa = x[a] / R[a + (long long)a * ldr];
+    x[a] = xa;
+    for (int t = 0; t < a; ++t) x[t] = fma(-R[t + (long long)a * ldr], xa, x[t]);
+  }
+}
+
+void launch_trsm_upper(const double* R, long long ldr, int k, double* B, long long ldb, int nb,
+                       cudaStream_t s) {
+  if (nb <= 0 || k <= 0) return;
+  k_trsm_upper<<<(nb + 127) / 128, 128, 0, s>>>(R, ldr, k, B, ldb, nb);
+}
+
 // ===========================================================================
 // Apply: batched gather - GEMV - scatter over right-hand sides.
 // trans = 0: 256 output rows per CTA, one row per thread (coalesced along M's

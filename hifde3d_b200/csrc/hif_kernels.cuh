@@ -144,6 +144,12 @@ void launch_id(const IdDesc* d_desc, int nd, int max_n, double eps, int* d_statu
 
 void launch_copy(const CopyDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
                  cudaStream_t s);
+
+// Solve R X = B in place (R: k x k upper triangular, non-unit; B: k x nb), one
+// right-hand side column per thread (the reference's dtrsm('L','U','N','N') call,
+// src/InterpDecomp.cpp:213-231).
+void launch_trsm_upper(const double* R, long long ldr, int k, double* B, long long ldb, int nb,
+                       cudaStream_t s);
 int copy_tiles(int m, int n);
 
 // contrib_ld: stride between right-hand sides in the contribution buffer.

@@ -87,6 +87,30 @@ int hif_solve_pcg(hif_handle h, const double* b, double* x, int nrhs, long long 
 int hif_solve_pcg_device(hif_handle h, const double* db, double* dx, int nrhs, long long ld,
                          double tol, int maxit, int* iters, double* relres);
 
+/* ---- the reference's free functions on the hot path -----------------------------
+ * Schur(matrix, data) -- include/Schur.hpp:72-100: eliminate the redundant DOFs of a
+ * dense block. matrix: m x m (ld); red / skel: positions (redundant_inds /
+ * skeleton_inds). Outputs (any may be NULL): A22 (nr x nr), A22^{-1} (nr x nr),
+ * X = A22^{-1} A21 (nr x ns), S = -A12 X (ns x ns), column-major, ld = rows. */
+int hif_schur(const double* matrix, int m, long long ld, const int* red, int nr,
+              const int* skel, int ns, double* A22, double* A22inv, double* X, double* S);
+/* The same on device memory, block given in [redundant | skeleton] order (n x n,
+ * ld n; r redundant): writes A22^{-1}, X and S. Allocates device workspace. */
+int hif_schur_device(const double* dB, int n, int r, double* dA22inv, double* dX, double* dS);
+/* InterpDecomp(M, W, skel, red, eps) -- src/InterpDecomp.cpp:86-138: column-pivoted
+ * QR of M (m x n, m >= n; overwritten, R on and above the diagonal), skeleton =
+ * {i : |R_ii| > eps |R_00|}, W = R11^{-1} R12 on the redundant columns. W holds
+ * rank x (n - rank) (room for n*n/4 + n doubles); skeleton_cols / redundant_cols in
+ * pivot order, 0-based. */
+int hif_interp_decomp(double* M, int m, int n, long long ldm, double eps, double* W,
+                      int* skeleton_cols, int* redundant_cols, int* rank);
+/* PivotedQRWrapper(A, jpvt) -- src/InterpDecomp.cpp:198-211 (geqp3; jpvt 0-based). */
+int hif_pivoted_qr(double* A, int m, int n, long long lda, int* jpvt);
+/* TriangularSolveWrapper(R, B) -- src/InterpDecomp.cpp:213-231: B := R^{-1} B with R
+ * upper triangular, non-unit (k x k), B k x nb. */
+int hif_triangular_solve(const double* R, int k, long long ldr, double* B, int nb,
+                         long long ldb);
+
 /* ---- introspection (schur_level_data / skel_level_data, include/Factor.hpp:50-51,
  *      declared but not defined by the reference) --------------------------------- */
 int hif_num_levels(hif_handle h, int* levels);
