@@ -47,5 +47,28 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+BUILD_DIR = os.path.join(HERE, "_build")
+SHIM_DIR = os.path.join(HERE, "..", "include", "hifde3d_b200")
+
+
+def build_drivers(reference_root: str, verbose: bool = False) -> list:
+    """Compile the reference's own drivers (tests/HIFDE3D/main.cpp, darcy.cpp),
+    unchanged, against the header-only drop-in (include/hifde3d_b200/hifde3d.hpp)
+    and libhif_b200.so. Outputs go to hifde3d_b200/_build/."""
+    build()
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    out = []
+    for name in ("main", "darcy"):
+        src = os.path.join(reference_root, "tests", "HIFDE3D", name + ".cpp")
+        dst = os.path.join(BUILD_DIR, "hif_driver_" + name)
+        cmd = ["g++", "-std=c++14", "-O2", "-I", SHIM_DIR, "-I", os.path.join(HERE, "..", "include"),
+               src, "-o", dst, "-L", HERE, "-lhif_b200", "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        out.append(dst)
+    return out
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
