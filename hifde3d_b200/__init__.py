@@ -74,6 +74,7 @@ _SIGNATURES = {
     "hif_kernel_stats": [_p, _i, _llp, _dp, _dp, _dp],
     "hif_schur": [_dp, _i, _ll, _ip, _i, _ip, _i, _dp, _dp, _dp, _dp],
     "hif_schur_device": [_p, _i, _i, _p, _p, _p],
+    "hif_schur_device_noalloc": [_p, _i, _i, _p, _p, _p, _p],
     "hif_interp_decomp": [_dp, _i, _i, _ll, _d, _dp, _ip, _ip, _ip],
     "hif_pivoted_qr": [_dp, _i, _i, _ll, _ip],
     "hif_triangular_solve": [_dp, _i, _ll, _dp, _i, _ll],

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhif_b200.so")
-SOURCES = ["hif_kernels.cu", "hif_engine.cpp"]
+SOURCES = ["hif_kernels.cu", "hif_engine.cpp", "hif_noalloc.cu"]
 HEADERS = ["hif_kernels.cuh", "hif_partition.hpp", os.path.join("..", "..", "include", "hif_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -97,6 +97,19 @@ int hif_schur(const double* matrix, int m, long long ld, const int* red, int nr,
 /* The same on device memory, block given in [redundant | skeleton] order (n x n,
  * ld n; r redundant): writes A22^{-1}, X and S. Allocates device workspace. */
 int hif_schur_device(const double* dB, int n, int r, double* dA22inv, double* dX, double* dS);
+/* Allocation-free variant of hif_schur_device; it has no counterpart in the reference.
+ * For callers that cannot allocate device memory: a process whose framework allocator
+ * already holds the whole GPU, or a loop that must not call into the allocator between
+ * its own kernels. All scratch lives in one fixed device array inside the library
+ * (about 2 MiB per GPU, held from library load until process exit), so blocks are limited
+ * to n <= 512 (larger ones return HIF_ERR_ARG). Inputs and outputs are the caller's
+ * device buffers; work is queued on `stream` (a cudaStream_t, NULL = legacy default)
+ * and the call waits for it to read the pivot status. Every call on a device shares the
+ * scratch array: calls whose kernels may overlap on the GPU race and must be
+ * serialised by the caller. The first call on a device looks up the array's device
+ * address with that device current. */
+int hif_schur_device_noalloc(const double* dB, int n, int r, double* dA22inv, double* dX,
+                             double* dS, void* stream);
 /* InterpDecomp(M, W, skel, red, eps) -- src/InterpDecomp.cpp:86-138: column-pivoted
  * QR of M (m x n, m >= n; overwritten, R on and above the diagonal), skeleton =
  * {i : |R_ii| > eps |R_00|}, W = R11^{-1} R12 on the redundant columns. W holds
