@@ -29,7 +29,7 @@ _lib = None
 HIF_OK, HIF_ERR_ARG, HIF_ERR_CUDA, HIF_ERR_NOMEM, HIF_ERR_SINGULAR = 0, 1, 2, 3, 4
 HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET = 5, 6, 7
 PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
-OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE = 1, 2, 3, 4
+OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE, OPT_ID_GROUP_MIN_N = 1, 2, 3, 4, 5
 KCLASS_NAMES = ["gather", "gemm", "sweep_small", "sweep_panel", "id", "gemv", "copy", "vector",
                 "qr"]
 TOP, BOTTOM, RIGHT, LEFT, FRONT, BACK = range(6)

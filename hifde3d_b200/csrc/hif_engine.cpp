@@ -157,6 +157,29 @@ struct Sources {
   BufList bufs;                // device memory holding the blocks
 };
 
+// One batched GEMM launch; 128x128 tiles when most of the work sits in
+// problems at least that large, else 64x64.
+template <class Timed>
+void gemm_batch(const std::vector<GemmDesc>& g, BufList& tmp, cudaStream_t stream, int cls,
+                Timed&& timed) {
+  if (g.empty()) return;
+  double big = 0, all = 0, fl = 0;
+  for (const GemmDesc& x : g) {
+    const double w = (double)x.m * x.n;
+    all += w;
+    if (x.m >= 96 && x.n >= 96) big += w;
+    fl += 2.0 * x.m * x.n * x.k;
+  }
+  const int tile = (big >= 0.5 * all) ? 128 : 64;
+  std::vector<int> toff(1, 0);
+  for (const GemmDesc& x : g) toff.push_back(toff.back() + dgemm_tiles(x.m, x.n, tile));
+  if (toff.back() == 0) return;
+  GemmDesc* dg = tmp.add(upload(g, stream));
+  int* dt = tmp.add(upload(toff, stream));
+  timed(cls, fl, 0.0, [&] { launch_dgemm(dg, dt, (int)g.size(), toff.back(), stream, tile); }, 1);
+  HIF_CK(cudaGetLastError());
+}
+
 // Dense elimination of a batch of blocks: descs[b].B holds [A22 A21; A12 A11]
 // (ld n); on return the compact A22^{-1}, X are written and B's trailing block
 // holds A11 - A12 X. Blocks up to kSmallSweepN are eliminated whole in shared
@@ -197,7 +220,7 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
   for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
   for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
     std::vector<int> active;
-    std::vector<int> rowt, colt, toff(1, 0);
+    std::vector<int> rowt, colt;
     std::vector<GemmDesc> gd;
     for (int b = 0; b < nl; ++b) {
       const SweepDesc& d = large[b];
@@ -205,10 +228,10 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
       active.push_back(b);
       const int k1 = std::min(d.r, k0 + kSweepNB);
       auto tiles = [&](std::vector<int>& out, int lo, int hi) {
-        for (int x = lo; x < hi; x += kSweepNB) {
+        for (int x = lo; x < hi; x += kPanelTile) {
           out.push_back(b);
           out.push_back(x);
-          out.push_back(std::min(hi, x + kSweepNB));
+          out.push_back(std::min(hi, x + kPanelTile));
           out.push_back(0);
         }
       };
@@ -230,7 +253,6 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
         g.alpha = -1.0;
         g.beta = 1.0;
         gd.push_back(g);
-        toff.push_back(toff.back() + dgemm_tiles(g.m, g.n));
       };
       gemm(0, k0, 0, k0);
       gemm(0, k0, k1, d.n);
@@ -242,15 +264,11 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
     int* dact = step.add(upload(active, stream));
     int* drow = step.add(upload(rowt, stream));
     int* dcol = step.add(upload(colt, stream));
-    GemmDesc* dg = step.add(upload(gd, stream));
-    int* dto = step.add(upload(toff, stream));
-    double gfl = 0;
-    for (const GemmDesc& g : gd) gfl += 2.0 * g.m * g.n * g.k;
     timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
       launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
       launch_sweep_rowpanel(dd, drow, (int)rowt.size() / 4, k0, dinv, stream);
     }, 2);
-    timed(HIF_KCLASS_GEMM, gfl, 0, [&] { launch_dgemm(dg, dto, (int)gd.size(), toff.back(), stream); });
+    gemm_batch(gd, step, stream, HIF_KCLASS_GEMM, timed);
     timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
       launch_sweep_colpanel(dd, dcol, (int)colt.size() / 4, k0, dinv, stream);
       launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
@@ -373,6 +391,14 @@ class Engine {
     n3 = (long long)NC * NC * NC;
     HIF_CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     stream = own_stream;
+    // keep freed pool memory reserved: factorizations reallocate the same
+    // workspace sizes, and growing the pool again costs more than the kernels
+    int dev = 0;
+    HIF_CK(cudaGetDevice(&dev));
+    cudaMemPool_t pool;
+    HIF_CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    unsigned long long keep = ~0ull;
+    HIF_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     d_status = dalloc<int>(4, stream);
     HIF_CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), stream));
     d_band = dalloc<double>(7 * n3, stream);
@@ -396,6 +422,15 @@ class Engine {
   }
 
   void sync() { HIF_CK(cudaStreamSynchronize(stream)); }
+  // verbose: print the time since the last mark (after a stream sync)
+  double mark_t = 0;
+  void mark(const char* what, int level) {
+    if (!verbose) return;
+    sync();
+    const double t = wall();
+    if (mark_t > 0) std::fprintf(stderr, "[hif]   L%d %-22s %9.3f ms\n", level, what, 1e3 * (t - mark_t));
+    mark_t = t;
+  }
   void sync_quiet() { cudaStreamSynchronize(stream); }
 
   void release_workspace() {
@@ -599,9 +634,11 @@ class Engine {
       g.owner = b;
       g.allowA = g.allowB = -1;
     }
+    mark("schur partition+upload", level);
     gather(tg, in, d_own, d_sd, d_dof, tmp);
     if (verbose) sync();
     t_gather += wall() - tg0;
+    mark("schur gather", level);
 
     // sources consumed: free them once the gather has run (stream order)
     in.bufs.release(stream);
@@ -637,6 +674,7 @@ class Engine {
     run_sweep(sd, tmp);
     if (verbose) sync();
     t_elim += wall() - te0;
+    mark("schur eliminate", level);
 
     if (keep_schur) {
       sync();
@@ -766,9 +804,11 @@ class Engine {
       g.allowA = cells.cell_src[blocks[f].cell];
       g.allowB = cells.cell_src[blocks[f].nbr];
     }
+    mark("skel partition+upload", level);
     gather(tg, cells, d_own, d_sd, d_dof, tmp);
     if (verbose) sync();
     t_gather += wall() - tg0;
+    mark("skel gather M", level);
 
     // interpolative decompositions
     double ti0 = wall();
@@ -786,23 +826,95 @@ class Engine {
       }
     }
     int* d_ord = orders.empty() ? nullptr : tmp.add(upload(orders, stream));
+    // Tall faces are first reduced to their triangular factor R0 (n x n) by an
+    // unpivoted blocked Householder QR; the pivoted QR of R0 makes the same
+    // pivot choices and yields the same R as that of M in exact arithmetic
+    // (both depend on M only through M^T M = R0^T R0).
+    std::vector<double*> idM(nf);
+    std::vector<int> idm(nf);
+    for (int f = 0; f < nf; ++f) {
+      idM[f] = dM + o_M[f];
+      idm[f] = rows_l[f].size();
+    }
+    compress_faces(blocks, rows_l, dM, o_M, idM, idm, tmp);
+    mark("skel row compression", level);
     std::vector<IdDesc> idd(nf);
     for (int f = 0; f < nf; ++f) {
       IdDesc& d = idd[f];
-      d.M = dM + o_M[f];
+      d.M = idM[f];
       d.order = d_ord ? d_ord + o_ord[f] : nullptr;
       d.jpvt = d_jp + o_i[f];
       d.rdiag = d_rd + o_i[f];
       d.keep = d_keep + o_i[f];
       d.rank = d_rank + f;
       d.W = dWs + o_W[f];
-      d.m = rows_l[f].size();
+      d.m = idm[f];
       d.n = blocks[f].global.size();
     }
-    IdDesc* d_idd = tmp.add(upload(idd, stream));
+    // small faces: one CTA each (k_id); compressed faces: grouped ID, several
+    // CTAs per face for the largest ones
+    std::vector<IdDesc> small_id;
+    std::vector<IdGroupDesc> g1, gbig;
+    int small_n = 0, g1_m = 0, g1_n = 0, big_m = 0, big_n = 0;
+    for (int f = 0; f < nf; ++f) {
+      const bool compressed = idM[f] != dM + o_M[f];
+      const int n = idd[f].n;
+      if (!compressed) {
+        small_id.push_back(idd[f]);
+        small_n = std::max(small_n, n);
+        continue;
+      }
+      IdGroupDesc gd{};
+      gd.id = idd[f];
+      (n >= kGroupMinN ? gbig : g1).push_back(gd);
+      if (n >= kGroupMinN) {
+        big_m = std::max(big_m, idd[f].m);
+        big_n = std::max(big_n, n);
+      } else {
+        g1_m = std::max(g1_m, idd[f].m);
+        g1_n = std::max(g1_n, n);
+      }
+    }
+    const int group = gbig.empty() ? 1 : std::max(1, std::min(16, 148 / (int)gbig.size()));
+    auto scratch_for = [&](std::vector<IdGroupDesc>& v, int grp) {
+      long long nd = 0, ni = 0;
+      for (const IdGroupDesc& g : v) nd += 2LL * g.id.n + grp + 2;
+      ni = 64LL * v.size();
+      double* dsc = tmp.add(dalloc<double>(nd, stream));
+      int* isc = tmp.add(dalloc<int>(ni, stream));
+      HIF_CK(cudaMemsetAsync(isc, 0, ni * sizeof(int), stream));
+      long long od = 0;
+      for (size_t q = 0; q < v.size(); ++q) {
+        v[q].norms = dsc + od;
+        v[q].cand = dsc + od + 2LL * v[q].id.n;
+        v[q].tau = dsc + od + 2LL * v[q].id.n + grp;
+        od += 2LL * v[q].id.n + grp + 2;
+        v[q].sync = isc + 64 * q;
+      }
+    };
     double idfl = 0;
     for (const IdDesc& d : idd) idfl += 4.0 * d.m * d.n * d.n - 4.0 / 3.0 * d.n * d.n * (double)d.n;
-    timed(HIF_KCLASS_ID, idfl, 0, [&] { launch_id(d_idd, nf, max_n, eps, d_status, stream); });
+    if (!small_id.empty()) {
+      IdDesc* d_idd = tmp.add(upload(small_id, stream));
+      timed(HIF_KCLASS_ID, idfl, 0,
+            [&] { launch_id(d_idd, (int)small_id.size(), small_n, eps, d_status, stream); });
+      idfl = 0;
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      std::vector<IdGroupDesc>& v = pass == 0 ? g1 : gbig;
+      if (v.empty()) continue;
+      const int grp = pass == 0 ? 1 : group;
+      scratch_for(v, grp);
+      IdGroupDesc* dg = tmp.add(upload(v, stream));
+      cudaError_t le = cudaSuccess;
+      timed(HIF_KCLASS_ID, idfl, 0, [&] {
+        le = launch_id_group(dg, (int)v.size(), grp, eps, d_status, stream,
+                             pass == 0 ? g1_m : big_m, pass == 0 ? g1_n : big_n);
+      });
+      idfl = 0;
+      if (le != cudaSuccess)
+        throw Error{HIF_ERR_CUDA, std::string("grouped ID launch: ") + cudaGetErrorString(le)};
+    }
     HIF_CK(cudaGetLastError());
     std::vector<int> h_jp(isz + 1), h_keep(isz + 1);
     std::vector<double> h_rd(isz + 1);
@@ -811,6 +923,7 @@ class Engine {
     HIF_CK(cudaMemcpyAsync(h_rd.data(), d_rd, isz * sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();
     t_id += wall() - ti0;
+    mark("skel pivoted QR", level);
 
     // skeleton / redundant sets (InterpDecomp.cpp:102-110), internal order
     th = wall();
@@ -891,9 +1004,11 @@ class Engine {
     gather(tg2, cells, d_own, d_sd, d_dof, tmp);
     if (verbose) sync();
     t_gather += wall() - tg0;
+    mark("skel gather A_ff", level);
 
     // rotation by the ID: B(red,:) -= W^T B(skel,:); B(:,red) -= B(:,skel) W; B(skel,skel) = 0
     te_rot_and_sweep(st, act, dB, o_B, dWs, o_W, tmp);
+    mark("skel rotate+eliminate", level);
 
     // keep-Schur: S_f = B(skel, skel) after the sweep
     if (keep_schur) {
@@ -938,6 +1053,110 @@ class Engine {
     tmp.release(stream);
     steps.push_back(std::move(st));
     t_host += wall() - th;
+  }
+
+  // Blocked Householder row compression of the faces with more than
+  // kCompressMinN columns: on return idM[f] / idm[f] point at R0 (n x n, ld n).
+  static constexpr int kCompressMinN = 64;
+  int kGroupMinN = 512;  // faces this wide get a CTA group (HIF_OPT_ID_GROUP_MIN_N)
+  void compress_faces(const std::vector<BlockInfo>& blocks,
+                      const std::vector<std::vector<int>>& rows_l, double* dM,
+                      const std::vector<long long>& o_M, std::vector<double*>& idM,
+                      std::vector<int>& idm, BufList& tmp) {
+    std::vector<int> list;
+    long long vsz = 0, wsz = 0, rsz = 0;
+    int maxn = 0;
+    for (size_t f = 0; f < blocks.size(); ++f) {
+      const int n = blocks[f].global.size(), m = rows_l[f].size();
+      if (n > kCompressMinN && m > n) {
+        list.push_back(f);
+        vsz += (long long)m * kQrNB;
+        wsz += (long long)kQrNB * n;
+        rsz += (long long)n * n;
+        maxn = std::max(maxn, n);
+      }
+    }
+    if (list.empty()) return;
+    double* V = tmp.add(dalloc<double>(vsz, stream));
+    double* Y = tmp.add(dalloc<double>(vsz, stream));
+    double* Wt = tmp.add(dalloc<double>(wsz, stream));
+    double* R0 = tmp.add(dalloc<double>(rsz, stream));
+    std::vector<QrDesc> qd;
+    std::vector<long long> o_w, o_r;
+    long long ov = 0, ow = 0, orr = 0;
+    for (int f : list) {
+      const int n = blocks[f].global.size(), m = rows_l[f].size();
+      qd.push_back(QrDesc{dM + o_M[f], V + ov, Y + ov, m, n});
+      o_w.push_back(ow);
+      o_r.push_back(orr);
+      ov += (long long)m * kQrNB;
+      ow += (long long)kQrNB * n;
+      orr += (long long)n * n;
+    }
+    QrDesc* dq = tmp.add(upload(qd, stream));
+    double qfl = 0;
+    for (int k0 = 0; k0 < maxn; k0 += kQrNB) {
+      std::vector<int> act;
+      std::vector<GemmDesc> g1, g2;
+      std::vector<int> t1(1, 0), t2(1, 0);
+      for (size_t q = 0; q < qd.size(); ++q) {
+        const QrDesc& d = qd[q];
+        if (d.n <= k0) continue;
+        act.push_back(q);
+        const int kb = std::min(kQrNB, d.n - k0), mt = d.m - k0, nt = d.n - k0 - kb;
+        qfl += 2.0 * mt * kb * kb;
+        if (nt <= 0) continue;
+        GemmDesc a{};  // Wt = Y^T C
+        a.C = Wt + o_w[q];
+        a.A = d.Y + k0;
+        a.B = d.M + k0 + (long long)(k0 + kb) * d.m;
+        a.ldc = kQrNB;
+        a.lda = d.m;
+        a.ldb = d.m;
+        a.m = kb;
+        a.n = nt;
+        a.k = mt;
+        a.transA = 1;
+        a.alpha = 1.0;
+        a.beta = 0.0;
+        g1.push_back(a);
+        t1.push_back(t1.back() + dgemm_tiles(a.m, a.n));
+        GemmDesc c{};  // C -= V Wt
+        c.C = d.M + k0 + (long long)(k0 + kb) * d.m;
+        c.A = d.V + k0;
+        c.B = Wt + o_w[q];
+        c.ldc = d.m;
+        c.lda = d.m;
+        c.ldb = kQrNB;
+        c.m = mt;
+        c.n = nt;
+        c.k = kb;
+        c.alpha = -1.0;
+        c.beta = 1.0;
+        g2.push_back(c);
+        t2.push_back(t2.back() + dgemm_tiles(c.m, c.n));
+      }
+      BufList step;
+      int* da = step.add(upload(act, stream));
+      timed(HIF_KCLASS_QR, 0, 0, [&] { launch_qr_panel(dq, da, (int)act.size(), k0, stream); });
+      for (auto* gp : {&g1, &g2}) {
+        gemm_batch(*gp, step, stream, HIF_KCLASS_QR,
+                   [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); });
+      }
+      HIF_CK(cudaGetLastError());
+      step.release(stream);
+    }
+    std::vector<TriuDesc> td;
+    for (size_t q = 0; q < qd.size(); ++q) {
+      const int f = list[q], n = qd[q].n;
+      td.push_back(TriuDesc{qd[q].M, R0 + o_r[q], qd[q].m, n, n});
+      idM[f] = R0 + o_r[q];
+      idm[f] = n;
+    }
+    TriuDesc* dtd = tmp.add(upload(td, stream));
+    timed(HIF_KCLASS_QR, 0, 0, [&] { launch_triu(dtd, (int)td.size(), stream); });
+    HIF_CK(cudaGetLastError());
+    (void)qfl;
   }
 
   void te_rot_and_sweep(StepData& st, const std::vector<int>& act, double* dB,
@@ -1001,14 +1220,9 @@ class Engine {
       ca.push_back(CopyDesc{B, st.arena + st.o_a22[f], n, r, r, r});
       ta.push_back(ta.back() + copy_tiles(r, r));
     }
-    auto run_gemm = [&](std::vector<GemmDesc>& g, std::vector<int>& t) {
-      if (g.empty()) return;
-      GemmDesc* d = tmp.add(upload(g, stream));
-      int* to = tmp.add(upload(t, stream));
-      double fl = 0;
-      for (const GemmDesc& x : g) fl += 2.0 * x.m * x.n * x.k;
-      timed(HIF_KCLASS_GEMM, fl, 0, [&] { launch_dgemm(d, to, (int)g.size(), t.back(), stream); });
-      HIF_CK(cudaGetLastError());
+    auto run_gemm = [&](std::vector<GemmDesc>& g, std::vector<int>&) {
+      gemm_batch(g, tmp, stream, HIF_KCLASS_GEMM,
+                 [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); });
     };
     auto run_copy = [&](std::vector<CopyDesc>& c, std::vector<int>& t) {
       if (c.empty()) return;
@@ -1048,6 +1262,8 @@ class Engine {
     cur_bytes = peak_bytes = 0;
     HIF_CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), stream));
     const double t0 = wall();
+    mark_t = 0;
+    mark("start", -1);
     Sources a, b;
     empty_sources(a, 0);
     for (int level = 0; level < L; ++level) {
@@ -1069,6 +1285,7 @@ class Engine {
     HIF_CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
     factored = true;
     if (st & kStatusTinyPivot) throw Error{HIF_ERR_SINGULAR, "zero or non-finite pivot"};
+    if (st & kStatusTimeout) throw Error{HIF_ERR_CUDA, "grouped ID: barrier wait timed out"};
     // the apply sweeps are part of the factorization's output: build them now
     const double tp = wall();
     ensure_workspace(1);
@@ -1671,6 +1888,10 @@ int hif_set_option(hif_handle h, int option, long long value) {
     case HIF_OPT_KEEP_SCHUR: h->e->keep_schur = value != 0; return HIF_OK;
     case HIF_OPT_VERBOSE: h->e->verbose = value != 0; return HIF_OK;
     case HIF_OPT_MEM_BUDGET_MB: h->e->budget_mb = value; return HIF_OK;
+    case HIF_OPT_ID_GROUP_MIN_N:
+      if (value < 2) return HIF_ERR_ARG;
+      h->e->kGroupMinN = (int)value;
+      return HIF_OK;
     case HIF_OPT_PROFILE:
       return guarded([&] {
         h->e->reset_profile();

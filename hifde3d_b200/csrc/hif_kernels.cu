@@ -18,6 +18,7 @@
 
 #include <cfloat>
 #include <climits>
+#include <algorithm>
 #include <cmath>
 
 namespace hif {
@@ -166,9 +167,9 @@ void launch_gather(const GatherTarget* d_tg, const int* d_tile_off, int ntg, int
 // ===========================================================================
 constexpr int kBM = 64, kBN = 64, kBK = 16;
 
-int dgemm_tiles(int m, int n) {
+int dgemm_tiles(int m, int n, int tile) {
   if (m <= 0 || n <= 0) return 0;
-  return ((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
+  return ((m + tile - 1) / tile) * ((n + tile - 1) / tile);
 }
 
 __global__ void __launch_bounds__(256) k_dgemm(const GemmDesc* __restrict__ descs,
@@ -272,10 +273,143 @@ __global__ void __launch_bounds__(256) k_dgemm(const GemmDesc* __restrict__ desc
   }
 }
 
+// ---------------------------------------------------------------------------
+// 128 x 128 x 16 tiles, 256 threads, 8 x 8 outputs per thread, operands staged
+// through a 3-stage cp.async pipeline (8-byte copies: sub-matrix views are
+// only 8-byte aligned; out-of-range elements are zero-filled by the copy).
+// ---------------------------------------------------------------------------
+constexpr int kLBM = 128, kLBN = 128, kLBK = 16, kLStages = 3;
+constexpr int kLAStride = kLBM + 2;  // doubles per k-row of the A stage
+constexpr int kLBStride = kLBN + 2;
+constexpr int kLSmem = kLStages * kLBK * (kLAStride + kLBStride) * (int)sizeof(double);
+// with beta != 0 the C tile is prefetched into shared memory with the first stages
+constexpr int kLSmemC = kLSmem + kLBM * kLBN * (int)sizeof(double);
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
+  const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
+  const int bytes = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(gmem),
+               "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict__ descs,
+                                                     const int* __restrict__ tile_off, int nd) {
+  extern __shared__ double lsm[];
+  double* As = lsm;                                  // [stage][k][kLAStride]
+  double* Bs = lsm + kLStages * kLBK * kLAStride;    // [stage][k][kLBStride]
+  const int di = find_desc(tile_off, nd, blockIdx.x);
+  const GemmDesc g = descs[di];
+  const int local = blockIdx.x - tile_off[di];
+  const int tiles_m = (g.m + kLBM - 1) / kLBM;
+  const int m0 = (local % tiles_m) * kLBM, n0 = (local / tiles_m) * kLBN;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+
+  auto issue = [&](int stage, int k0) {
+    double* as = As + stage * kLBK * kLAStride;
+    double* bs = Bs + stage * kLBK * kLBStride;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      int mm, kk;
+      if (g.transA == 0) { mm = e % kLBM; kk = e / kLBM; } else { mm = e / kLBK; kk = e % kLBK; }
+      const int gm = m0 + mm, gk = k0 + kk;
+      const bool ok = gm < g.m && gk < g.k;
+      const double* src = ok ? ((g.transA == 0) ? g.A + gm + (long long)gk * g.lda
+                                                : g.A + gk + (long long)gm * g.lda)
+                             : g.A;
+      cp_async8(as + kk * kLAStride + mm, src, ok);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      int nn, kk;
+      if (g.transB == 0) { kk = e % kLBK; nn = e / kLBK; } else { nn = e % kLBN; kk = e / kLBN; }
+      const int gn = n0 + nn, gk = k0 + kk;
+      const bool ok = gn < g.n && gk < g.k;
+      const double* src = ok ? ((g.transB == 0) ? g.B + gk + (long long)gn * g.ldb
+                                                : g.B + gn + (long long)gk * g.ldb)
+                             : g.B;
+      cp_async8(bs + kk * kLBStride + nn, src, ok);
+    }
+  };
+
+  double acc[8][8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+
+  double* Cs = lsm + kLStages * kLBK * (kLAStride + kLBStride);  // [col][row], 128 x 128
+  const bool prefetch_c = g.beta != 0.0;
+  if (prefetch_c) {
+    for (int e = tid; e < kLBM * kLBN; e += 256) {
+      const int i = e % kLBM, j = e / kLBM;
+      const bool ok = (m0 + i) < g.m && (n0 + j) < g.n;
+      cp_async8(Cs + e, ok ? g.C + (m0 + i) + (long long)(n0 + j) * g.ldc : g.C, ok);
+    }
+  }
+  const int nk = (g.k + kLBK - 1) / kLBK;
+#pragma unroll
+  for (int st = 0; st < kLStages - 1; ++st) {
+    if (st < nk) issue(st, st * kLBK);
+    cp_async_commit();  // the first group also carries the C tile
+  }
+  for (int t = 0; t < nk; ++t) {
+    cp_async_wait<kLStages - 2>();
+    __syncthreads();
+    const int nt = t + kLStages - 1;
+    if (nt < nk) issue(nt % kLStages, nt * kLBK);
+    cp_async_commit();
+    const double* as = As + (t % kLStages) * kLBK * kLAStride;
+    const double* bs = Bs + (t % kLStages) * kLBK * kLBStride;
+#pragma unroll
+    for (int kk = 0; kk < kLBK; ++kk) {
+      double av[8], bv[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) av[a] = as[kk * kLAStride + tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) bv[b] = bs[kk * kLBStride + ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const int gn = n0 + ty + 16 * b;
+    if (gn >= g.n) continue;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int gm = m0 + tx + 16 * a;
+      if (gm >= g.m) continue;
+      double* c = g.C + gm + (long long)gn * g.ldc;
+      const double v = g.alpha * acc[a][b];
+      *c = prefetch_c ? fma(g.beta, Cs[(ty + 16 * b) * kLBM + tx + 16 * a], v) : v;
+    }
+  }
+}
+
 void launch_dgemm(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
-                  cudaStream_t s) {
+                  cudaStream_t s, int tile) {
   if (total_tiles <= 0) return;
-  k_dgemm<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
+  if (tile == 128) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_dgemm128, cudaFuncAttributeMaxDynamicSharedMemorySize, kLSmemC);
+      attr = true;
+    }
+    k_dgemm128<<<total_tiles, 256, kLSmemC, s>>>(d_desc, d_tile_off, nd);
+  } else {
+    k_dgemm<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
+  }
 }
 
 // ===========================================================================
@@ -364,7 +498,7 @@ __global__ void __launch_bounds__(256) k_sweep_diag(const SweepDesc* __restrict_
   const int di = active[blockIdx.x];
   const SweepDesc d = descs[di];
   const int nb = min(kSweepNB, d.r - k0);
-  __shared__ double S[kSweepNB * kSweepNB];
+  extern __shared__ double S[];  // nb x nb
   __shared__ double s_ip;
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
     const int i = e % nb, j = e / nb;
@@ -402,7 +536,13 @@ __global__ void __launch_bounds__(256) k_sweep_diag(const SweepDesc* __restrict_
 void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
                        double* d_dinv, int* d_status, cudaStream_t s) {
   if (nact <= 0) return;
-  k_sweep_diag<<<nact, 256, 0, s>>>(d_desc, d_active, k0, d_dinv, d_status);
+  const int smem = kSweepNB * kSweepNB * (int)sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  k_sweep_diag<<<nact, 256, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
 }
 
 // Row panel: tile of up to 64 columns [lo, hi) of rows K.
@@ -434,7 +574,7 @@ __global__ void __launch_bounds__(256) k_sweep_rowpanel(const SweepDesc* __restr
 void launch_sweep_rowpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
                            const double* d_dinv, cudaStream_t s) {
   if (ntiles <= 0) return;
-  const int smem = 2 * kSweepNB * kSweepNB * (int)sizeof(double);
+  const int smem = (kSweepNB * kSweepNB + kSweepNB * kPanelTile) * (int)sizeof(double);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_sweep_rowpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -473,7 +613,7 @@ __global__ void __launch_bounds__(256) k_sweep_colpanel(const SweepDesc* __restr
 void launch_sweep_colpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
                            const double* d_dinv, cudaStream_t s) {
   if (ntiles <= 0) return;
-  const int smem = 2 * kSweepNB * kSweepNB * (int)sizeof(double);
+  const int smem = (kSweepNB * kSweepNB + kSweepNB * kPanelTile) * (int)sizeof(double);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_sweep_colpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -701,6 +841,288 @@ __global__ void __launch_bounds__(512) k_id(const IdDesc* __restrict__ descs, do
   }
 }
 
+// ---------------------------------------------------------------------------
+// Grouped ID (see hif_kernels.cuh).
+// ---------------------------------------------------------------------------
+namespace {
+
+// Barrier of the `group` CTAs of one face: arrival counter sync[0], generation
+// sync[1]. Bounded spin; on timeout the status word records kStatusTimeout and
+// *ok turns false (every CTA then skips to the end).
+__device__ void group_barrier(int* sync, int group, int* status, bool* ok) {
+  __syncthreads();
+  if (group > 1 && threadIdx.x == 0) {
+    volatile int* gen = sync + 1;
+    const int g0 = *gen;
+    __threadfence();
+    if (atomicAdd(sync, 1) == group - 1) {
+      atomicExch(sync, 0);
+      __threadfence();
+      atomicAdd(sync + 1, 1);
+    } else {
+      long long spins = 0;
+      while (*gen == g0) {
+        if (++spins > (1LL << 28)) {
+          atomicOr(status, kStatusTimeout);
+          *ok = false;
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(512) k_id_group(const IdGroupDesc* __restrict__ descs,
+                                                  int group, double eps,
+                                                  int* __restrict__ status) {
+  const int face = blockIdx.x / group, me = blockIdx.x % group;
+  const IdGroupDesc gd = descs[face];
+  const IdDesc d = gd.id;
+  const int m = d.m, n = d.n;
+  double* M = d.M;
+  double* vn1 = gd.norms;
+  double* vn2 = gd.norms + n;
+  int* jp = d.jpvt;
+  extern __shared__ double gsm[];
+  double* vsh = gsm;          // reflector rows i..m-1 (m doubles)
+  __shared__ double scratch[64];
+  __shared__ int iscr[32];
+  __shared__ int s_pvt;
+  __shared__ bool s_ok;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = nthr >> 5;
+  const double tol3z = sqrt(DBL_EPSILON * 0.5);
+  if (tid == 0) s_ok = true;
+  __syncthreads();
+
+  // own columns: j = me, me + group, ...
+  for (int j = me + warp * group; j < n; j += nw * group) {
+    double sacc = 0.0;
+    for (int r = lane; r < m; r += 32) {
+      const double v = __ldcg(M + r + (long long)j * m);
+      sacc = fma(v, v, sacc);
+    }
+    sacc = warp_sum(sacc);
+    if (lane == 0) {
+      __stcg(vn1 + j, sqrt(sacc));
+      __stcg(vn2 + j, sqrt(sacc));
+      __stcg(jp + j, j);
+    }
+  }
+  group_barrier(gd.sync, group, status, &s_ok);
+
+  const int steps = min(m, n);
+  for (int i = 0; i < steps && s_ok; ++i) {
+    // ---- candidates over own columns >= i
+    double best = -1.0;
+    int bi = INT_MAX;
+    if (d.order != nullptr) {
+      const int want = d.order[i];
+      for (int j = i + ((me - i % group + group) % group) + tid * group; j < n; j += nthr * group)
+        if (__ldcg(jp + j) == want) { best = 1.0; bi = j; }
+    } else {
+      for (int j = i + ((me - i % group + group) % group) + tid * group; j < n; j += nthr * group) {
+        const double v = __ldcg(vn1 + j);
+        if (v > best || (v == best && j < bi)) { best = v; bi = j; }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (lane == 0) { scratch[warp] = best; iscr[warp] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double b = scratch[0];
+      int bb = iscr[0];
+      for (int w = 1; w < nw; ++w)
+        if (scratch[w] > b || (scratch[w] == b && iscr[w] < bb)) { b = scratch[w]; bb = iscr[w]; }
+      __stcg(gd.cand + me, b);
+      __stcg(gd.sync + 32 + me, bb);
+    }
+    group_barrier(gd.sync, group, status, &s_ok);
+    if (!s_ok) break;
+    if (tid == 0) {
+      double b = -1.0;
+      int bb = INT_MAX;
+      for (int c = 0; c < group; ++c) {
+        const double cb = __ldcg(gd.cand + c);
+        const int ci = __ldcg(gd.sync + 32 + c);
+        if (cb > b || (cb == b && ci < bb)) { b = cb; bb = ci; }
+      }
+      s_pvt = (bb == INT_MAX) ? i : bb;
+    }
+    __syncthreads();
+    const int pvt = s_pvt;
+    // ---- owner of column i: swap, reflector
+    if (i % group == me) {
+      if (pvt != i) {
+        for (int r = tid; r < m; r += nthr) {
+          const double a = __ldcg(M + r + (long long)i * m);
+          const double b = __ldcg(M + r + (long long)pvt * m);
+          __stcg(M + r + (long long)i * m, b);
+          __stcg(M + r + (long long)pvt * m, a);
+        }
+        if (tid == 0) {
+          const int t = __ldcg(jp + pvt);
+          __stcg(jp + pvt, __ldcg(jp + i));
+          __stcg(jp + i, t);
+          __stcg(vn1 + pvt, __ldcg(vn1 + i));
+          __stcg(vn2 + pvt, __ldcg(vn2 + i));
+        }
+      }
+      __syncthreads();
+      double xs = 0.0;
+      for (int r = i + 1 + tid; r < m; r += nthr) {
+        const double v = __ldcg(M + r + (long long)i * m);
+        xs = fma(v, v, xs);
+      }
+      const double xnorm = sqrt(block_sum(xs, scratch));
+      const double alpha = __ldcg(M + i + (long long)i * m);
+      double tau = 0.0, beta = alpha;
+      if (xnorm != 0.0) {
+        beta = -copysign(hypot(alpha, xnorm), alpha);
+        tau = (beta - alpha) / beta;
+        const double scal = 1.0 / (alpha - beta);
+        for (int r = i + 1 + tid; r < m; r += nthr)
+          __stcg(M + r + (long long)i * m, __ldcg(M + r + (long long)i * m) * scal);
+      }
+      __syncthreads();
+      if (tid == 0) {
+        __stcg(M + i + (long long)i * m, beta);
+        d.rdiag[i] = beta;
+        __stcg(gd.tau, tau);
+      }
+    }
+    group_barrier(gd.sync, group, status, &s_ok);
+    if (!s_ok) break;
+    // ---- every CTA: cache the reflector, update its own columns > i
+    const double tau = __ldcg(gd.tau);
+    for (int r = i + 1 + tid; r < m; r += nthr) vsh[r - i - 1] = __ldcg(M + r + (long long)i * m);
+    __syncthreads();
+    const int len = m - i - 1;
+    const int jfirst = i + 1 + ((me - (i + 1) % group + group) % group);
+    if (tau != 0.0) {
+      for (int j = jfirst + warp * group; j < n; j += nw * group) {
+        double* cj = M + (long long)j * m;
+        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+        int r = lane;
+        for (; r + 96 < len; r += 128) {
+          w0 = fma(vsh[r], __ldcg(cj + i + 1 + r), w0);
+          w1 = fma(vsh[r + 32], __ldcg(cj + i + 1 + r + 32), w1);
+          w2 = fma(vsh[r + 64], __ldcg(cj + i + 1 + r + 64), w2);
+          w3 = fma(vsh[r + 96], __ldcg(cj + i + 1 + r + 96), w3);
+        }
+        for (; r < len; r += 32) w0 = fma(vsh[r], __ldcg(cj + i + 1 + r), w0);
+        double w = warp_sum((w0 + w1) + (w2 + w3));
+        const double ci = __ldcg(cj + i);
+        w = (w + ci) * tau;
+        if (lane == 0) __stcg(cj + i, ci - w);
+        for (r = lane; r < len; r += 32)
+          __stcg(cj + i + 1 + r, fma(-w, vsh[r], __ldcg(cj + i + 1 + r)));
+      }
+    }
+    __syncthreads();
+    // ---- norm downdate of own columns (thread per column), recompute on cancellation
+    for (int j = jfirst + tid * group; j < n; j += nthr * group) {
+      const double v1 = __ldcg(vn1 + j);
+      if (v1 != 0.0) {
+        double temp = fabs(__ldcg(M + i + (long long)j * m)) / v1;
+        temp = fmax(1.0 - temp * temp, 0.0);
+        const double q = v1 / __ldcg(vn2 + j);
+        if (temp * q * q <= tol3z) __stcg(vn2 + j, -1.0);  // flag: recompute
+        else __stcg(vn1 + j, v1 * sqrt(temp));
+      }
+    }
+    __syncthreads();
+    for (int j = jfirst + warp * group; j < n; j += nw * group) {
+      if (__ldcg(vn2 + j) != -1.0) continue;
+      double sacc = 0.0;
+      for (int r = i + 1 + lane; r < m; r += 32) {
+        const double v = __ldcg(M + r + (long long)j * m);
+        sacc = fma(v, v, sacc);
+      }
+      sacc = warp_sum(sacc);
+      if (lane == 0) {
+        const double nv = (i + 1 < m) ? sqrt(sacc) : 0.0;
+        __stcg(vn1 + j, nv);
+        __stcg(vn2 + j, nv);
+      }
+    }
+    __syncthreads();
+  }
+  group_barrier(gd.sync, group, status, &s_ok);
+  if (!s_ok) return;
+
+  // ---- rank test (every CTA computes the same list) and W (red columns split over the group)
+  int* flag = reinterpret_cast<int*>(vsh);
+  int* pos = flag + n;
+  __shared__ int s_k;
+  const double r00 = fabs(__ldcg(M));
+  const double tol = r00 * eps;
+  if (tid == 0) {
+    int k = 0;
+    for (int i = 0; i < n; ++i) {
+      const int kp = fabs(__ldcg(M + i + (long long)i * m)) > tol;
+      flag[i] = kp;
+      if (kp) pos[k++] = i;
+    }
+    int rr = k;
+    for (int i = 0; i < n; ++i)
+      if (!flag[i]) pos[rr++] = i;
+    s_k = k;
+    if (me == 0) {
+      *d.rank = k;
+      if (r00 == 0.0) atomicOr(status, kStatusIdZero);
+    }
+  }
+  __syncthreads();
+  const int k = s_k;
+  if (me == 0)
+    for (int j = tid; j < n; j += nthr) {
+      d.jpvt[j] = __ldcg(jp + j);
+      d.keep[j] = flag[j];
+    }
+  const int nred = n - k;
+  for (int b = me * nthr + tid; b < nred; b += nthr * group) {
+    const int c = pos[k + b];
+    double* x = d.W + (long long)b * k;
+    for (int a = 0; a < k; ++a) x[a] = (c >= a) ? __ldcg(M + pos[a] + (long long)c * m) : 0.0;
+    for (int a = k - 1; a >= 0; --a) {
+      const double xa = x[a] / __ldcg(M + pos[a] + (long long)a * m);
+      x[a] = xa;
+      for (int t = 0; t < a; ++t) x[t] = fma(-__ldcg(M + pos[t] + (long long)a * m), xa, x[t]);
+    }
+  }
+}
+
+cudaError_t launch_id_group(const IdGroupDesc* d_desc, int nd, int group, double eps,
+                            int* d_status, cudaStream_t s, int max_m, int max_n) {
+  if (nd <= 0) return cudaSuccess;
+  size_t smem = (size_t)std::max(max_m, 2 * max_n) * sizeof(double) + 64;
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    cudaFuncSetAttribute(k_id_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = smem;
+  }
+  int grid = nd * group;
+  if (group > 1) {
+    // co-residency of the whole grid is required by the group barriers; the
+    // cooperative launch guarantees it or fails without running
+    void* args[] = {(void*)&d_desc, (void*)&group, (void*)&eps, (void*)&d_status};
+    return cudaLaunchCooperativeKernel((const void*)k_id_group, dim3(grid), dim3(512), args, smem,
+                                       s);
+  }
+  k_id_group<<<grid, 512, smem, s>>>(d_desc, group, eps, d_status);
+  return cudaGetLastError();
+}
+
 void launch_id(const IdDesc* d_desc, int nd, int max_n, double eps, int* d_status,
                cudaStream_t s) {
   if (nd <= 0) return;
@@ -739,6 +1161,119 @@ void launch_copy(const CopyDesc* d_desc, const int* d_tile_off, int nd, int tota
                  cudaStream_t s) {
   if (total_tiles <= 0) return;
   k_copy<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
+}
+
+// ===========================================================================
+// Row compression: blocked Householder QR panels (one CTA per face)
+// ===========================================================================
+__global__ void __launch_bounds__(512) k_qr_panel(const QrDesc* __restrict__ descs,
+                                                  const int* __restrict__ active, int k0) {
+  const QrDesc d = descs[active[blockIdx.x]];
+  const int m = d.m, kb = min(kQrNB, d.n - k0);
+  double* M = d.M;
+  __shared__ double s_tau[kQrNB];
+  __shared__ double scratch[64];
+  __shared__ double T[kQrNB * kQrNB];
+  __shared__ double Wd[kQrNB * kQrNB];
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int nw = nthr >> 5;
+  for (int j = 0; j < kb; ++j) {
+    const int col = k0 + j;
+    double* cc = M + (long long)col * m;
+    double xs = 0.0;
+    for (int r = col + 1 + tid; r < m; r += nthr) xs = fma(cc[r], cc[r], xs);
+    const double xnorm = sqrt(block_sum(xs, scratch));
+    const double alpha = cc[col];
+    double tau = 0.0, beta = alpha;
+    if (xnorm != 0.0) {
+      beta = -copysign(hypot(alpha, xnorm), alpha);
+      tau = (beta - alpha) / beta;
+      const double scal = 1.0 / (alpha - beta);
+      for (int r = col + 1 + tid; r < m; r += nthr) cc[r] *= scal;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      cc[col] = beta;
+      s_tau[j] = tau;
+    }
+    __syncthreads();
+    if (tau != 0.0) {
+      for (int c = col + 1 + warp; c < k0 + kb; c += nw) {
+        double* cj = M + (long long)c * m;
+        double w = (lane == 0) ? cj[col] : 0.0;
+        for (int r = col + 1 + lane; r < m; r += 32) w = fma(cc[r], cj[r], w);
+        w = warp_sum(w) * tau;
+        if (lane == 0) cj[col] -= w;
+        for (int r = col + 1 + lane; r < m; r += 32) cj[r] = fma(-w, cc[r], cj[r]);
+      }
+    }
+    __syncthreads();
+  }
+  // explicit V (unit diagonal, zeros above) for rows k0..m-1
+  const int mt = m - k0;
+  for (long long e = tid; e < (long long)mt * kb; e += nthr) {
+    const int rr = (int)(e % mt), j = (int)(e / mt);
+    const int r = k0 + rr;
+    double v = 0.0;
+    if (r == k0 + j) v = 1.0;
+    else if (r > k0 + j) v = M[r + (long long)(k0 + j) * m];
+    d.V[r + (long long)j * m] = v;
+  }
+  __syncthreads();
+  // Wd[i, j] = V[:, i]^T V[:, j] for i < j (rows >= k0 + j, where V[:, j] lives)
+  const int npair = kb * (kb - 1) / 2;
+  for (int pidx = warp; pidx < npair; pidx += nw) {
+    int j = 1, base = 0;
+    while (base + j <= pidx) { base += j; ++j; }
+    const int i = pidx - base;
+    double w = 0.0;
+    for (int r = k0 + j + lane; r < m; r += 32)
+      w = fma(d.V[r + (long long)i * m], d.V[r + (long long)j * m], w);
+    w = warp_sum(w);
+    if (lane == 0) Wd[i + j * kQrNB] = w;
+  }
+  __syncthreads();
+  // T (dlarft, forward columnwise): T[j,j] = tau_j, T[0:j, j] = -tau_j T[0:j,0:j] w[0:j, j]
+  for (int j = 0; j < kb; ++j) {
+    if (tid < j) {
+      double acc = 0.0;
+      for (int l = tid; l < j; ++l) acc = fma(T[tid + l * kQrNB], Wd[l + j * kQrNB], acc);
+      T[tid + j * kQrNB] = -s_tau[j] * acc;
+    }
+    if (tid == 0) T[j + j * kQrNB] = s_tau[j];
+    for (int i = j + 1 + tid; i < kQrNB; i += nthr) T[i + j * kQrNB] = 0.0;
+    __syncthreads();
+  }
+  // Y = V T
+  for (long long e = tid; e < (long long)mt * kb; e += nthr) {
+    const int rr = (int)(e % mt), j = (int)(e / mt);
+    const int r = k0 + rr;
+    double acc = 0.0;
+    for (int l = 0; l <= j; ++l) acc = fma(d.V[r + (long long)l * m], T[l + j * kQrNB], acc);
+    d.Y[r + (long long)j * m] = acc;
+  }
+}
+
+void launch_qr_panel(const QrDesc* d_desc, const int* d_active, int nact, int k0,
+                     cudaStream_t s) {
+  if (nact <= 0) return;
+  k_qr_panel<<<nact, 512, 0, s>>>(d_desc, d_active, k0);
+}
+
+__global__ void k_triu(const TriuDesc* __restrict__ descs) {
+  const TriuDesc d = descs[blockIdx.y];
+  const long long nn = (long long)d.n * d.n;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % d.n), j = (int)(e / d.n);
+    d.dst[i + j * d.ldd] = (i <= j) ? d.src[i + j * d.lds] : 0.0;
+  }
+}
+
+void launch_triu(const TriuDesc* d_desc, int nd, cudaStream_t s) {
+  if (nd <= 0) return;
+  dim3 grid(64, nd);
+  k_triu<<<grid, 256, 0, s>>>(d_desc);
 }
 
 __global__ void k_trsm_upper(const double* __restrict__ R, long long ldr, int k,

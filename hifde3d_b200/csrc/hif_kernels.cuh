@@ -114,9 +114,11 @@ void launch_gather(const GatherTarget* d_tg, const int* d_tile_off, int ntg, int
                    const double* d_band, long long ncell3, int NC, cudaStream_t s);
 int gather_tiles(int m, int n);
 
+// tile: 64 (64x64x16, 4x4 per thread) or 128 (128x128x16, 8x8 per thread,
+// 3-stage cp.async pipeline); tile offsets must be built with the same tile.
 void launch_dgemm(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
-                  cudaStream_t s);
-int dgemm_tiles(int m, int n);
+                  cudaStream_t s, int tile = 64);
+int dgemm_tiles(int m, int n, int tile = 64);
 
 // In-shared-memory Gauss-Jordan sweep of the first r pivots (n <= kSmallSweepN).
 constexpr int kSmallSweepN = 160;
@@ -124,12 +126,14 @@ void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_statu
                         cudaStream_t s);
 
 // Blocked sweep, one pivot block [k0, k0+nbk) of every active block.
-constexpr int kSweepNB = 64;
+constexpr int kSweepNB = 128;
+constexpr int kPanelTile = 64;  // rows / columns per panel tile
 void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
                        double* d_dinv, int* d_status, cudaStream_t s);
-// Panel tile maps hold 4 ints per tile: {descriptor, lo, hi, unused}; the
-// row panel covers columns [lo, hi) of pivot rows, the column panel rows
-// [lo, hi) of pivot columns. d_dinv holds kSweepNB^2 doubles per descriptor.
+// Panel tile maps hold 4 ints per tile: {descriptor, lo, hi, unused} with
+// hi - lo <= kPanelTile; the row panel covers columns [lo, hi) of pivot rows,
+// the column panel rows [lo, hi) of pivot columns. d_dinv holds kSweepNB^2
+// doubles per descriptor.
 void launch_sweep_rowpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
                            const double* d_dinv, cudaStream_t s);
 void launch_sweep_colpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
@@ -144,6 +148,50 @@ void launch_id(const IdDesc* d_desc, int nd, int max_n, double eps, int* d_statu
 
 void launch_copy(const CopyDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
                  cudaStream_t s);
+
+// Grouped interpolative decomposition: `group` CTAs cooperate on one face,
+// owning its columns cyclically (column j belongs to CTA j % group). Per
+// column step: candidates -> group barrier -> the pivot column's owner swaps
+// and builds the reflector -> group barrier -> every CTA updates its columns.
+// Cross-CTA data goes through L2; barrier waits are bounded (a timeout sets
+// kStatusTimeout and the kernel returns). Results equal k_id's. Needs all CTAs
+// co-resident: launched cooperatively when group > 1.
+// work: per face 4 * n doubles + 64 ints of scratch (norms, pivots, barrier).
+enum { kStatusTimeout = 8 };
+struct IdGroupDesc {
+  IdDesc id;
+  double* norms;  // 2n (vn1, vn2)
+  int* sync;      // 64 ints: barrier count / generation, candidates
+  double* cand;   // group doubles
+  double* tau;    // 1
+};
+cudaError_t launch_id_group(const IdGroupDesc* d_desc, int nd, int group, double eps,
+                            int* d_status, cudaStream_t s, int max_m, int max_n);
+
+// Row compression of a tall face block before its pivoted QR: blocked
+// Householder QR (no pivoting) in 32-column panels. For panel [k0, k0+kb) the
+// panel kernel factors M[k0:m, k0:k0+kb) in place and writes the explicit
+// reflector block V (unit diagonal, zeros above) and Y = V T, T the upper
+// triangular factor of the compact WY form I - V T V^T, both m x 32 with ld m
+// (rows below k0 unused). The trailing columns are then updated by two batched
+// GEMMs: Wt = Y^T C, C -= V Wt.
+constexpr int kQrNB = 32;
+struct QrDesc {
+  double* M;  // m x n, ld m
+  double* V;  // m x kQrNB, ld m
+  double* Y;  // m x kQrNB, ld m
+  int m, n;
+};
+void launch_qr_panel(const QrDesc* d_desc, const int* d_active, int nact, int k0,
+                     cudaStream_t s);
+// dst (n x n, ld ldd) = upper triangle of src (ld lds), zeros below.
+struct TriuDesc {
+  const double* src;
+  double* dst;
+  long long lds, ldd;
+  int n;
+};
+void launch_triu(const TriuDesc* d_desc, int nd, cudaStream_t s);
 
 // Solve R X = B in place (R: k x k upper triangular, non-unit; B: k x nb), one
 // right-hand side column per thread (the reference's dtrsm('L','U','N','N') call,

@@ -31,7 +31,7 @@ extern thread_local std::string g_last_error;
 namespace {
 
 constexpr int kNoAllocMaxN = 512;
-constexpr int kNB = hif::kSweepNB;
+constexpr int kNB = 64;  // pivot block of this variant
 constexpr size_t kScratchDoubles = (size_t)kNoAllocMaxN * kNoAllocMaxN + kNB * kNB + 32;
 constexpr size_t kNoAllocScratchBytes = kScratchDoubles * sizeof(double);
 static_assert(kNoAllocScratchBytes < (2u << 20) + (64u << 10), "scratch stays about 2 MiB");

@@ -147,7 +147,8 @@ enum hif_option {
   HIF_OPT_KEEP_SCHUR = 1,    /* keep every Schur complement for hif_block_matrix(which=4) */
   HIF_OPT_VERBOSE = 2,       /* per-phase timings on stderr */
   HIF_OPT_MEM_BUDGET_MB = 3, /* refuse factorizations whose device memory exceeds this */
-  HIF_OPT_PROFILE = 4        /* time every launch with CUDA events (resets the counters) */
+  HIF_OPT_PROFILE = 4,       /* time every launch with CUDA events (resets the counters) */
+  HIF_OPT_ID_GROUP_MIN_N = 5 /* faces with at least this many columns get a CTA group (default 512) */
 };
 int hif_set_option(hif_handle h, int option, long long value);
 
