@@ -72,6 +72,8 @@ _SIGNATURES = {
     "hif_set_replay_pivots": [_p, _i, _i, _ip, _ip],
     "hif_factor_stats": [_p, _dp, _dp, _dp, _dp, _dp, _llp],
     "hif_kernel_stats": [_p, _i, _llp, _dp, _dp, _dp],
+    "hif_memory": [_p, _llp, _llp],
+    "hif_trim": [_p],
     "hif_schur": [_dp, _i, _ll, _ip, _i, _ip, _i, _dp, _dp, _dp, _dp],
     "hif_schur_device": [_p, _i, _i, _p, _p, _p],
     "hif_schur_device_noalloc": [_p, _i, _i, _p, _p, _p, _p],
@@ -290,6 +292,15 @@ class HIFFactor:
                                           ctypes.byref(fl), ctypes.byref(by)))
             out[name] = {"launches": n.value, "ms": ms.value, "flops": fl.value, "bytes": by.value}
         return out
+
+    def memory(self) -> dict:
+        fb, wb = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().hif_memory(self._h, ctypes.byref(fb), ctypes.byref(wb)))
+        return {"factor_bytes": fb.value, "workspace_bytes": wb.value}
+
+    def trim(self):
+        """Return the factorization workspace to the device (the factor stays)."""
+        _check(lib().hif_trim(self._h))
 
     def factor_stats(self) -> dict:
         vals = [ctypes.c_double() for _ in range(5)]

@@ -28,8 +28,10 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <atomic>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/hif_b200.h"
@@ -81,6 +83,28 @@ T* upload(const std::vector<T>& v, cudaStream_t s) {
   return d;
 }
 
+// Host parallel loop over [0, n) in chunks (partitioning of cells / faces).
+template <class F>
+void parallel_for(int n, F&& f) {
+  const int nt = std::min<int>(std::max(1u, std::thread::hardware_concurrency()), 32);
+  if (n < 256 || nt <= 1) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<int> next(0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&] {
+      for (;;) {
+        const int i0 = next.fetch_add(64);
+        if (i0 >= n) break;
+        const int i1 = std::min(n, i0 + 64);
+        for (int i = i0; i < i1; ++i) f(i);
+      }
+    });
+  for (std::thread& x : th) x.join();
+}
+
 // Keeps device buffers of one phase alive until released together.
 struct BufList {
   std::vector<void*> p;
@@ -92,6 +116,62 @@ struct BufList {
   void release(cudaStream_t s) {
     for (void* x : p) dfree(x, s);
     p.clear();
+  }
+};
+
+// Device memory for the factorization's big buffers: chunks obtained from
+// cudaMalloc once and kept for the life of the handle, bump-allocated, and
+// made free again by reset(). All users are on one stream, so a reset followed
+// by new allocations is ordered after the previous users' kernels. Successive
+// factorizations of one size request the same sequence, so after the first the
+// chunks are reused as they are and no allocator call is made.
+struct Arena {
+  struct Chunk {
+    char* p;
+    size_t size, used;
+  };
+  std::vector<Chunk> chunks;
+  size_t cur = 0;
+  static constexpr size_t kMinChunk = size_t(256) << 20;
+
+  template <class T>
+  T* alloc(size_t count) {
+    size_t bytes = (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
+    for (; cur < chunks.size(); ++cur) {
+      Chunk& c = chunks[cur];
+      if (c.size - c.used >= bytes) {
+        void* r = c.p + c.used;
+        c.used += bytes;
+        return static_cast<T*>(r);
+      }
+    }
+    const size_t sz = std::max(bytes, kMinChunk);
+    void* p = nullptr;
+    HIF_CK(cudaMalloc(&p, sz));
+    chunks.push_back(Chunk{static_cast<char*>(p), sz, bytes});
+    cur = chunks.size() - 1;
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* upload(const std::vector<T>& v, cudaStream_t s) {
+    T* d = alloc<T>(v.size());
+    if (!v.empty())
+      HIF_CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    return d;
+  }
+  void reset() {
+    for (Chunk& c : chunks) c.used = 0;
+    cur = 0;
+  }
+  size_t reserved() const {
+    size_t t = 0;
+    for (const Chunk& c : chunks) t += c.size;
+    return t;
+  }
+  void release() {
+    for (Chunk& c : chunks) cudaFree(c.p);
+    chunks.clear();
+    cur = 0;
   }
 };
 
@@ -158,25 +238,72 @@ struct Sources {
 };
 
 // One batched GEMM launch; 128x128 tiles when most of the work sits in
-// problems at least that large, else 64x64.
+// problems at least that large (or when forced: in-place panel products rely on
+// a single output tile along the aliased dimension), else 64x64. Problems with
+// a reduction much longer than their output dimensions are split along k into
+// partial products and summed in a fixed order.
 template <class Timed>
-void gemm_batch(const std::vector<GemmDesc>& g, BufList& tmp, cudaStream_t stream, int cls,
-                Timed&& timed) {
-  if (g.empty()) return;
-  double big = 0, all = 0, fl = 0;
+void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t stream, int cls,
+                Timed&& timed, int force_tile = 0) {
+  if (gin.empty()) return;
+  std::vector<GemmDesc> g;
+  std::vector<SplitKDesc> red;
+  double fl = 0;
+  long long psz = 0;
+  struct Split {
+    size_t idx;
+    int S;
+  };
+  std::vector<Split> splits;
+  for (size_t q = 0; q < gin.size(); ++q) {
+    const GemmDesc& x = gin[q];
+    fl += 2.0 * x.m * x.n * x.k;
+    const int big = std::max(x.m, x.n);
+    if (force_tile == 0 && x.k >= 2048 && x.k >= 8 * big) {
+      const int S = std::min(32, (x.k + 1023) / 1024);
+      splits.push_back(Split{q, S});
+      psz += (long long)S * x.m * x.n;
+    } else {
+      g.push_back(x);
+    }
+  }
+  double* P = psz ? tmp.add(dalloc<double>(psz, stream)) : nullptr;
+  long long po = 0;
+  for (const Split& sp : splits) {
+    const GemmDesc& x = gin[sp.idx];
+    const int chunk = (x.k + sp.S - 1) / sp.S;
+    for (int q = 0; q < sp.S; ++q) {
+      const int k0 = q * chunk, kk = std::min(chunk, x.k - k0);
+      GemmDesc y = x;
+      y.C = P + po + (long long)q * x.m * x.n;
+      y.ldc = x.m;
+      y.k = std::max(kk, 0);
+      y.A = x.transA == 0 ? x.A + (long long)k0 * x.lda : x.A + k0;
+      y.B = x.transB == 0 ? x.B + k0 : x.B + (long long)k0 * x.ldb;
+      y.alpha = 1.0;
+      y.beta = 0.0;
+      g.push_back(y);
+    }
+    red.push_back(SplitKDesc{x.C, P + po, x.ldc, x.m, x.n, sp.S, x.alpha, x.beta});
+    po += (long long)sp.S * x.m * x.n;
+  }
+  double big = 0, all = 0;
   for (const GemmDesc& x : g) {
     const double w = (double)x.m * x.n;
     all += w;
     if (x.m >= 96 && x.n >= 96) big += w;
-    fl += 2.0 * x.m * x.n * x.k;
   }
-  const int tile = (big >= 0.5 * all) ? 128 : 64;
+  const int tile = force_tile ? force_tile : ((big >= 0.5 * all) ? 128 : 64);
   std::vector<int> toff(1, 0);
   for (const GemmDesc& x : g) toff.push_back(toff.back() + dgemm_tiles(x.m, x.n, tile));
-  if (toff.back() == 0) return;
+  if (toff.back() == 0 && red.empty()) return;
   GemmDesc* dg = tmp.add(upload(g, stream));
   int* dt = tmp.add(upload(toff, stream));
   timed(cls, fl, 0.0, [&] { launch_dgemm(dg, dt, (int)g.size(), toff.back(), stream, tile); }, 1);
+  if (!red.empty()) {
+    SplitKDesc* dr = tmp.add(upload(red, stream));
+    timed(cls, 0.0, 0.0, [&] { launch_splitk_reduce(dr, (int)red.size(), stream); }, 1);
+  }
   HIF_CK(cudaGetLastError());
 }
 
@@ -220,26 +347,50 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
   for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
   for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
     std::vector<int> active;
-    std::vector<int> rowt, colt;
-    std::vector<GemmDesc> gd;
+    std::vector<GemmDesc> gd, rowg, colg;
     for (int b = 0; b < nl; ++b) {
       const SweepDesc& d = large[b];
       if (d.r <= k0) continue;
       active.push_back(b);
       const int k1 = std::min(d.r, k0 + kSweepNB);
-      auto tiles = [&](std::vector<int>& out, int lo, int hi) {
-        for (int x = lo; x < hi; x += kPanelTile) {
-          out.push_back(b);
-          out.push_back(x);
-          out.push_back(std::min(hi, x + kPanelTile));
-          out.push_back(0);
-        }
-      };
-      tiles(rowt, 0, k0);
-      tiles(rowt, k1, d.n);
-      tiles(colt, 0, k0);
-      tiles(colt, k1, d.r);
       const int nbk = k1 - k0;
+      const double* Dv = dinv + (long long)b * kSweepNB * kSweepNB;  // nbk x nbk, ld nbk
+      // row panel B[K, c0:c1) = Dinv B[K, c0:c1), in place: one 128-row tile
+      auto rowp = [&](int c0, int c1) {
+        if (c1 <= c0) return;
+        GemmDesc g{};
+        g.C = d.B + k0 + (long long)c0 * d.n;
+        g.A = Dv;
+        g.B = g.C;
+        g.ldc = g.ldb = d.n;
+        g.lda = nbk;
+        g.m = nbk;
+        g.n = c1 - c0;
+        g.k = nbk;
+        g.alpha = 1.0;
+        g.beta = 0.0;
+        rowg.push_back(g);
+      };
+      // column panel B[r0:r1, K] = -B[r0:r1, K] Dinv, in place: one 128-column tile
+      auto colp = [&](int r0, int r1) {
+        if (r1 <= r0) return;
+        GemmDesc g{};
+        g.C = d.B + r0 + (long long)k0 * d.n;
+        g.A = g.C;
+        g.B = Dv;
+        g.ldc = g.lda = d.n;
+        g.ldb = nbk;
+        g.m = r1 - r0;
+        g.n = nbk;
+        g.k = nbk;
+        g.alpha = -1.0;
+        g.beta = 0.0;
+        colg.push_back(g);
+      };
+      rowp(0, k0);
+      rowp(k1, d.n);
+      colp(0, k0);
+      colp(k1, d.r);
       auto gemm = [&](int r0, int r1, int c0, int c1) {
         if (r1 <= r0 || c1 <= c0) return;
         GemmDesc g{};
@@ -262,17 +413,15 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
     }
     BufList step;
     int* dact = step.add(upload(active, stream));
-    int* drow = step.add(upload(rowt, stream));
-    int* dcol = step.add(upload(colt, stream));
     timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
       launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
-      launch_sweep_rowpanel(dd, drow, (int)rowt.size() / 4, k0, dinv, stream);
-    }, 2);
+    });
+    gemm_batch(rowg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
     gemm_batch(gd, step, stream, HIF_KCLASS_GEMM, timed);
+    gemm_batch(colg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
     timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
-      launch_sweep_colpanel(dd, dcol, (int)colt.size() / 4, k0, dinv, stream);
       launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
-    }, 2);
+    });
     HIF_CK(cudaGetLastError());
     step.release(stream);
   }
@@ -306,6 +455,9 @@ class Engine {
   bool have_op = false, initialized = false, factored = false;
   std::vector<uint8_t> rem;
   std::vector<StepData> steps;
+  // factor storage (persistent) and per-level workspace (alternating by level)
+  Arena arena_factor, arena_work[2];
+  Arena* cur_work = &arena_work[0];
   bool keep_schur = false, verbose = false;
   long long budget_mb = 0;
   std::map<int, std::vector<std::vector<int>>> replay;
@@ -414,6 +566,10 @@ class Engine {
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     release_factor();
     release_workspace();
+    sync_quiet();
+    arena_factor.release();
+    arena_work[0].release();
+    arena_work[1].release();
     dfree(d_band, stream);
     dfree(d_status, stream);
     cudaStreamSynchronize(stream);
@@ -454,12 +610,8 @@ class Engine {
     dfree(d_contrib, stream);
     d_contrib = nullptr;
     contrib_cap = 0;
-    for (StepData& st : steps) {
-      dfree(st.arena, stream);
-      dfree(st.d_red, stream);
-      dfree(st.d_skel, stream);
-    }
     steps.clear();
+    arena_factor.reset();
     factored = false;
   }
 
@@ -558,15 +710,12 @@ class Engine {
     Partitioner part{N, P, NC, rem.data()};
     const int ncell = cpd * cpd * cpd;
     st.blocks.resize(ncell);
-    for (int ci = 0; ci < cpd; ++ci)
-      for (int cj = 0; cj < cpd; ++cj)
-        for (int ck = 0; ck < cpd; ++ck) {
-          const int idx = (ci * cpd + cj) * cpd + ck;
-          const int c[3] = {ci, cj, ck};
-          BlockInfo& b = st.blocks[idx];
-          part.cell_index(level, c, b.global, b.red_pos, b.skel_pos);
-          b.cell = idx;
-        }
+    parallel_for(ncell, [&](int idx) {
+      const int c[3] = {idx / (cpd * cpd), (idx / cpd) % cpd, idx % cpd};
+      BlockInfo& b = st.blocks[idx];
+      part.cell_index(level, c, b.global, b.red_pos, b.skel_pos);
+      b.cell = idx;
+    });
     // sizes and device layout
     std::vector<int> red_all, skel_all;
     long long bsz = 0, asz = 0;
@@ -607,12 +756,15 @@ class Engine {
     t_host += wall() - th;
 
     track((bsz + asz) * 8);
-    double* dB = dalloc<double>(bsz, stream);
-    st.arena = dalloc<double>(asz, stream);
-    st.d_red = upload(red_all, stream);
-    st.d_skel = upload(skel_all, stream);
+    // this level's workspace: what it held (level - 2) is no longer read
+    Arena& work = arena_work[level & 1];
+    work.reset();
+    double* dB = work.alloc<double>(bsz);
+    st.arena = arena_factor.alloc<double>(asz);
+    st.d_red = arena_factor.upload(red_all, stream);
+    st.d_skel = arena_factor.upload(skel_all, stream);
     BufList tmp;
-    int* drows = tmp.add(upload(rows_all, stream));
+    int* drows = work.upload(rows_all, stream);
 
     // gather every cell block
     double tg0 = wall();
@@ -713,7 +865,6 @@ class Engine {
         out.dof_src[(2 * slot + 1) * n3 + p] = t;
       }
     }
-    out.bufs.add(dB);
     // remove eliminated DOFs (UpdateRemainingDOFs, src/Factor.cpp:91-111)
     for (int p : red_all) rem[p] = 0;
     tmp.release(stream);
@@ -732,24 +883,32 @@ class Engine {
     Partitioner part{N, P, NC, rem.data()};
     std::vector<std::vector<int>> rows_l;
     std::vector<BlockInfo>& blocks = st.blocks;
-    std::vector<int> rws, cls;
-    for (int ci = 0; ci < cpd; ++ci)
-      for (int cj = 0; cj < cpd; ++cj)
-        for (int ck = 0; ck < cpd; ++ck) {
-          const int c[3] = {ci, cj, ck};
-          for (int face : {TOP, FRONT, LEFT}) {
-            int nb[3];
-            if (!part.skel_interaction(level, c, face, rws, cls, nb)) continue;
-            if (cls.empty()) continue;
-            BlockInfo b;
-            b.face = face;
-            b.global = cls;
-            b.cell = (ci * cpd + cj) * cpd + ck;
-            b.nbr = (nb[0] * cpd + nb[1]) * cpd + nb[2];
-            blocks.push_back(std::move(b));
-            rows_l.push_back(rws);
-          }
+    {
+      const int ncell = cpd * cpd * cpd;
+      std::vector<std::vector<BlockInfo>> pb(ncell);
+      std::vector<std::vector<std::vector<int>>> pr(ncell);
+      parallel_for(ncell, [&](int idx) {
+        const int c[3] = {idx / (cpd * cpd), (idx / cpd) % cpd, idx % cpd};
+        std::vector<int> rw, cl;
+        for (int face : {TOP, FRONT, LEFT}) {
+          int nb[3];
+          if (!part.skel_interaction(level, c, face, rw, cl, nb)) continue;
+          if (cl.empty()) continue;
+          BlockInfo b;
+          b.face = face;
+          b.global = cl;
+          b.cell = idx;
+          b.nbr = (nb[0] * cpd + nb[1]) * cpd + nb[2];
+          pb[idx].push_back(std::move(b));
+          pr[idx].push_back(rw);
         }
+      });
+      for (int idx = 0; idx < ncell; ++idx)
+        for (size_t q = 0; q < pb[idx].size(); ++q) {
+          blocks.push_back(std::move(pb[idx][q]));
+          rows_l.push_back(std::move(pr[idx][q]));
+        }
+    }
     const int nf = (int)blocks.size();
     // M blocks (rows x cols) and ID workspace
     std::vector<int> idx_all;
@@ -775,8 +934,10 @@ class Engine {
 
     BufList tmp;
     track((msz + wsz) * 8);
-    double* dM = tmp.add(dalloc<double>(msz, stream));
-    double* dWs = tmp.add(dalloc<double>(wsz, stream));
+    Arena& work = arena_work[level & 1];
+    cur_work = &work;
+    double* dM = work.alloc<double>(msz);
+    double* dWs = work.alloc<double>(wsz);
     int* didx = tmp.add(upload(idx_all, stream));
     int* d_jp = tmp.add(dalloc<int>(isz + 1, stream));
     int* d_keep = tmp.add(dalloc<int>(isz + 1, stream));
@@ -973,11 +1134,11 @@ class Engine {
     t_host += wall() - th;
 
     track((bsz + asz) * 8);
-    double* dB = dalloc<double>(bsz, stream);
-    st.arena = dalloc<double>(asz, stream);
-    st.d_red = upload(red_all, stream);
-    st.d_skel = upload(skel_all, stream);
-    int* drows2 = tmp.add(upload(rows2, stream));
+    double* dB = work.alloc<double>(bsz);
+    st.arena = arena_factor.alloc<double>(asz);
+    st.d_red = arena_factor.upload(red_all, stream);
+    st.d_skel = arena_factor.upload(skel_all, stream);
+    int* drows2 = work.upload(rows2, stream);
 
     // A_ff in [red | skel] order (SchurAfterID, src/Factor.cpp:113-153)
     tg0 = wall();
@@ -1048,7 +1209,6 @@ class Engine {
     // T_c buffers move to the output set; add this phase's B
     out.bufs.p = cells.bufs.p;
     cells.bufs.p.clear();
-    out.bufs.add(dB);
     for (int p : red_all) rem[p] = 0;
     tmp.release(stream);
     steps.push_back(std::move(st));
@@ -1077,16 +1237,19 @@ class Engine {
       }
     }
     if (list.empty()) return;
-    double* V = tmp.add(dalloc<double>(vsz, stream));
-    double* Y = tmp.add(dalloc<double>(vsz, stream));
-    double* Wt = tmp.add(dalloc<double>(wsz, stream));
-    double* R0 = tmp.add(dalloc<double>(rsz, stream));
+    Arena& work = *cur_work;
+    double* V = work.alloc<double>(vsz);
+    double* Tm = work.alloc<double>((size_t)list.size() * kQrNB * kQrNB);
+    double* Z = work.alloc<double>(wsz);
+    double* Z2 = work.alloc<double>(wsz);
+    double* R0 = work.alloc<double>(rsz);
     std::vector<QrDesc> qd;
     std::vector<long long> o_w, o_r;
     long long ov = 0, ow = 0, orr = 0;
-    for (int f : list) {
+    for (size_t q = 0; q < list.size(); ++q) {
+      const int f = list[q];
       const int n = blocks[f].global.size(), m = rows_l[f].size();
-      qd.push_back(QrDesc{dM + o_M[f], V + ov, Y + ov, m, n});
+      qd.push_back(QrDesc{dM + o_M[f], V + ov, Tm + (long long)q * kQrNB * kQrNB, m, n});
       o_w.push_back(ow);
       o_r.push_back(orr);
       ov += (long long)m * kQrNB;
@@ -1094,22 +1257,21 @@ class Engine {
       orr += (long long)n * n;
     }
     QrDesc* dq = tmp.add(upload(qd, stream));
-    double qfl = 0;
+    auto tm = [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); };
     for (int k0 = 0; k0 < maxn; k0 += kQrNB) {
       std::vector<int> act;
-      std::vector<GemmDesc> g1, g2;
-      std::vector<int> t1(1, 0), t2(1, 0);
+      std::vector<GemmDesc> g1, g2, g3;
       for (size_t q = 0; q < qd.size(); ++q) {
         const QrDesc& d = qd[q];
         if (d.n <= k0) continue;
         act.push_back(q);
         const int kb = std::min(kQrNB, d.n - k0), mt = d.m - k0, nt = d.n - k0 - kb;
-        qfl += 2.0 * mt * kb * kb;
         if (nt <= 0) continue;
-        GemmDesc a{};  // Wt = Y^T C
-        a.C = Wt + o_w[q];
-        a.A = d.Y + k0;
-        a.B = d.M + k0 + (long long)(k0 + kb) * d.m;
+        double* C = d.M + k0 + (long long)(k0 + kb) * d.m;
+        GemmDesc a{};  // Z = V^T C
+        a.C = Z + o_w[q];
+        a.A = d.V + k0;
+        a.B = C;
         a.ldc = kQrNB;
         a.lda = d.m;
         a.ldb = d.m;
@@ -1120,11 +1282,24 @@ class Engine {
         a.alpha = 1.0;
         a.beta = 0.0;
         g1.push_back(a);
-        t1.push_back(t1.back() + dgemm_tiles(a.m, a.n));
-        GemmDesc c{};  // C -= V Wt
-        c.C = d.M + k0 + (long long)(k0 + kb) * d.m;
+        GemmDesc t{};  // Z2 = T^T Z
+        t.C = Z2 + o_w[q];
+        t.A = d.T;
+        t.B = Z + o_w[q];
+        t.ldc = kQrNB;
+        t.lda = kQrNB;
+        t.ldb = kQrNB;
+        t.m = kb;
+        t.n = nt;
+        t.k = kb;
+        t.transA = 1;
+        t.alpha = 1.0;
+        t.beta = 0.0;
+        g2.push_back(t);
+        GemmDesc c{};  // C -= V Z2
+        c.C = C;
         c.A = d.V + k0;
-        c.B = Wt + o_w[q];
+        c.B = Z2 + o_w[q];
         c.ldc = d.m;
         c.lda = d.m;
         c.ldb = kQrNB;
@@ -1133,16 +1308,14 @@ class Engine {
         c.k = kb;
         c.alpha = -1.0;
         c.beta = 1.0;
-        g2.push_back(c);
-        t2.push_back(t2.back() + dgemm_tiles(c.m, c.n));
+        g3.push_back(c);
       }
       BufList step;
       int* da = step.add(upload(act, stream));
       timed(HIF_KCLASS_QR, 0, 0, [&] { launch_qr_panel(dq, da, (int)act.size(), k0, stream); });
-      for (auto* gp : {&g1, &g2}) {
-        gemm_batch(*gp, step, stream, HIF_KCLASS_QR,
-                   [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); });
-      }
+      gemm_batch(g1, step, stream, HIF_KCLASS_QR, tm);
+      gemm_batch(g2, step, stream, HIF_KCLASS_QR, tm);
+      gemm_batch(g3, step, stream, HIF_KCLASS_QR, tm);
       HIF_CK(cudaGetLastError());
       step.release(stream);
     }
@@ -1156,7 +1329,6 @@ class Engine {
     TriuDesc* dtd = tmp.add(upload(td, stream));
     timed(HIF_KCLASS_QR, 0, 0, [&] { launch_triu(dtd, (int)td.size(), stream); });
     HIF_CK(cudaGetLastError());
-    (void)qfl;
   }
 
   void te_rot_and_sweep(StepData& st, const std::vector<int>& act, double* dB,
@@ -1924,7 +2096,10 @@ int hif_factor_stats(hif_handle h, double* total_s, double* gather_s, double* el
   if (elim_s) *elim_s = e.t_elim;
   if (id_s) *id_s = e.t_id;
   if (host_s) *host_s = e.t_host;
-  if (device_bytes) *device_bytes = e.peak_bytes;
+  if (device_bytes)
+    *device_bytes = (long long)(e.arena_factor.reserved() + e.arena_work[0].reserved() +
+                                e.arena_work[1].reserved()) +
+                    7LL * e.n3 * 8;
   return HIF_OK;
 }
 
@@ -2130,6 +2305,23 @@ int hif_triangular_solve(const double* R, int k, long long ldr, double* B, int n
                              cudaMemcpyDeviceToHost, c.stream));
     HIF_CK(cudaStreamSynchronize(c.stream));
   });
+}
+
+int hif_trim(hif_handle h) {
+  if (!h) return HIF_ERR_ARG;
+  return guarded([&] {
+    h->e->sync();
+    h->e->arena_work[0].release();
+    h->e->arena_work[1].release();
+  });
+}
+
+int hif_memory(hif_handle h, long long* factor_bytes, long long* workspace_bytes) {
+  if (!h) return HIF_ERR_ARG;
+  if (factor_bytes) *factor_bytes = (long long)h->e->arena_factor.reserved();
+  if (workspace_bytes)
+    *workspace_bytes = (long long)(h->e->arena_work[0].reserved() + h->e->arena_work[1].reserved());
+  return HIF_OK;
 }
 
 int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, double* flops,

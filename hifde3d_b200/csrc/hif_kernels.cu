@@ -412,6 +412,25 @@ void launch_dgemm(const GemmDesc* d_desc, const int* d_tile_off, int nd, int tot
   }
 }
 
+__global__ void k_splitk_reduce(const SplitKDesc* __restrict__ descs) {
+  const SplitKDesc d = descs[blockIdx.y];
+  const long long mn = (long long)d.m * d.n;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < mn;
+       e += (long long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int q = 0; q < d.S; ++q) acc += d.P[e + q * mn];
+    const int i = (int)(e % d.m), j = (int)(e / d.m);
+    double* c = d.C + i + (long long)j * d.ldc;
+    *c = (d.beta == 0.0) ? d.alpha * acc : fma(d.beta, *c, d.alpha * acc);
+  }
+}
+
+void launch_splitk_reduce(const SplitKDesc* d_desc, int nd, cudaStream_t s) {
+  if (nd <= 0) return;
+  dim3 grid(64, nd);
+  k_splitk_reduce<<<grid, 256, 0, s>>>(d_desc);
+}
+
 // ===========================================================================
 // Gauss-Jordan sweep. For B = [A22 A21; A12 A11] (red first), eliminating
 // pivots 0..r-1 in place gives [A22^{-1} X; * A11 - A12 X] with
@@ -1220,20 +1239,29 @@ __global__ void __launch_bounds__(512) k_qr_panel(const QrDesc* __restrict__ des
     d.V[r + (long long)j * m] = v;
   }
   __syncthreads();
-  // Wd[i, j] = V[:, i]^T V[:, j] for i < j (rows >= k0 + j, where V[:, j] lives)
-  const int npair = kb * (kb - 1) / 2;
-  for (int pidx = warp; pidx < npair; pidx += nw) {
-    int j = 1, base = 0;
-    while (base + j <= pidx) { base += j; ++j; }
-    const int i = pidx - base;
-    double w = 0.0;
-    for (int r = k0 + j + lane; r < m; r += 32)
-      w = fma(d.V[r + (long long)i * m], d.V[r + (long long)j * m], w);
-    w = warp_sum(w);
-    if (lane == 0) Wd[i + j * kQrNB] = w;
+  // Wd = V^T V in one pass over the rows: lane c holds V[r, c]; the products
+  // with every other column come by shuffle. Warps add their partial sums in
+  // warp order (deterministic).
+  {
+    double acc[kQrNB];
+#pragma unroll
+    for (int i = 0; i < kQrNB; ++i) acc[i] = 0.0;
+    for (int r = k0 + warp; r < m; r += nw) {
+      const double v = (lane < kb) ? d.V[r + (long long)lane * m] : 0.0;
+#pragma unroll
+      for (int i = 0; i < kQrNB; ++i) acc[i] = fma(__shfl_sync(0xffffffffu, v, i), v, acc[i]);
+    }
+    for (int e = tid; e < kQrNB * kQrNB; e += nthr) Wd[e] = 0.0;
+    __syncthreads();
+    for (int w = 0; w < nw; ++w) {
+      if (warp == w) {
+#pragma unroll
+        for (int i = 0; i < kQrNB; ++i) Wd[i + lane * kQrNB] += acc[i];
+      }
+      __syncthreads();
+    }
   }
-  __syncthreads();
-  // T (dlarft, forward columnwise): T[j,j] = tau_j, T[0:j, j] = -tau_j T[0:j,0:j] w[0:j, j]
+  // T (forward, columnwise): T[j,j] = tau_j, T[0:j, j] = -tau_j T[0:j,0:j] Wd[0:j, j]
   for (int j = 0; j < kb; ++j) {
     if (tid < j) {
       double acc = 0.0;
@@ -1244,13 +1272,9 @@ __global__ void __launch_bounds__(512) k_qr_panel(const QrDesc* __restrict__ des
     for (int i = j + 1 + tid; i < kQrNB; i += nthr) T[i + j * kQrNB] = 0.0;
     __syncthreads();
   }
-  // Y = V T
-  for (long long e = tid; e < (long long)mt * kb; e += nthr) {
-    const int rr = (int)(e % mt), j = (int)(e / mt);
-    const int r = k0 + rr;
-    double acc = 0.0;
-    for (int l = 0; l <= j; ++l) acc = fma(d.V[r + (long long)l * m], T[l + j * kQrNB], acc);
-    d.Y[r + (long long)j * m] = acc;
+  for (int e = tid; e < kQrNB * kQrNB; e += nthr) {
+    const int i = e % kQrNB, j = e / kQrNB;
+    d.T[e] = (i < kb && j < kb) ? T[e] : 0.0;
   }
 }
 

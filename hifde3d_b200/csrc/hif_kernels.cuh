@@ -120,6 +120,17 @@ void launch_dgemm(const GemmDesc* d_desc, const int* d_tile_off, int nd, int tot
                   cudaStream_t s, int tile = 64);
 int dgemm_tiles(int m, int n, int tile = 64);
 
+// Split-K reduction: C = alpha * sum_{s < S} P_s + beta * C, P_s = P + s * m * n
+// (ld m), summed in order s = 0, 1, ... (deterministic).
+struct SplitKDesc {
+  double* C;
+  const double* P;
+  long long ldc;
+  int m, n, S;
+  double alpha, beta;
+};
+void launch_splitk_reduce(const SplitKDesc* d_desc, int nd, cudaStream_t s);
+
 // In-shared-memory Gauss-Jordan sweep of the first r pivots (n <= kSmallSweepN).
 constexpr int kSmallSweepN = 160;
 void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_status,
@@ -171,15 +182,15 @@ cudaError_t launch_id_group(const IdGroupDesc* d_desc, int nd, int group, double
 // Row compression of a tall face block before its pivoted QR: blocked
 // Householder QR (no pivoting) in 32-column panels. For panel [k0, k0+kb) the
 // panel kernel factors M[k0:m, k0:k0+kb) in place and writes the explicit
-// reflector block V (unit diagonal, zeros above) and Y = V T, T the upper
-// triangular factor of the compact WY form I - V T V^T, both m x 32 with ld m
-// (rows below k0 unused). The trailing columns are then updated by two batched
-// GEMMs: Wt = Y^T C, C -= V Wt.
+// reflector block V (unit diagonal, zeros above; m x 32, ld m, rows below k0
+// unused) and T, the upper triangular factor of the compact WY form
+// Q = I - V T V^T (32 x 32, ld 32). The trailing columns C are then updated by
+// batched GEMMs: Z = V^T C, Z = T^T Z, C -= V Z.
 constexpr int kQrNB = 32;
 struct QrDesc {
   double* M;  // m x n, ld m
   double* V;  // m x kQrNB, ld m
-  double* Y;  // m x kQrNB, ld m
+  double* T;  // kQrNB x kQrNB
   int m, n;
 };
 void launch_qr_panel(const QrDesc* d_desc, const int* d_active, int nact, int k0,

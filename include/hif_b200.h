@@ -193,6 +193,12 @@ enum hif_kernel_class {
 int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, double* flops,
                      double* bytes);
 
+/* Device memory held by the handle: the factor (kept until the next hif_factor or
+ * hif_destroy) and the factorization workspace (kept for reuse by later
+ * factorizations; hif_trim returns it to the device). */
+int hif_memory(hif_handle h, long long* factor_bytes, long long* workspace_bytes);
+int hif_trim(hif_handle h);
+
 /* Message of the last error on this thread. */
 const char* hif_last_error(void);
 
