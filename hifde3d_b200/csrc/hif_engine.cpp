@@ -244,8 +244,23 @@ struct Sources {
 // partial products and summed in a fixed order.
 template <class Timed>
 void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t stream, int cls,
-                Timed&& timed, int force_tile = 0) {
+                Timed&& timed, int force_tile = 0, bool mixed = false) {
   if (gin.empty()) return;
+  if (mixed) {  // split-TF32 tensor-core path (Schur-complement updates)
+    double fl = 0;
+    std::vector<int> toff(1, 0);
+    for (const GemmDesc& x : gin) {
+      fl += 2.0 * x.m * x.n * x.k;
+      toff.push_back(toff.back() + dgemm_tiles(x.m, x.n, 128));
+    }
+    if (toff.back() == 0) return;
+    GemmDesc* dg = tmp.add(upload(gin, stream));
+    int* dt = tmp.add(upload(toff, stream));
+    timed(HIF_KCLASS_GEMM_MIXED, fl, 0.0,
+          [&] { launch_gemm_mixed(dg, dt, (int)gin.size(), toff.back(), stream); }, 1);
+    HIF_CK(cudaGetLastError());
+    return;
+  }
   std::vector<GemmDesc> g;
   std::vector<SplitKDesc> red;
   double fl = 0;
@@ -314,7 +329,7 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
 // `timed(kernel class, flops, bytes, launch, launches)` wraps every launch.
 template <class Timed>
 void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t stream,
-                int* d_status, Timed&& timed) {
+                int* d_status, Timed&& timed, bool mixed = false) {
   std::vector<SweepDesc> small, large;
   int max_small = 0;
   for (const SweepDesc& d : descs) {
@@ -347,7 +362,7 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
   for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
   for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
     std::vector<int> active;
-    std::vector<GemmDesc> gd, rowg, colg;
+    std::vector<GemmDesc> gd, gmx, rowg, colg;
     for (int b = 0; b < nl; ++b) {
       const SweepDesc& d = large[b];
       if (d.r <= k0) continue;
@@ -391,8 +406,45 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
       rowp(k1, d.n);
       colp(0, k0);
       colp(k1, d.r);
+      // mixed precision: the A22 block (rows and columns < r) stays FP64; the
+      // Schur-complement updates (columns >= r: X; rows >= r: A12 side and T)
+      // go to the split-TF32 tensor-core kernel
       auto gemm = [&](int r0, int r1, int c0, int c1) {
         if (r1 <= r0 || c1 <= c0) return;
+        if (mixed && (c1 > d.r || r0 >= d.r)) {
+          if (r0 < d.r && c0 < d.r) {  // split at column r
+            const int cm = d.r;
+            GemmDesc lo{}, hi{};
+            lo.C = d.B + r0 + (long long)c0 * d.n;
+            lo.A = d.B + r0 + (long long)k0 * d.n;
+            lo.B = d.B + k0 + (long long)c0 * d.n;
+            lo.ldc = lo.lda = lo.ldb = d.n;
+            lo.m = r1 - r0;
+            lo.n = cm - c0;
+            lo.k = nbk;
+            lo.alpha = -1.0;
+            lo.beta = 1.0;
+            gd.push_back(lo);
+            hi = lo;
+            hi.C = d.B + r0 + (long long)cm * d.n;
+            hi.B = d.B + k0 + (long long)cm * d.n;
+            hi.n = c1 - cm;
+            gmx.push_back(hi);
+            return;
+          }
+          GemmDesc x{};
+          x.C = d.B + r0 + (long long)c0 * d.n;
+          x.A = d.B + r0 + (long long)k0 * d.n;
+          x.B = d.B + k0 + (long long)c0 * d.n;
+          x.ldc = x.lda = x.ldb = d.n;
+          x.m = r1 - r0;
+          x.n = c1 - c0;
+          x.k = nbk;
+          x.alpha = -1.0;
+          x.beta = 1.0;
+          gmx.push_back(x);
+          return;
+        }
         GemmDesc g{};
         g.C = d.B + r0 + (long long)c0 * d.n;
         g.A = d.B + r0 + (long long)k0 * d.n;
@@ -418,6 +470,7 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
     });
     gemm_batch(rowg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
     gemm_batch(gd, step, stream, HIF_KCLASS_GEMM, timed);
+    gemm_batch(gmx, step, stream, HIF_KCLASS_GEMM_MIXED, timed, 128, true);
     gemm_batch(colg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
     timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
       launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
@@ -459,6 +512,7 @@ class Engine {
   Arena arena_factor, arena_work[2];
   Arena* cur_work = &arena_work[0];
   bool keep_schur = false, verbose = false;
+  int precision = HIF_PRECISION_FP64;
   long long budget_mb = 0;
   std::map<int, std::vector<std::vector<int>>> replay;
   double t_total = 0, t_gather = 0, t_elim = 0, t_id = 0, t_host = 0, t_plan = 0;
@@ -660,7 +714,8 @@ class Engine {
   // A22^{-1}, X are written and B's trailing block holds A11 - A12 X.
   void run_sweep(const std::vector<SweepDesc>& descs, BufList& tmp) {
     sweep_blocks(descs, tmp, stream, d_status,
-                 [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); });
+                 [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); },
+                 precision == HIF_PRECISION_MIXED);
   }
 
   void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
@@ -2060,6 +2115,10 @@ int hif_set_option(hif_handle h, int option, long long value) {
     case HIF_OPT_KEEP_SCHUR: h->e->keep_schur = value != 0; return HIF_OK;
     case HIF_OPT_VERBOSE: h->e->verbose = value != 0; return HIF_OK;
     case HIF_OPT_MEM_BUDGET_MB: h->e->budget_mb = value; return HIF_OK;
+    case HIF_OPT_PRECISION:
+      if (value != HIF_PRECISION_FP64 && value != HIF_PRECISION_MIXED) return HIF_ERR_ARG;
+      h->e->precision = (int)value;
+      return HIF_OK;
     case HIF_OPT_ID_GROUP_MIN_N:
       if (value < 2) return HIF_ERR_ARG;
       h->e->kGroupMinN = (int)value;

@@ -432,6 +432,151 @@ void launch_splitk_reduce(const SplitKDesc* d_desc, int nd, cudaStream_t s) {
 }
 
 // ===========================================================================
+// Split-TF32 tensor-core GEMM (mixed precision). CTA tile 128 x 128, k step
+// 16; 8 warps as 2 (m) x 4 (n), warp tile 64 x 32 = 4 x 4 mma.m16n8k8 tiles.
+// Fragment layouts (PTX ISA, mma.m16n8k8 .tf32): with g = lane / 4 and
+// t = lane % 4, A regs hold (g, t), (g + 8, t), (g, t + 4), (g + 8, t + 4);
+// B regs hold (k = t, n = g), (k = t + 4, n = g); C holds (g, 2t), (g, 2t+1),
+// (g + 8, 2t), (g + 8, 2t + 1).
+// ===========================================================================
+constexpr int kMBM = 128, kMBN = 128, kMBK = 16;
+constexpr int kMStr = kMBK + 4;  // floats per smem row (conflict-free fragment loads)
+
+__device__ __forceinline__ unsigned tf32_of(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float* c, const unsigned* a, const unsigned* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(256, 1) k_gemm_mixed(const GemmDesc* __restrict__ descs,
+                                                       const int* __restrict__ tile_off, int nd) {
+  __shared__ unsigned Ahi[kMBM * kMStr], Alo[kMBM * kMStr];  // [m][k]
+  __shared__ unsigned Bhi[kMBN * kMStr], Blo[kMBN * kMStr];  // [n][k]
+  const int di = find_desc(tile_off, nd, blockIdx.x);
+  const GemmDesc g = descs[di];
+  const int local = blockIdx.x - tile_off[di];
+  const int tiles_m = (g.m + kMBM - 1) / kMBM;
+  const int m0 = (local % tiles_m) * kMBM, n0 = (local / tiles_m) * kMBN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  const int gq = lane >> 2, tq = lane & 3;
+
+  float acc[4][4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+
+  double ra[8], rb[8];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      int mm, kk;
+      if (g.transA == 0) { mm = e % kMBM; kk = e / kMBM; } else { mm = e / kMBK; kk = e % kMBK; }
+      const int gm = m0 + mm, gk = k0 + kk;
+      ra[q] = (gm < g.m && gk < g.k)
+                  ? ((g.transA == 0) ? g.A[gm + (long long)gk * g.lda] : g.A[gk + (long long)gm * g.lda])
+                  : 0.0;
+      int nn, kb;
+      if (g.transB == 0) { kb = e % kMBK; nn = e / kMBK; } else { nn = e % kMBN; kb = e / kMBN; }
+      const int gn = n0 + nn, gk2 = k0 + kb;
+      rb[q] = (gn < g.n && gk2 < g.k)
+                  ? ((g.transB == 0) ? g.B[gk2 + (long long)gn * g.ldb] : g.B[gn + (long long)gk2 * g.ldb])
+                  : 0.0;
+    }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      int mm, kk;
+      if (g.transA == 0) { mm = e % kMBM; kk = e / kMBM; } else { mm = e / kMBK; kk = e % kMBK; }
+      const float x = (float)ra[q];
+      const unsigned hi = tf32_of(x);
+      Ahi[mm * kMStr + kk] = hi;
+      Alo[mm * kMStr + kk] = tf32_of(x - __uint_as_float(hi));
+      int nn, kb;
+      if (g.transB == 0) { kb = e % kMBK; nn = e / kMBK; } else { nn = e % kMBN; kb = e / kMBN; }
+      const float y = (float)rb[q];
+      const unsigned yh = tf32_of(y);
+      Bhi[nn * kMStr + kb] = yh;
+      Blo[nn * kMStr + kb] = tf32_of(y - __uint_as_float(yh));
+    }
+  };
+
+  const int nk = (g.k + kMBK - 1) / kMBK;
+  if (nk > 0) load(0);
+  for (int t = 0; t < nk; ++t) {
+    __syncthreads();
+    store();
+    __syncthreads();
+    if (t + 1 < nk) load((t + 1) * kMBK);
+#pragma unroll
+    for (int k8 = 0; k8 < kMBK; k8 += 8) {
+      unsigned ah[4][4], al[4][4], bh[4][2], bl[4][2];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int r0 = wm + a * 16 + gq;
+        ah[a][0] = Ahi[r0 * kMStr + k8 + tq];
+        ah[a][1] = Ahi[(r0 + 8) * kMStr + k8 + tq];
+        ah[a][2] = Ahi[r0 * kMStr + k8 + tq + 4];
+        ah[a][3] = Ahi[(r0 + 8) * kMStr + k8 + tq + 4];
+        al[a][0] = Alo[r0 * kMStr + k8 + tq];
+        al[a][1] = Alo[(r0 + 8) * kMStr + k8 + tq];
+        al[a][2] = Alo[r0 * kMStr + k8 + tq + 4];
+        al[a][3] = Alo[(r0 + 8) * kMStr + k8 + tq + 4];
+      }
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int c0 = wn + b * 8 + gq;
+        bh[b][0] = Bhi[c0 * kMStr + k8 + tq];
+        bh[b][1] = Bhi[c0 * kMStr + k8 + tq + 4];
+        bl[b][0] = Blo[c0 * kMStr + k8 + tq];
+        bl[b][1] = Blo[c0 * kMStr + k8 + tq + 4];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          mma_tf32(acc[a][b], al[a], bh[b]);
+          mma_tf32(acc[a][b], ah[a], bl[b]);
+          mma_tf32(acc[a][b], ah[a], bh[b]);
+        }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int gm = m0 + wm + a * 16 + gq + ((c & 2) ? 8 : 0);
+        const int gn = n0 + wn + b * 8 + tq * 2 + (c & 1);
+        if (gm >= g.m || gn >= g.n) continue;
+        double* cp = g.C + gm + (long long)gn * g.ldc;
+        const double v = g.alpha * (double)acc[a][b][c];
+        *cp = (g.beta == 0.0) ? v : fma(g.beta, *cp, v);
+      }
+}
+
+void launch_gemm_mixed(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                       cudaStream_t s) {
+  if (total_tiles <= 0) return;
+  k_gemm_mixed<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
+}
+
+// ===========================================================================
 // Gauss-Jordan sweep. For B = [A22 A21; A12 A11] (red first), eliminating
 // pivots 0..r-1 in place gives [A22^{-1} X; * A11 - A12 X] with
 // X = A22^{-1} A21: the three outputs of the reference's Schur().

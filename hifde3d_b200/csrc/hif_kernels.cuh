@@ -131,6 +131,14 @@ struct SplitKDesc {
 };
 void launch_splitk_reduce(const SplitKDesc* d_desc, int nd, cudaStream_t s);
 
+// Mixed-precision variant of launch_dgemm for Schur-complement updates: the
+// FP64 operands are rounded to FP32 and split into two TF32 parts each
+// (x = hi + lo); hi*hi + hi*lo + lo*hi run on the tensor cores (mma.sync
+// m16n8k8, FP32 accumulation), then C (FP64) = beta C + alpha acc.
+// 128 x 128 x 16 tiles; tile offsets from dgemm_tiles(m, n, 128).
+void launch_gemm_mixed(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                       cudaStream_t s);
+
 // In-shared-memory Gauss-Jordan sweep of the first r pivots (n <= kSmallSweepN).
 constexpr int kSmallSweepN = 160;
 void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_status,

@@ -148,8 +148,15 @@ enum hif_option {
   HIF_OPT_VERBOSE = 2,       /* per-phase timings on stderr */
   HIF_OPT_MEM_BUDGET_MB = 3, /* refuse factorizations whose device memory exceeds this */
   HIF_OPT_PROFILE = 4,       /* time every launch with CUDA events (resets the counters) */
-  HIF_OPT_ID_GROUP_MIN_N = 5 /* faces with at least this many columns get a CTA group (default 512) */
+  HIF_OPT_ID_GROUP_MIN_N = 5, /* faces with at least this many columns get a CTA group (default 512) */
+  HIF_OPT_PRECISION = 6       /* HIF_PRECISION_FP64 (default) or HIF_PRECISION_MIXED */
 };
+/* Arithmetic of the factorization. MIXED: the Schur-complement updates of every
+ * elimination (the X and skeleton-row regions) run on the tensor cores as split-TF32
+ * products with FP32 accumulation; the pivoted QR, the row compression, the
+ * eliminated diagonal blocks (A22 and its inverse), the factor storage, the apply and
+ * the PCG residual stay FP64. */
+enum hif_precision { HIF_PRECISION_FP64 = 0, HIF_PRECISION_MIXED = 1 };
 int hif_set_option(hif_handle h, int option, long long value);
 
 /* Test hook: prescribe the ID column order of every face of one level (replay of
@@ -186,7 +193,8 @@ enum hif_kernel_class {
   HIF_KCLASS_COPY = 6,        /* compact copies of factor blocks */
   HIF_KCLASS_VECTOR = 7,      /* reductions / vector updates of the apply */
   HIF_KCLASS_QR = 8,          /* blocked Householder row compression of face blocks */
-  HIF_KCLASS_COUNT = 9
+  HIF_KCLASS_GEMM_MIXED = 9,  /* split-TF32 tensor-core Schur-complement updates */
+  HIF_KCLASS_COUNT = 10
 };
 /* Accumulated launches, milliseconds (CUDA events on the handle's stream), algorithmic
  * flops and bytes of one kernel class since HIF_OPT_PROFILE was last set. */
