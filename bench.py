@@ -216,49 +216,64 @@ def run_ours(args, rank: int, world: int):
         it, rr = f.solve_pcg_device(db.data_ptr(), dx.data_ptr(), 1, NC ** 3, 1e-10, 100)
         return int(it[0]), float(rr[0])
 
-    # warm-up
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # timed region: K steps, profiled launch by launch (CUDA events on the stream)
-    f.set_option(hb.OPT_PROFILE, 1)
-    clocks = ClockSampler(local)
-    barrier()
-    clocks.start()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    iters, rel, fac = [], [], []
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        it, rr = step()
-        iters.append(it)
-        rel.append(rr)
-        fac.append(f.factor_stats()["total_s"])
-    t_end.record(stream)
-    t_end.synchronize()
-    barrier()
-    clk = clocks.stop()
-    ms_total = t_start.elapsed_time(t_end)
-    kst = f.kernel_stats()
-    f.set_option(hb.OPT_PROFILE, 0)
+    def measure(prec):
+        """W warm-up steps, then K timed steps (CUDA events on the engine stream,
+        every launch profiled), then solve-only timings with the resident factor."""
+        f.set_option(hb.OPT_PRECISION, prec)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        f.set_option(hb.OPT_PROFILE, 1)
+        clocks = ClockSampler(local)
+        barrier()
+        clocks.start()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        iters, rel, fac = [], [], []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            it, rr = step()
+            iters.append(it)
+            rel.append(rr)
+            fac.append(f.factor_stats()["total_s"])
+        t_end.record(stream)
+        t_end.synchronize()
+        barrier()
+        clk = clocks.stop()
+        ms_total = t_start.elapsed_time(t_end)
+        kst = f.kernel_stats()
+        f.set_option(hb.OPT_PROFILE, 0)
+        solve_ms = []
+        for _ in range(max(3, args.steps)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            f.solve_pcg_device(db.data_ptr(), dx.data_ptr(), 1, NC ** 3, 1e-10, 100)
+            e1.record(stream)
+            e1.synchronize()
+            solve_ms.append(e0.elapsed_time(e1))
+        return {"ms_step": ms_total / args.steps, "factor_s": float(np.mean(fac)),
+                "solve_ms": float(np.median(solve_ms)), "pcg_iters": iters[-1],
+                "pcg_relres": rel[-1], "clocks": clk, "kst": kst}
 
-    # solve-only throughput with the resident factor
-    solve_ms = []
-    for _ in range(max(3, args.steps)):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        f.solve_pcg_device(db.data_ptr(), dx.data_ptr(), 1, NC ** 3, 1e-10, 100)
-        e1.record(stream)
-        e1.synchronize()
-        solve_ms.append(e0.elapsed_time(e1))
+    runs = {}
+    precs = {"fp64": [hb.PRECISION_FP64], "mixed": [hb.PRECISION_MIXED],
+             "both": [hb.PRECISION_FP64, hb.PRECISION_MIXED]}[args.precision]
+    for prec in precs:
+        runs[prec] = measure(prec)
+    head_prec = precs[-1]
+    head = runs[head_prec]
+    ms_total = head["ms_step"] * args.steps
+    kst = head["kst"]
+    clk = head["clocks"]
+    iters, rel, fac = [head["pcg_iters"]], [head["pcg_relres"]], [head["factor_s"]]
+    solve_ms = [head["solve_ms"]]
 
     # end to end through the public API with host buffers
     e2e_s, it_e2e, rr_e2e = float("nan"), None, None
@@ -298,7 +313,16 @@ def run_ours(args, rank: int, world: int):
     if os.path.exists(pk_path):
         with open(pk_path) as fh:
             peaks = json.load(fh)
-    if k["flops"] > 0:
+    if k["flops"] > 0 and dom == "gemm_mixed":
+        achieved = k["flops"] / max(k["launches"], 1) / (per_launch_ms * 1e-3) / 1e12
+        tf32 = peaks.get("bf16_tflops", 1590.0) / 2
+        roof = {"bound": "tensor", "kernel_class": dom, "achieved": achieved, "peak": tf32,
+                "unit": "TFLOP/s", "frac": achieved / tf32, "traffic": traffic,
+                "launches": k["launches"], "avg_launch_ms": per_launch_ms,
+                "peak_source": "TF32 dense rate taken as half of MEASURED_PEAKS.json bf16_tflops; "
+                               "achieved counts each FP64-equivalent product once (split-TF32 "
+                               "issues three tensor products per product)"}
+    elif k["flops"] > 0:
         achieved = k["flops"] / max(k["launches"], 1) / (per_launch_ms * 1e-3) / 1e12
         roof = {"bound": "fp64", "kernel_class": dom, "achieved": achieved, "peak": peak_fp64,
                 "unit": "TFLOP/s", "frac": achieved / peak_fp64 if peak_fp64 else None,
@@ -338,10 +362,13 @@ def run_ours(args, rank: int, world: int):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64" if head_prec == hb.PRECISION_FP64 else "f64+split-tf32",
         "data": "synthetic",
         "config": {"workload": f"hif factor + pcg(1e-10), n={n} (N={N}, {dofs(n)} DOFs), "
-                               f"face a=exp(GRF ell=1/16 sigma=1), eps={eps}, P=4, FP64",
+                               f"face a=exp(GRF ell=1/16 sigma=1), eps={eps}, P=4, "
+                               + ("FP64" if head_prec == hb.PRECISION_FP64 else
+                                  "mixed: split-TF32 tensor-core Schur updates, FP64 QR / "
+                                  "diagonal blocks / residual"),
                    "parallelism": f"replicas x{world}", "l2_flush": "256 MB write per step",
                    "inputs": "coefficients and rhs resident in HBM"},
         "factor_s": float(np.mean(fac)),
@@ -359,6 +386,17 @@ def run_ours(args, rank: int, world: int):
         "gpu_launches": int(sum(v["launches"] for v in kst.values()) / args.steps),
         "cpu_baseline": cpu,
     }
+    for name, prec in (("fp64", hb.PRECISION_FP64), ("mixed", hb.PRECISION_MIXED)):
+        if prec in runs:
+            r = runs[prec]
+            line[name] = {"steps_per_s": 1e3 / r["ms_step"], "ms_per_step": r["ms_step"],
+                          "factor_s": r["factor_s"], "solve_ms": r["solve_ms"],
+                          "solves_per_s": 1e3 / r["solve_ms"], "pcg_iters": r["pcg_iters"],
+                          "pcg_relres": r["pcg_relres"]}
+    if len(runs) == 2:
+        line["mixed_vs_fp64"] = {
+            "step_speedup": runs[hb.PRECISION_FP64]["ms_step"] / runs[hb.PRECISION_MIXED]["ms_step"],
+            "factor_speedup": runs[hb.PRECISION_FP64]["factor_s"] / runs[hb.PRECISION_MIXED]["factor_s"]}
     print(json.dumps(line))
     f.close()
 
@@ -373,6 +411,7 @@ def main():
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling)")
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

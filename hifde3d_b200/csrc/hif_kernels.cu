@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
   const int local = blockIdx.x - tile_off[di];
   const int tiles_m = (g.m + kLBM - 1) / kLBM;
   const int m0 = (local % tiles_m) * kLBM, n0 = (local / tiles_m) * kLBN;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int tid = threadIdx.x;
 
   auto issue = [&](int stage, int k0) {
     double* as = As + stage * kLBK * kLAStride;
@@ -338,11 +338,18 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
     }
   };
 
-  double acc[8][8];
+  // FP64 tensor cores: mma.sync m8n8k4 (DMMA). 8 warps as 2 (m) x 4 (n), warp
+  // tile 64 x 32 = 8 x 4 MMA tiles. Fragments (PTX ISA, m8n8k4 .f64): with
+  // g = lane / 4, t = lane % 4, A holds (row g, k t), B holds (k t, col g),
+  // C holds (row g, cols 2t and 2t + 1).
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  const int gq = lane >> 2, tq = lane & 3;
+  double acc[8][4][2];
 #pragma unroll
   for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 
   double* Cs = lsm + kLStages * kLBK * (kLAStride + kLBStride);  // [col][row], 128 x 128
   const bool prefetch_c = g.beta != 0.0;
@@ -368,32 +375,39 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
     const double* as = As + (t % kLStages) * kLBK * kLAStride;
     const double* bs = Bs + (t % kLStages) * kLBK * kLBStride;
 #pragma unroll
-    for (int kk = 0; kk < kLBK; ++kk) {
-      double av[8], bv[8];
+    for (int k4 = 0; k4 < kLBK; k4 += 4) {
+      double af[8], bf[4];
 #pragma unroll
-      for (int a = 0; a < 8; ++a) av[a] = as[kk * kLAStride + tx + 16 * a];
+      for (int a = 0; a < 8; ++a) af[a] = as[(k4 + tq) * kLAStride + wm + a * 8 + gq];
 #pragma unroll
-      for (int b = 0; b < 8; ++b) bv[b] = bs[kk * kLBStride + ty + 16 * b];
+      for (int b = 0; b < 4; ++b) bf[b] = bs[(k4 + tq) * kLBStride + wn + b * 8 + gq];
 #pragma unroll
       for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        for (int b = 0; b < 4; ++b)
+          asm volatile(
+              "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+              : "+d"(acc[a][b][0]), "+d"(acc[a][b][1])
+              : "d"(af[a]), "d"(bf[b]));
     }
   }
   cp_async_wait<0>();
   __syncthreads();
 #pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    const int gn = n0 + ty + 16 * b;
-    if (gn >= g.n) continue;
+  for (int a = 0; a < 8; ++a) {
+    const int gm = m0 + wm + a * 8 + gq;
+    if (gm >= g.m) continue;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      const int gm = m0 + tx + 16 * a;
-      if (gm >= g.m) continue;
-      double* c = g.C + gm + (long long)gn * g.ldc;
-      const double v = g.alpha * acc[a][b];
-      *c = prefetch_c ? fma(g.beta, Cs[(ty + 16 * b) * kLBM + tx + 16 * a], v) : v;
-    }
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int cl = wn + b * 8 + tq * 2 + c;
+        const int gn = n0 + cl;
+        if (gn >= g.n) continue;
+        double* cp = g.C + gm + (long long)gn * g.ldc;
+        const double v = g.alpha * acc[a][b][c];
+        *cp = prefetch_c ? fma(g.beta, Cs[cl * kLBM + wm + a * 8 + gq], v) : v;
+      }
   }
 }
 
