@@ -179,6 +179,112 @@ def fp64_gemm_peak(torch, dev):
     return best
 
 
+# ---------------------------------------------------------------------------
+# serving: operators of n in {32, 48, 64, 96} resident on the GPU, Poisson arrivals
+# ---------------------------------------------------------------------------
+SERVE_SIZES = (32, 48, 64, 96)
+
+
+def serving_schedule(nreq: int, rate: float, seed: int = 5):
+    """Seeded arrivals: (time s, kind, size index or op slot, nrhs, rhs seed).
+    70 % solves of 1-32 right-hand sides against resident operators, 30 % new
+    factorizations of a random pool size."""
+    from hifde3d_b200 import synth
+    u = synth.uniform(seed, 5 * nreq).reshape(nreq, 5)
+    t = np.cumsum(-np.log(1.0 - u[:, 0]) / rate)
+    out = []
+    for q in range(nreq):
+        kind = "factor" if u[q, 1] < 0.3 else "solve"
+        out.append((float(t[q]), kind, int(u[q, 2] * 1e6), 1 + int(u[q, 3] * 32), 1000 + q))
+    return out
+
+
+def run_serving(hb, synth, prec: int, nreq: int, rate: float, budget_gb: float = 120.0,
+                max_resident: int = 12):
+    """One pass of the serving workload at one precision; latencies from the
+    server's own submit/complete clock."""
+    srv = hb.Server(budget_bytes=int(budget_gb * (1 << 30)), max_active_solves=64,
+                    factor_workers=2)
+    sched = serving_schedule(nreq, rate)
+    next_op = [0]
+    resident = []  # (op id, n) usable as solve targets, oldest first
+    releases = []
+    fids, sids = [], []
+
+    def new_op(n):
+        op = next_op[0]
+        next_op[0] += 1
+        N = n - 1
+        ax, ay, az = synth.face_coefficients_lognormal(N, 100 + op, 1.0)
+        V = np.zeros((n + 1,) * 3)
+        return op, srv.submit_factor(op, N, ax, ay, az, V, eps=1e-6, precision=prec)
+
+    # warm pool: one operator of each size, ready before the clock starts
+    for n in SERVE_SIZES:
+        op, rid = new_op(n)
+        r = srv.wait(rid)
+        if r["status"] != hb.HIF_OK:
+            raise RuntimeError(f"serving warm pool: {r}")
+        resident.append((op, n))
+    rhs_cache = {}
+
+    def rhs(n, nrhs, seed):
+        key = (n, nrhs, seed % 8)
+        if key not in rhs_cache:
+            rhs_cache[key] = synth.dof_vector(n - 1, seed % 8, nrhs)
+        return rhs_cache[key]
+
+    t0 = time.perf_counter()
+    for (ta, kind, pick, nrhs, seed) in sched:
+        dt = ta - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        if kind == "factor":
+            n = SERVE_SIZES[pick % len(SERVE_SIZES)]
+            if len(resident) >= max_resident:
+                old, _ = resident.pop(0)
+                th = threading.Thread(target=srv.release, args=(old,))
+                th.start()
+                releases.append(th)
+            op, rid = new_op(n)
+            fids.append((rid, n))
+            resident.append((op, n))
+        else:
+            op, n = resident[pick % len(resident)]
+            sids.append((srv.submit_solve(op, rhs(n, nrhs, seed), tol=1e-10, maxit=100), n,
+                         nrhs))
+    lat_s, lat_f, iters, worst, rhs_total, fails = [], [], [], 0.0, 0, 0
+    for rid, n, nrhs in sids:
+        r = srv.wait(rid)
+        if r["status"] != hb.HIF_OK:
+            fails += 1
+            continue
+        lat_s.append(r["latency_ms"])
+        iters.append(r["iters"])
+        worst = max(worst, r["relres"])
+        rhs_total += nrhs
+    for rid, n in fids:
+        r = srv.wait(rid)
+        if r["status"] != hb.HIF_OK:
+            fails += 1
+            continue
+        lat_f.append(r["latency_ms"])
+    makespan = time.perf_counter() - t0
+    for th in releases:
+        th.join()
+    st = srv.stats()
+    srv.close()
+    pct = lambda v, q: float(np.percentile(v, q)) if v else None  # noqa: E731
+    return {"requests": nreq, "solves": len(lat_s), "factorizations": len(lat_f),
+            "failed": fails, "makespan_s": makespan,
+            "solves_per_s": len(lat_s) / makespan, "rhs_per_s": rhs_total / makespan,
+            "solve_p50_ms": pct(lat_s, 50), "solve_p99_ms": pct(lat_s, 99),
+            "factor_p50_ms": pct(lat_f, 50), "factor_p99_ms": pct(lat_f, 99),
+            "pcg_iters_max": max(iters) if iters else None, "relres_max": worst,
+            "server_iterations": st["iterations"], "batched_launches": st["batched_launches"],
+            "peak_resident_ops": max_resident}
+
+
 def run_ours(args, rank: int, world: int):
     import torch
     import torch.distributed as dist
@@ -393,6 +499,19 @@ def run_ours(args, rank: int, world: int):
                           "factor_s": r["factor_s"], "solve_ms": r["solve_ms"],
                           "solves_per_s": 1e3 / r["solve_ms"], "pcg_iters": r["pcg_iters"],
                           "pcg_relres": r["pcg_relres"]}
+    if not args.no_serving:
+        serve = {}
+        for name, prec in (("fp64", hb.PRECISION_FP64), ("mixed", hb.PRECISION_MIXED)):
+            if prec in runs:
+                serve[name] = run_serving(hb, synth, prec, args.serve_requests, args.serve_rate)
+        line["serving"] = {
+            "workload": (f"{args.serve_requests} requests, Poisson arrivals at "
+                         f"{args.serve_rate}/s (seed 5): 30% factorizations of n in "
+                         f"{list(SERVE_SIZES)} (a = exp(N(0,1)) per face, per-operator seed), "
+                         "70% PCG solves to 1e-10 of 1-32 right-hand sides against resident "
+                         "operators; HBM budget 120 GB; at most 12 resident operators (oldest "
+                         "released); 64 solve slots batched per iteration"),
+            **serve}
     if len(runs) == 2:
         line["mixed_vs_fp64"] = {
             "step_speedup": runs[hb.PRECISION_FP64]["ms_step"] / runs[hb.PRECISION_MIXED]["ms_step"],
@@ -412,6 +531,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling)")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
+    ap.add_argument("--serve-requests", type=int, default=80)
+    ap.add_argument("--serve-rate", type=float, default=8.0, help="arrivals per second")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -82,6 +82,13 @@ _SIGNATURES = {
     "hif_interp_decomp": [_dp, _i, _i, _ll, _d, _dp, _ip, _ip, _ip],
     "hif_pivoted_qr": [_dp, _i, _i, _ll, _ip],
     "hif_triangular_solve": [_dp, _i, _ll, _dp, _i, _ll],
+    "hif_server_create": [_ll, _i, _i, ctypes.POINTER(_p)],
+    "hif_server_destroy": [_p],
+    "hif_server_submit_factor": [_p, _i, _i, _i, _d, _i, _i, _d, _dp, _dp, _dp, _dp, _llp],
+    "hif_server_submit_solve": [_p, _i, _dp, _i, _d, _i, _dp, _llp],
+    "hif_server_wait": [_p, _ll, _ip, _ip, _dp, _dp],
+    "hif_server_release": [_p, _i],
+    "hif_server_stats": [_p, _llp, _llp, _llp, _llp, _llp],
     "hif_partition_cell": [_i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
                            _ip, _ip, _ip, _ip],
     "hif_partition_face": [_i, _i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
@@ -218,14 +225,25 @@ class HIFFactor:
         return y
 
     def solve_pcg(self, b: np.ndarray, tol: float = 1e-10, maxit: int = 200):
-        """PCG on A x = b preconditioned by the inverse apply. Returns (x, iters, relres)."""
-        b = np.ascontiguousarray(b, dtype=np.float64)
-        x = np.zeros_like(b)
-        it = np.zeros(1, np.int32)
-        rr = np.zeros(1)
-        _check(lib().hif_solve_pcg(self._h, _dptr(b), _dptr(x), 1, b.size, tol, maxit,
+        """PCG on A x = b preconditioned by the inverse apply. Returns (x, iters, relres);
+        for b of shape (NC^3, nrhs) iters and relres are per right-hand side."""
+        b = np.asarray(b, dtype=np.float64)
+        if b.ndim == 1:
+            b = np.ascontiguousarray(b)
+            x = np.zeros_like(b)
+            it = np.zeros(1, np.int32)
+            rr = np.zeros(1)
+            _check(lib().hif_solve_pcg(self._h, _dptr(b), _dptr(x), 1, b.size, tol, maxit,
+                                       _iptr(it), _dptr(rr)))
+            return x, int(it[0]), float(rr[0])
+        b = np.asfortranarray(b)
+        n, nrhs = b.shape
+        x = np.zeros((n, nrhs), order="F")
+        it = np.zeros(nrhs, np.int32)
+        rr = np.zeros(nrhs)
+        _check(lib().hif_solve_pcg(self._h, _dptr(b), _dptr(x), nrhs, n, tol, maxit,
                                    _iptr(it), _dptr(rr)))
-        return x, int(it[0]), float(rr[0])
+        return x, it, rr
 
     def solve_pcg_device(self, db: int, dx: int, nrhs: int, ld: int, tol: float, maxit: int):
         it = np.zeros(nrhs, np.int32)
@@ -312,6 +330,90 @@ class HIFFactor:
         d = {k: v.value for k, v in zip(keys, vals)}
         d["device_bytes"] = nb.value
         return d
+
+
+class Server:
+    """Many factored operators resident on one GPU, with iteration-level batched
+    PCG solves across them (``hif_server_*`` in include/hif_b200.h).
+
+    ``submit_factor`` / ``submit_solve`` return a request id at once; ``wait``
+    blocks until the request ends and returns a dict with ``status``, ``iters``,
+    ``relres``, ``latency_ms`` and, for solves, ``x`` (NC^3 x nrhs, float64,
+    column-major like the right-hand sides)."""
+
+    def __init__(self, budget_bytes: int, max_active_solves: int = 64, factor_workers: int = 2):
+        h = _p()
+        _check(lib().hif_server_create(int(budget_bytes), int(max_active_solves),
+                                       int(factor_workers), ctypes.byref(h)))
+        self._h = h
+        self._out = {}
+        self._n3 = {}
+
+    def close(self):
+        if self._h:
+            _check(lib().hif_server_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit_factor(self, op_id: int, N: int, ax, ay, az, V, P: int = 4, eps: float = 1e-6,
+                      precision: int = 0, partition: int = 0, h: float | None = None) -> int:
+        arrs = [np.ascontiguousarray(np.asarray(x, np.float64).ravel(order="F"))
+                for x in (ax, ay, az, V)]
+        for x in arrs:
+            if x.size != (N + 2) ** 3:
+                raise HIFError(HIF_ERR_ARG, "face arrays must be (N+2)^3")
+        rid = _ll()
+        hstep = 1.0 / (N + 1) if h is None else float(h)
+        _check(lib().hif_server_submit_factor(self._h, int(op_id), N, P, float(eps),
+                                              int(partition), int(precision), hstep,
+                                              *[_dptr(x) for x in arrs], ctypes.byref(rid)))
+        self._n3[int(op_id)] = (N + 1) ** 3
+        self._out[rid.value] = (None, arrs)  # inputs stay alive until the copy
+        return rid.value
+
+    def submit_solve(self, op_id: int, b, tol: float = 1e-10, maxit: int = 100) -> int:
+        n3 = self._n3[int(op_id)]
+        bb = np.asarray(b, np.float64)
+        nrhs = 1 if bb.ndim == 1 else bb.shape[1]
+        bf = np.ascontiguousarray(bb.reshape(n3, nrhs, order="F").T).ravel()
+        x = np.zeros(n3 * nrhs)
+        rid = _ll()
+        _check(lib().hif_server_submit_solve(self._h, int(op_id), _dptr(bf), nrhs, float(tol),
+                                             int(maxit), _dptr(x), ctypes.byref(rid)))
+        self._out[rid.value] = (x, (nrhs, bb.ndim))
+        return rid.value
+
+    def wait(self, request_id: int) -> dict:
+        st, it = _i(), _i()
+        rr, lat = _d(), _d()
+        code = lib().hif_server_wait(self._h, int(request_id), ctypes.byref(st), ctypes.byref(it),
+                                     ctypes.byref(rr), ctypes.byref(lat))
+        _check(code)
+        x, meta = self._out.pop(int(request_id), (None, None))
+        res = {"status": st.value, "iters": it.value, "relres": rr.value,
+               "latency_ms": lat.value}
+        if st.value != HIF_OK:
+            res["error"] = lib().hif_last_error().decode()
+        if x is not None:
+            nrhs, ndim = meta
+            xm = x.reshape(nrhs, -1).T
+            res["x"] = xm[:, 0].copy() if ndim == 1 else np.asfortranarray(xm)
+        return res
+
+    def release(self, op_id: int) -> None:
+        _check(lib().hif_server_release(self._h, int(op_id)))
+        self._n3.pop(int(op_id), None)
+
+    def stats(self) -> dict:
+        vals = [_ll() for _ in range(5)]
+        _check(lib().hif_server_stats(self._h, *[ctypes.byref(v) for v in vals]))
+        keys = ("device_bytes", "resident_ops", "completed", "iterations", "batched_launches")
+        return {k: v.value for k, v in zip(keys, vals)}
 
 
 def SetupStencil(factor: HIFFactor, N: int, h: float, A: np.ndarray, V: np.ndarray) -> None:

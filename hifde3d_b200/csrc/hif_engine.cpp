@@ -25,9 +25,13 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <list>
 #include <map>
+#include <mutex>
 #include <atomic>
 #include <memory>
 #include <string>
@@ -210,6 +214,8 @@ struct StepData {
 // One launch of the apply sweep.
 struct ApplyLaunch {
   double bytes = 0;  // matrix bytes streamed per right-hand-side group
+  long long key = 0;  // stage order shared by all operators (batched solves)
+  std::vector<GemvDesc> hdesc;  // host copy of the descriptors
   int type = 0;  // 0 gemv, 1 reduce-scatter
   GemvDesc* d_desc = nullptr;
   int* d_toff = nullptr;
@@ -1524,8 +1530,10 @@ class Engine {
   // ---- Apply (src/Factor.cpp:992-1081) ------------------------------------
   // Builds the launch list of one sweep. Matrices: X (r x s, ld r),
   // W (k x r, ld k), A22 / A22^{-1} (r x r, ld r).
+  long long plan_key = 0;  // stage key for the next launches added to a plan
   void add_gemv(ApplyPlan& plan, const StepData& st, int which, int trans, bool in_red,
                 bool out_red, double alpha, int mode, int in_vec, int out_vec) {
+    const long long my_key = plan_key++;  // taken even when the launch is empty
     std::vector<GemvDesc> dd;
     std::vector<int> toff(1, 0);
     double mbytes = 0;
@@ -1570,10 +1578,13 @@ class Engine {
     l.out_vec = out_vec;
     l.d_toff = plan.bufs.add(upload(toff, stream));
     l.d_desc = plan.bufs.add(upload(dd, stream));
+    l.hdesc = dd;
+    l.key = my_key;
     plan.launches.push_back(l);
   }
 
   void add_reduce(ApplyPlan& plan, const StepData& st, double alpha, int vec) {
+    const long long my_key = plan_key++;
     // every skeleton DOF of the level with its contribution slots, in block order
     std::vector<int> head(n3, -1), dof, cnt;
     for (size_t b = 0; b < st.blocks.size(); ++b) {
@@ -1609,6 +1620,7 @@ class Engine {
     l.ndof = dof.size();
     l.alpha = alpha;
     l.out_vec = vec;
+    l.key = my_key;
     plan.launches.push_back(l);
   }
 
@@ -1629,28 +1641,41 @@ class Engine {
     // index steps by (level, kind)
     std::vector<const StepData*> sch(L, nullptr), skl(L, nullptr);
     for (const StepData& st : steps) (st.skel ? skl : sch)[st.level] = &st;
+    // Stage keys: forward sweeps (segment 0, level ascending), diagonal
+    // (segment 1), backward sweeps (segment 2, level descending); within a
+    // stage the launch order. Every operator's own launch order is increasing in
+    // key, so launches of several operators with equal keys can share a launch.
+    auto key = [](int seg, int lev, int sub) {
+      return ((long long)seg << 32) | ((long long)lev << 8) | sub;
+    };
     // inverse
     {
       ApplyPlan& p = plan_inv;
       for (int l = 0; l < L - 1; ++l) {
         if (sch[l]) {
+          plan_key = key(0, l, 0);
           add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 0, 0);
           add_reduce(p, *sch[l], -1.0, 0);
         }
         if (skl[l]) {
+          plan_key = key(0, l, 4);
           add_gemv(p, *skl[l], 1, 1, false, true, -1.0, 0, 0, 0);
           add_gemv(p, *skl[l], 0, 1, true, false, -1.0, 0, 0, 0);
         }
       }
       for (int l = 0; l < L; ++l) {
+        plan_key = key(1, l, 0);
         if (sch[l]) add_gemv(p, *sch[l], 3, 0, true, true, 1.0, 2, 0, 1);
+        plan_key = key(1, l, 4);
         if (skl[l]) add_gemv(p, *skl[l], 3, 0, true, true, 1.0, 2, 0, 1);
       }
       for (int l = L - 2; l >= 0; --l) {
         if (skl[l]) {
+          plan_key = key(2, 255 - l, 0);
           add_gemv(p, *skl[l], 0, 0, false, true, -1.0, 0, 1, 1);
           add_gemv(p, *skl[l], 1, 0, true, false, -1.0, 0, 1, 1);
         }
+        plan_key = key(2, 255 - l, 4);
         if (sch[l]) add_gemv(p, *sch[l], 0, 0, false, true, -1.0, 0, 1, 1);
       }
     }
@@ -2436,3 +2461,5 @@ int hif_partition_face(int N, int P, int level, int ci, int cj, int ck, int face
 }
 
 }  // extern "C"
+
+#include "hif_server.inl"

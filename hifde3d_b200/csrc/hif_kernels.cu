@@ -1498,14 +1498,16 @@ __device__ __forceinline__ void gemv_emit(const GemvDesc& g, int i, int c, doubl
   else u_out[g.out_idx[i] + (long long)c * ldu] = g.alpha * y;
 }
 
-__global__ void __launch_bounds__(256) k_gemv(const GemvDesc* __restrict__ descs,
-                                              const int* __restrict__ tile_off, int nd,
-                                              const double* __restrict__ u_in,
-                                              double* __restrict__ u_out, int nrhs,
-                                              long long ldu, long long contrib_ld) {
-  const int di = find_desc(tile_off, nd, blockIdx.x);
-  const GemvDesc g = descs[di];
-  const int local = blockIdx.x - tile_off[di];
+__device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
+                                          const double* __restrict__ u_in_k,
+                                          double* __restrict__ u_out_k, int nrhs_k,
+                                          long long ldu_k, long long contrib_ld_k) {
+  GemvDesc g = g0;
+  const double* u_in = g.uin ? g.uin : u_in_k;
+  double* u_out = g.uin ? g.uout : u_out_k;
+  const int nrhs = g.uin ? g.nrhs : nrhs_k;
+  const long long ldu = g.uin ? g.ldu : ldu_k;
+  const long long contrib_ld = g.uin ? g.cld : contrib_ld_k;
   __shared__ double xs[kXChunk][kRhsGroup];
   const int tid = threadIdx.x;
   if (g.trans == 0) {
@@ -1573,6 +1575,51 @@ __global__ void __launch_bounds__(256) k_gemv(const GemvDesc* __restrict__ descs
       }
     }
   }
+}
+
+__global__ void __launch_bounds__(256) k_gemv(const GemvDesc* __restrict__ descs,
+                                              const int* __restrict__ tile_off, int nd,
+                                              const double* __restrict__ u_in,
+                                              double* __restrict__ u_out, int nrhs,
+                                              long long ldu, long long contrib_ld) {
+  const int di = find_desc(tile_off, nd, blockIdx.x);
+  gemv_tile(descs[di], blockIdx.x - tile_off[di], u_in, u_out, nrhs, ldu, contrib_ld);
+}
+
+__global__ void __launch_bounds__(256) k_gemv_seg(const GemvSeg* __restrict__ segs,
+                                                  const int* __restrict__ seg_off, int nseg) {
+  const int si = find_desc(seg_off, nseg, blockIdx.x);
+  const GemvSeg sg = segs[si];
+  const int t = blockIdx.x - seg_off[si];
+  const int di = find_desc(sg.toff, sg.nd, t);
+  gemv_tile(sg.desc[di], t - sg.toff[di], nullptr, nullptr, 0, 0, 0);
+}
+
+void launch_gemv_seg(const GemvSeg* d_segs, const int* d_seg_off, int nseg, int total_tiles,
+                     cudaStream_t s) {
+  if (total_tiles <= 0) return;
+  k_gemv_seg<<<total_tiles, 256, 0, s>>>(d_segs, d_seg_off, nseg);
+}
+
+__global__ void k_reduce_seg(const ReduceSeg* __restrict__ segs, const int* __restrict__ seg_off,
+                             int nseg) {
+  const int total = seg_off[nseg];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int si = find_desc(seg_off, nseg, t);
+    const ReduceSeg sg = segs[si];
+    const int e = t - seg_off[si];
+    const int d = e % sg.ndof, c = e / sg.ndof;
+    double sum = 0.0;
+    for (int q = sg.off[d]; q < sg.off[d + 1]; ++q) sum += sg.contrib[sg.slot[q] + (long long)c * sg.cld];
+    sg.u[sg.dof[d] + (long long)c * sg.ldu] += sg.alpha * sum;
+  }
+}
+
+void launch_reduce_seg(const ReduceSeg* d_segs, const int* d_seg_off, int nseg, int total,
+                       cudaStream_t s) {
+  if (total <= 0) return;
+  const int blocks = std::min((total + 255) / 256, 4096);
+  k_reduce_seg<<<blocks, 256, 0, s>>>(d_segs, d_seg_off, nseg);
 }
 
 void launch_gemv(const GemvDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,

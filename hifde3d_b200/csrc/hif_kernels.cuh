@@ -96,7 +96,37 @@ struct GemvDesc {
   int trans;            // 0: y = M x (len m), 1: y = M^T x (len n)
   double alpha;
   int mode;             // 0: u_out[out] += alpha y; 1: contrib = y; 2: u_out[out] = alpha y
+  // Optional per-descriptor vectors (batched solves of several operators in one
+  // launch); when uin is null the launch's vectors and sizes apply.
+  const double* uin;
+  double* uout;
+  int nrhs;
+  long long ldu, cld;
 };
+
+// A batch of descriptor arrays (one per request) in one launch: tiles are
+// counted over segments by seg_off (prefix, device), then within a segment by
+// its own tile offsets.
+struct GemvSeg {
+  const GemvDesc* desc;
+  const int* toff;
+  int nd;
+};
+void launch_gemv_seg(const GemvSeg* d_segs, const int* d_seg_off, int nseg, int total_tiles,
+                     cudaStream_t s);
+struct ReduceSeg {
+  const int* dof;
+  const int* off;
+  const int* slot;
+  const double* contrib;
+  double* u;
+  long long cld, ldu;
+  int ndof, nrhs;
+  double alpha;
+};
+// d_seg_off: prefix over segments of ndof * nrhs.
+void launch_reduce_seg(const ReduceSeg* d_segs, const int* d_seg_off, int nseg, int total,
+                       cudaStream_t s);
 
 struct CopyDesc {
   const double* src;

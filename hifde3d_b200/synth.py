@@ -124,3 +124,13 @@ def face_coefficients_blocks(N: int, seed: int, nblk: int = 8, lo: float = -3.0,
     ay = hm(node[:-1, :-1, :-1], node[:-1, 1:, :-1])
     az = hm(node[:-1, :-1, :-1], node[:-1, :-1, 1:])
     return ax, ay, az
+
+
+def face_coefficients_lognormal(N: int, seed: int, sigma: float = 1.0):
+    """Face coefficients a = exp(sigma z), z i.i.d. N(0,1) per face: a lognormal
+    field with no spatial correlation. Arrays of shape (NC+1)^3 as
+    face_coefficients_grf."""
+    T = N + 2
+    z = normal(seed, 3 * T ** 3).reshape(3, T, T, T)
+    ax, ay, az = (np.exp(sigma * z[q]) for q in range(3))
+    return ax, ay, az

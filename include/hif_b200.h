@@ -207,6 +207,41 @@ int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, 
 int hif_memory(hif_handle h, long long* factor_bytes, long long* workspace_bytes);
 int hif_trim(hif_handle h);
 
+/* ---- Serving: many operators resident on one GPU ------------------------------
+ * No reference counterpart (the reference factors one operator per process,
+ * tests/HIFDE3D/main.cpp). A server keeps factored operators in device memory and
+ * runs requests from any host thread:
+ *   - factor requests (face-coefficient operator, as hif_setup_stencil_faces) run on
+ *     worker threads, each on its operator's own stream; one is admitted when its
+ *     expected device footprint fits in budget_bytes beside the resident factors;
+ *   - solve requests (PCG preconditioned by the inverse apply, as hif_solve_pcg)
+ *     are batched across operators at every iteration: up to max_active_solves run
+ *     together, one launch per apply stage for all of them; requests join and
+ *     leave between iterations. A request's result equals hif_solve_pcg's on the
+ *     same operator and right-hand sides, bit for bit, whatever else runs with it.
+ * Submitting returns a request id at once; hif_server_wait blocks until it ends.
+ * x_out (NC^3 x nrhs, host) must stay valid until then. Operator ids are chosen by
+ * the caller; a solve may be submitted while its operator is still being factored.
+ * Destroy the server only after every request has been waited for. */
+typedef struct hif_server_s* hif_server;
+int hif_server_create(long long budget_bytes, int max_active_solves, int factor_workers,
+                      hif_server* out);
+int hif_server_destroy(hif_server s);
+int hif_server_submit_factor(hif_server s, int op_id, int N, int P, double epsilon,
+                             int partition, int precision, double hstep, const double* ax,
+                             const double* ay, const double* az, const double* V,
+                             long long* request_id);
+int hif_server_submit_solve(hif_server s, int op_id, const double* b, int nrhs, double tol,
+                            int maxit, double* x_out, long long* request_id);
+/* status: HIF_OK or the request's error; iters / relres: the largest over its
+ * right-hand sides; latency_ms: submit to completion. */
+int hif_server_wait(hif_server s, long long request_id, int* status, int* iters,
+                    double* relres, double* latency_ms);
+/* Waits for the operator's solves in flight, then frees its factor. */
+int hif_server_release(hif_server s, int op_id);
+int hif_server_stats(hif_server s, long long* device_bytes, long long* resident_ops,
+                     long long* completed, long long* iterations, long long* batched_launches);
+
 /* Message of the last error on this thread. */
 const char* hif_last_error(void);
 
