@@ -82,6 +82,7 @@ _SIGNATURES = {
     "hif_interp_decomp": [_dp, _i, _i, _ll, _d, _dp, _ip, _ip, _ip],
     "hif_pivoted_qr": [_dp, _i, _i, _ll, _ip],
     "hif_triangular_solve": [_dp, _i, _ll, _dp, _i, _ll],
+    "hif_gemm_mixed_device": [_i, _i, _i, _i, _i, _d, _p, _ll, _p, _ll, _d, _p, _ll],
     "hif_server_create": [_ll, _i, _i, ctypes.POINTER(_p)],
     "hif_server_destroy": [_p],
     "hif_server_submit_factor": [_p, _i, _i, _i, _d, _i, _i, _d, _dp, _dp, _dp, _dp, _llp],
@@ -332,6 +333,14 @@ class HIFFactor:
         return d
 
 
+def GemmMixedDevice(transA: int, transB: int, m: int, n: int, k: int, alpha: float, dA: int,
+                    lda: int, dB: int, ldb: int, beta: float, dC: int, ldc: int) -> None:
+    """C = alpha op(A) op(B) + beta C on device pointers (column-major), split-TF32
+    products on the tcgen05 tensor cores with FP32 accumulation."""
+    _check(lib().hif_gemm_mixed_device(int(transA), int(transB), m, n, k, float(alpha), _p(dA),
+                                       lda, _p(dB), ldb, float(beta), _p(dC), ldc))
+
+
 class Server:
     """Many factored operators resident on one GPU, with iteration-level batched
     PCG solves across them (``hif_server_*`` in include/hif_b200.h).
@@ -377,7 +386,9 @@ class Server:
         return rid.value
 
     def submit_solve(self, op_id: int, b, tol: float = 1e-10, maxit: int = 100) -> int:
-        n3 = self._n3[int(op_id)]
+        n3 = self._n3.get(int(op_id))
+        if n3 is None:
+            raise HIFError(HIF_ERR_ARG, f"unknown operator {op_id}")
         bb = np.asarray(b, np.float64)
         nrhs = 1 if bb.ndim == 1 else bb.shape[1]
         bf = np.ascontiguousarray(bb.reshape(n3, nrhs, order="F").T).ravel()

@@ -250,9 +250,9 @@ struct Sources {
 // partial products and summed in a fixed order.
 template <class Timed>
 void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t stream, int cls,
-                Timed&& timed, int force_tile = 0, bool mixed = false) {
+                Timed&& timed, int force_tile = 0, int* mixed_status = nullptr) {
   if (gin.empty()) return;
-  if (mixed) {  // split-TF32 tensor-core path (Schur-complement updates)
+  if (mixed_status) {  // split-TF32 tensor-core path (Schur-complement updates)
     double fl = 0;
     std::vector<int> toff(1, 0);
     for (const GemmDesc& x : gin) {
@@ -263,7 +263,8 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
     GemmDesc* dg = tmp.add(upload(gin, stream));
     int* dt = tmp.add(upload(toff, stream));
     timed(HIF_KCLASS_GEMM_MIXED, fl, 0.0,
-          [&] { launch_gemm_mixed(dg, dt, (int)gin.size(), toff.back(), stream); }, 1);
+          [&] { launch_gemm_mixed(dg, dt, (int)gin.size(), toff.back(), mixed_status, stream); },
+          1);
     HIF_CK(cudaGetLastError());
     return;
   }
@@ -361,6 +362,12 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
     HIF_CK(cudaGetLastError());
   }
   if (large.empty()) return;
+  // Large blocks (include/Schur.hpp:72-100 in the reference's order):
+  //   1. A22^{-1} in place by a blocked Gauss-Jordan sweep over the r x r block
+  //      only (FP64 in both precisions: the diagonal-block factorization);
+  //   2. X = A22^{-1} A21, one product with k = r, written to the compact X;
+  //   3. S = A11 - A12 X, one product with k = r, in place in the trailing block.
+  // Product 3 goes to the split-TF32 tensor-core kernel in mixed precision.
   const int nl = (int)large.size();
   SweepDesc* dd = tmp.add(upload(large, stream));
   double* dinv = tmp.add(dalloc<double>((size_t)nl * kSweepNB * kSweepNB, stream));
@@ -368,7 +375,7 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
   for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
   for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
     std::vector<int> active;
-    std::vector<GemmDesc> gd, gmx, rowg, colg;
+    std::vector<GemmDesc> gd, rowg, colg;
     for (int b = 0; b < nl; ++b) {
       const SweepDesc& d = large[b];
       if (d.r <= k0) continue;
@@ -409,48 +416,11 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
         colg.push_back(g);
       };
       rowp(0, k0);
-      rowp(k1, d.n);
+      rowp(k1, d.r);
       colp(0, k0);
       colp(k1, d.r);
-      // mixed precision: the A22 block (rows and columns < r) stays FP64; the
-      // Schur-complement updates (columns >= r: X; rows >= r: A12 side and T)
-      // go to the split-TF32 tensor-core kernel
       auto gemm = [&](int r0, int r1, int c0, int c1) {
         if (r1 <= r0 || c1 <= c0) return;
-        if (mixed && (c1 > d.r || r0 >= d.r)) {
-          if (r0 < d.r && c0 < d.r) {  // split at column r
-            const int cm = d.r;
-            GemmDesc lo{}, hi{};
-            lo.C = d.B + r0 + (long long)c0 * d.n;
-            lo.A = d.B + r0 + (long long)k0 * d.n;
-            lo.B = d.B + k0 + (long long)c0 * d.n;
-            lo.ldc = lo.lda = lo.ldb = d.n;
-            lo.m = r1 - r0;
-            lo.n = cm - c0;
-            lo.k = nbk;
-            lo.alpha = -1.0;
-            lo.beta = 1.0;
-            gd.push_back(lo);
-            hi = lo;
-            hi.C = d.B + r0 + (long long)cm * d.n;
-            hi.B = d.B + k0 + (long long)cm * d.n;
-            hi.n = c1 - cm;
-            gmx.push_back(hi);
-            return;
-          }
-          GemmDesc x{};
-          x.C = d.B + r0 + (long long)c0 * d.n;
-          x.A = d.B + r0 + (long long)k0 * d.n;
-          x.B = d.B + k0 + (long long)c0 * d.n;
-          x.ldc = x.lda = x.ldb = d.n;
-          x.m = r1 - r0;
-          x.n = c1 - c0;
-          x.k = nbk;
-          x.alpha = -1.0;
-          x.beta = 1.0;
-          gmx.push_back(x);
-          return;
-        }
         GemmDesc g{};
         g.C = d.B + r0 + (long long)c0 * d.n;
         g.A = d.B + r0 + (long long)k0 * d.n;
@@ -464,10 +434,9 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
         gd.push_back(g);
       };
       gemm(0, k0, 0, k0);
-      gemm(0, k0, k1, d.n);
+      gemm(0, k0, k1, d.r);
       gemm(k1, d.r, 0, k0);
-      gemm(k1, d.r, k1, d.n);
-      gemm(d.r, d.n, k1, d.n);
+      gemm(k1, d.r, k1, d.r);
     }
     BufList step;
     int* dact = step.add(upload(active, stream));
@@ -476,7 +445,6 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
     });
     gemm_batch(rowg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
     gemm_batch(gd, step, stream, HIF_KCLASS_GEMM, timed);
-    gemm_batch(gmx, step, stream, HIF_KCLASS_GEMM_MIXED, timed, 128, true);
     gemm_batch(colg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
     timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
       launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
@@ -484,16 +452,50 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
     HIF_CK(cudaGetLastError());
     step.release(stream);
   }
-  // compact copies of A22^{-1} and X
+  // X = A22^{-1} A21 and S = A11 - A12 X
+  std::vector<GemmDesc> gx, gs;
+  for (const SweepDesc& d : large) {
+    const int r = d.r, sk = d.n - d.r;
+    if (sk == 0) continue;
+    GemmDesc x{};
+    x.C = d.X;
+    x.ldc = r;
+    x.A = d.B;
+    x.lda = d.n;
+    x.B = d.B + (long long)r * d.n;
+    x.ldb = d.n;
+    x.m = r;
+    x.n = sk;
+    x.k = r;
+    x.alpha = 1.0;
+    x.beta = 0.0;
+    gx.push_back(x);
+    GemmDesc y{};
+    y.C = d.B + r + (long long)r * d.n;
+    y.ldc = d.n;
+    y.A = d.B + r;
+    y.lda = d.n;
+    y.B = d.X;
+    y.ldb = r;
+    y.m = sk;
+    y.n = sk;
+    y.k = r;
+    y.alpha = -1.0;
+    y.beta = 1.0;
+    gs.push_back(y);
+  }
+  // X stays FP64: it comes from the explicit inverse, whose entries exceed X's by
+  // about cond(A22), so a TF32-level product would lose that factor in X.
+  gemm_batch(gx, tmp, stream, HIF_KCLASS_GEMM, timed);
+  if (mixed) gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM_MIXED, timed, 128, d_status);
+  else gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM, timed);
+  // compact copy of A22^{-1}
   std::vector<CopyDesc> cd;
   std::vector<int> coff(1, 0);
   for (const SweepDesc& d : large) {
     CopyDesc a{d.B, d.a22inv, d.n, d.r, d.r, d.r};
     cd.push_back(a);
     coff.push_back(coff.back() + copy_tiles(d.r, d.r));
-    CopyDesc x{d.B + (long long)d.r * d.n, d.X, d.n, d.r, d.r, d.n - d.r};
-    cd.push_back(x);
-    coff.push_back(coff.back() + copy_tiles(d.r, d.n - d.r));
   }
   CopyDesc* dcd = tmp.add(upload(cd, stream));
   int* dco = tmp.add(upload(coff, stream));
@@ -1518,7 +1520,9 @@ class Engine {
     HIF_CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
     factored = true;
     if (st & kStatusTinyPivot) throw Error{HIF_ERR_SINGULAR, "zero or non-finite pivot"};
-    if (st & kStatusTimeout) throw Error{HIF_ERR_CUDA, "grouped ID: barrier wait timed out"};
+    if (st & kStatusTimeout)
+      throw Error{HIF_ERR_CUDA, "a bounded device wait timed out (grouped ID barrier or tensor-core "
+                                "pipeline)"};
     // the apply sweeps are part of the factorization's output: build them now
     const double tp = wall();
     ensure_workspace(1);
@@ -2258,6 +2262,37 @@ int hif_schur_device(const double* dB, int n, int r, double* dA22inv, double* dX
       schur_on_device(c, dB, n, r, dA22inv, dX, dS);
     }
     if (c.status() & hif::kStatusTinyPivot) throw hif::Error{HIF_ERR_SINGULAR, "zero pivot"};
+  });
+}
+
+int hif_gemm_mixed_device(int transA, int transB, int m, int n, int k, double alpha,
+                          const double* dA, long long lda, const double* dB, long long ldb,
+                          double beta, double* dC, long long ldc) {
+  if (m < 0 || n < 0 || k < 0 || (m && n && (!dC || ldc < m)) ||
+      (m && n && k && (!dA || !dB || lda < (transA ? k : m) || ldb < (transB ? n : k))))
+    return HIF_ERR_ARG;
+  if (int e = check_device()) return e;
+  return guarded([&] {
+    if (m == 0 || n == 0) return;
+    FreeCtx c;
+    hif::GemmDesc g{};
+    g.C = dC;
+    g.A = dA;
+    g.B = dB;
+    g.ldc = ldc;
+    g.lda = lda;
+    g.ldb = ldb;
+    g.m = m;
+    g.n = n;
+    g.k = k;
+    g.transA = transA ? 1 : 0;
+    g.transB = transB ? 1 : 0;
+    g.alpha = alpha;
+    g.beta = beta;
+    hif::gemm_batch(std::vector<hif::GemmDesc>{g}, c.bufs, c.stream, HIF_KCLASS_GEMM_MIXED,
+                    [&](int, double, double, auto&& f, int = 1) { f(); }, 128, c.d_status);
+    if (c.status() & hif::kStatusTimeout)
+      throw hif::Error{HIF_ERR_CUDA, "tensor-core pipeline wait timed out"};
   });
 }
 

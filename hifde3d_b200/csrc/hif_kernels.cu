@@ -445,149 +445,279 @@ void launch_splitk_reduce(const SplitKDesc* d_desc, int nd, cudaStream_t s) {
   k_splitk_reduce<<<grid, 256, 0, s>>>(d_desc);
 }
 
-// ===========================================================================
-// Split-TF32 tensor-core GEMM (mixed precision). CTA tile 128 x 128, k step
-// 16; 8 warps as 2 (m) x 4 (n), warp tile 64 x 32 = 4 x 4 mma.m16n8k8 tiles.
-// Fragment layouts (PTX ISA, mma.m16n8k8 .tf32): with g = lane / 4 and
-// t = lane % 4, A regs hold (g, t), (g + 8, t), (g, t + 4), (g + 8, t + 4);
-// B regs hold (k = t, n = g), (k = t + 4, n = g); C holds (g, 2t), (g, 2t+1),
-// (g + 8, 2t), (g + 8, 2t + 1).
-// ===========================================================================
-constexpr int kMBM = 128, kMBN = 128, kMBK = 16;
-constexpr int kMStr = kMBK + 4;  // floats per smem row (conflict-free fragment loads)
-
+// TF32 rounding of an FP32 value (round to nearest, ties away), as a 32-bit container.
 __device__ __forceinline__ unsigned tf32_of(float x) {
   unsigned r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
   return r;
 }
 
-__device__ __forceinline__ void mma_tf32(float* c, const unsigned* a, const unsigned* b) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+// ===========================================================================
+// Split-TF32 GEMM on the 5th-generation tensor cores (tcgen05). One CTA per
+// 128 x 128 tile of C; k runs in stages of 32. All 8 warps load the FP64
+// operands of a stage, split each value into a TF32 pair (hi = rn(x),
+// lo = rn(x - hi)) and store the four parts (A hi / lo, B hi / lo) in shared
+// memory in the K-major canonical layout without swizzle: 8-row x 16-byte
+// core matrices, 128 bytes each, K-adjacent core matrices 128 bytes apart
+// (LBO), 8-row groups 1024 bytes apart (SBO). One thread issues, per k-step of
+// 8, the products lo*hi, hi*lo, hi*hi (M = 128, N = 128, K = 8, FP32
+// accumulation in tensor memory) and commits them to the stage's mbarrier,
+// which the loaders wait on before refilling that stage. After every 256
+// values of k the accumulator is read with tcgen05.ld (warp w reads lanes
+// 32 (w % 4) .. + 31, columns 64 (w / 4) .. + 63) and added to C in FP64
+// (the first chunk writes alpha acc + beta C), so FP32 sums never run over
+// more than 256 terms.
+// Every mbarrier wait is bounded (globaltimer, 2 s): on timeout the status
+// word gets kStatusTimeout, the tile is not written and the CTA still frees
+// its tensor memory.
+// ===========================================================================
+constexpr int kTcM = 128, kTcN = 128, kTcK = 32, kTcStages = 2, kTcChunk = 256;
+constexpr int kTcPart = kTcM * kTcK * 4;             // bytes of one operand part per stage
+constexpr int kTcStage = 4 * kTcPart;                // A hi, A lo, B hi, B lo
+constexpr int kTcSmem = kTcStages * kTcStage + 128;  // + mbarriers, tensor memory address
+constexpr unsigned long long kTcWaitNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
 }
 
-__global__ void __launch_bounds__(256, 1) k_gemm_mixed(const GemmDesc* __restrict__ descs,
-                                                       const int* __restrict__ tile_off, int nd) {
-  __shared__ unsigned Ahi[kMBM * kMStr], Alo[kMBM * kMStr];  // [m][k]
-  __shared__ unsigned Bhi[kMBN * kMStr], Blo[kMBN * kMStr];  // [n][k]
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the completion of the mbarrier phase with the given parity.
+__device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity) {
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (global_ns() - t0 > kTcWaitNs) return false;
+  }
+}
+
+// Shared-memory matrix descriptor: K-major, no swizzle, LBO 128 B, SBO 1024 B,
+// descriptor version 1 (sm_100).
+__device__ __forceinline__ unsigned long long tc_desc(unsigned addr) {
+  unsigned long long d = (unsigned long long)((addr >> 4) & 0x3FFF);
+  d |= (unsigned long long)(128 >> 4) << 16;
+  d |= (unsigned long long)(1024 >> 4) << 32;
+  d |= 1ull << 46;
+  return d;
+}
+
+// Instruction descriptor, kind::tf32: D F32 (bits 4-5 = 1), A and B TF32
+// (bits 7-9, 10-12 = 2), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr unsigned kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(kTcN >> 3) << 17) |
+                              ((unsigned)(kTcM >> 4) << 24);
+
+// Byte offset of element (row, k) of one 128 x 32 operand part.
+__device__ __forceinline__ int tc_off(int row, int kc) {
+  return (((row >> 3) * (kTcK / 4) + kc) << 7) + ((row & 7) << 4);
+}
+
+__global__ void __launch_bounds__(256, 1) k_gemm_tc(const GemmDesc* __restrict__ descs,
+                                                    const int* __restrict__ tile_off, int nd,
+                                                    int* __restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tc_smem + kTcStages * kTcStage);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(tc_smem + kTcStages * kTcStage + 64);
   const int di = find_desc(tile_off, nd, blockIdx.x);
   const GemmDesc g = descs[di];
   const int local = blockIdx.x - tile_off[di];
-  const int tiles_m = (g.m + kMBM - 1) / kMBM;
-  const int m0 = (local % tiles_m) * kMBM, n0 = (local / tiles_m) * kMBN;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
-  const int gq = lane >> 2, tq = lane & 3;
+  const int tiles_m = (g.m + kTcM - 1) / kTcM;
+  const int m0 = (local % tiles_m) * kTcM, n0 = (local / tiles_m) * kTcN;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  float acc[4][4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kTcN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const unsigned tmem = *tmem_slot;
 
-  double ra[8], rb[8];
+  // loader mapping: row = tid % 128 of the tile, k chunks (4 values) half, half + 2, ...
+  const int lr = tid & 127, lh = tid >> 7;
+  double ra[16], rb[16];
   auto load = [&](int k0) {
+    const int gm = m0 + lr, gn = n0 + lr;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int e = tid + 256 * q;
-      int mm, kk;
-      if (g.transA == 0) { mm = e % kMBM; kk = e / kMBM; } else { mm = e / kMBK; kk = e % kMBK; }
-      const int gm = m0 + mm, gk = k0 + kk;
-      ra[q] = (gm < g.m && gk < g.k)
-                  ? ((g.transA == 0) ? g.A[gm + (long long)gk * g.lda] : g.A[gk + (long long)gm * g.lda])
-                  : 0.0;
-      int nn, kb;
-      if (g.transB == 0) { kb = e % kMBK; nn = e / kMBK; } else { nn = e % kMBN; kb = e / kMBN; }
-      const int gn = n0 + nn, gk2 = k0 + kb;
-      rb[q] = (gn < g.n && gk2 < g.k)
-                  ? ((g.transB == 0) ? g.B[gk2 + (long long)gn * g.ldb] : g.B[gn + (long long)gk2 * g.ldb])
-                  : 0.0;
+    for (int i = 0; i < 4; ++i) {
+      const int kc = lh + 2 * i;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int gk = k0 + 4 * kc + e;
+        const bool ka = gk < g.k;
+        ra[4 * i + e] = (ka && gm < g.m) ? (g.transA == 0 ? g.A[gm + (long long)gk * g.lda]
+                                                         : g.A[gk + (long long)gm * g.lda])
+                                         : 0.0;
+        rb[4 * i + e] = (ka && gn < g.n) ? (g.transB == 0 ? g.B[gk + (long long)gn * g.ldb]
+                                                         : g.B[gn + (long long)gk * g.ldb])
+                                         : 0.0;
+      }
     }
   };
-  auto store = [&]() {
+  auto store = [&](int s) {
+    unsigned char* st = tc_smem + s * kTcStage;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int e = tid + 256 * q;
-      int mm, kk;
-      if (g.transA == 0) { mm = e % kMBM; kk = e / kMBM; } else { mm = e / kMBK; kk = e % kMBK; }
-      const float x = (float)ra[q];
-      const unsigned hi = tf32_of(x);
-      Ahi[mm * kMStr + kk] = hi;
-      Alo[mm * kMStr + kk] = tf32_of(x - __uint_as_float(hi));
-      int nn, kb;
-      if (g.transB == 0) { kb = e % kMBK; nn = e / kMBK; } else { nn = e % kMBN; kb = e / kMBN; }
-      const float y = (float)rb[q];
-      const unsigned yh = tf32_of(y);
-      Bhi[nn * kMStr + kb] = yh;
-      Blo[nn * kMStr + kb] = tf32_of(y - __uint_as_float(yh));
+    for (int i = 0; i < 4; ++i) {
+      const int off = tc_off(lr, lh + 2 * i);
+      uint4 ah, al, bh, bl;
+      unsigned* pah = &ah.x;
+      unsigned* pal = &al.x;
+      unsigned* pbh = &bh.x;
+      unsigned* pbl = &bl.x;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float x = (float)ra[4 * i + e];
+        const unsigned xh = tf32_of(x);
+        pah[e] = xh;
+        pal[e] = tf32_of(x - __uint_as_float(xh));
+        const float y = (float)rb[4 * i + e];
+        const unsigned yh = tf32_of(y);
+        pbh[e] = yh;
+        pbl[e] = tf32_of(y - __uint_as_float(yh));
+      }
+      *reinterpret_cast<uint4*>(st + 0 * kTcPart + off) = ah;
+      *reinterpret_cast<uint4*>(st + 1 * kTcPart + off) = al;
+      *reinterpret_cast<uint4*>(st + 2 * kTcPart + off) = bh;
+      *reinterpret_cast<uint4*>(st + 3 * kTcPart + off) = bl;
     }
   };
 
-  const int nk = (g.k + kMBK - 1) / kMBK;
+  // C (FP64) accumulates the FP32 tensor-memory sums chunk by chunk
+  // (kTcChunk values of k each), so no FP32 sum runs over more terms.
+  const int q4 = warp & 3, h2 = warp >> 2;
+  const int em = m0 + 32 * q4 + lane;
+  auto drain = [&](bool first) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      unsigned v[16];
+      const unsigned taddr = tmem + ((unsigned)(32 * q4) << 16) + (unsigned)(64 * h2 + 16 * c);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+          "%13,%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr)
+          : "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (em < g.m) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const int gn = n0 + 64 * h2 + 16 * c + e;
+          if (gn < g.n) {
+            double* cp = g.C + em + (long long)gn * g.ldc;
+            const double val = g.alpha * (double)__uint_as_float(v[e]);
+            if (first) *cp = (g.beta == 0.0) ? val : fma(g.beta, *cp, val);
+            else *cp += val;
+          }
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  };
+
+  const int nk = (g.k + kTcK - 1) / kTcK;
+  constexpr int spc = kTcChunk / kTcK;  // stages per chunk
+  bool failed = false;
   if (nk > 0) load(0);
   for (int t = 0; t < nk; ++t) {
-    __syncthreads();
-    store();
-    __syncthreads();
-    if (t + 1 < nk) load((t + 1) * kMBK);
+    const int s = t % kTcStages;
+    bool late = false;
+    if (t >= kTcStages) late = !mbar_wait(smem_u32(&mbar[s]), (unsigned)((t / kTcStages - 1) & 1));
+    if (!late) store(s);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (__syncthreads_or(late)) {
+      failed = true;
+      break;
+    }
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned base = smem_u32(tc_smem + s * kTcStage);
 #pragma unroll
-    for (int k8 = 0; k8 < kMBK; k8 += 8) {
-      unsigned ah[4][4], al[4][4], bh[4][2], bl[4][2];
+      for (int j = 0; j < kTcK / 8; ++j) {
+        const unsigned long long dah = tc_desc(base + 0 * kTcPart + 256 * j);
+        const unsigned long long dal = tc_desc(base + 1 * kTcPart + 256 * j);
+        const unsigned long long dbh = tc_desc(base + 2 * kTcPart + 256 * j);
+        const unsigned long long dbl = tc_desc(base + 3 * kTcPart + 256 * j);
+        const unsigned long long da[3] = {dal, dah, dah}, db[3] = {dbh, dbl, dbh};
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int r0 = wm + a * 16 + gq;
-        ah[a][0] = Ahi[r0 * kMStr + k8 + tq];
-        ah[a][1] = Ahi[(r0 + 8) * kMStr + k8 + tq];
-        ah[a][2] = Ahi[r0 * kMStr + k8 + tq + 4];
-        ah[a][3] = Ahi[(r0 + 8) * kMStr + k8 + tq + 4];
-        al[a][0] = Alo[r0 * kMStr + k8 + tq];
-        al[a][1] = Alo[(r0 + 8) * kMStr + k8 + tq];
-        al[a][2] = Alo[r0 * kMStr + k8 + tq + 4];
-        al[a][3] = Alo[(r0 + 8) * kMStr + k8 + tq + 4];
-      }
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int c0 = wn + b * 8 + gq;
-        bh[b][0] = Bhi[c0 * kMStr + k8 + tq];
-        bh[b][1] = Bhi[c0 * kMStr + k8 + tq + 4];
-        bl[b][0] = Blo[c0 * kMStr + k8 + tq];
-        bl[b][1] = Blo[c0 * kMStr + k8 + tq + 4];
-      }
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          mma_tf32(acc[a][b], al[a], bh[b]);
-          mma_tf32(acc[a][b], ah[a], bl[b]);
-          mma_tf32(acc[a][b], ah[a], bh[b]);
+        for (int p = 0; p < 3; ++p) {
+          const unsigned acc = (t % spc > 0 || j > 0 || p > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred q;\n\t"
+              "setp.ne.b32 q, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, q;\n\t}\n" ::"r"(tmem),
+              "l"(da[p]), "l"(db[p]), "r"(kTcIdesc), "r"(acc)
+              : "memory");
         }
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(&mbar[s]))
+          : "memory");
+    }
+    if (t + 1 < nk) load((t + 1) * kTcK);
+    if ((t + 1) % spc == 0 || t + 1 == nk) {
+      // end of a chunk: its products are done once this stage's commit arrived
+      const bool ok = mbar_wait(smem_u32(&mbar[s]), (unsigned)((t / kTcStages) & 1));
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      drain(t < spc);
     }
   }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int gm = m0 + wm + a * 16 + gq + ((c & 2) ? 8 : 0);
-        const int gn = n0 + wn + b * 8 + tq * 2 + (c & 1);
-        if (gm >= g.m || gn >= g.n) continue;
-        double* cp = g.C + gm + (long long)gn * g.ldc;
-        const double v = g.alpha * (double)acc[a][b][c];
-        *cp = (g.beta == 0.0) ? v : fma(g.beta, *cp, v);
+  if (failed) {
+    if (tid == 0) atomicOr(status, kStatusTimeout);
+  } else if (nk == 0 && em < g.m) {
+    for (int c = 0; c < 64; ++c) {
+      const int gn = n0 + 64 * h2 + c;
+      if (gn < g.n) {
+        double* cp = g.C + em + (long long)gn * g.ldc;
+        *cp = (g.beta == 0.0) ? 0.0 : g.beta * *cp;
       }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN)
+                 : "memory");
+  }
 }
 
 void launch_gemm_mixed(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
-                       cudaStream_t s) {
+                       int* d_status, cudaStream_t s) {
   if (total_tiles <= 0) return;
-  k_gemm_mixed<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    attr = true;
+  }
+  k_gemm_tc<<<total_tiles, 256, kTcSmem, s>>>(d_desc, d_tile_off, nd, d_status);
 }
 
 // ===========================================================================

@@ -166,8 +166,11 @@ void launch_splitk_reduce(const SplitKDesc* d_desc, int nd, cudaStream_t s);
 // (x = hi + lo); hi*hi + hi*lo + lo*hi run on the tensor cores (mma.sync
 // m16n8k8, FP32 accumulation), then C (FP64) = beta C + alpha acc.
 // 128 x 128 x 16 tiles; tile offsets from dgemm_tiles(m, n, 128).
+// Split-TF32 tensor-core GEMM (tcgen05, FP32 accumulation in tensor memory):
+// C = alpha op(A) op(B) + beta C over the descriptors, 128 x 128 tiles counted
+// by d_tile_off; bounded waits report kStatusTimeout in d_status.
 void launch_gemm_mixed(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
-                       cudaStream_t s);
+                       int* d_status, cudaStream_t s);
 
 // In-shared-memory Gauss-Jordan sweep of the first r pivots (n <= kSmallSweepN).
 constexpr int kSmallSweepN = 160;

@@ -207,6 +207,17 @@ int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, 
 int hif_memory(hif_handle h, long long* factor_bytes, long long* workspace_bytes);
 int hif_trim(hif_handle h);
 
+/* Mixed-precision GEMM on device pointers, the kernel of the HIF_PRECISION_MIXED
+ * Schur-complement updates: C = alpha op(A) op(B) + beta C (column-major; op(A) is
+ * m x k, op(B) k x n) with each FP64 operand split into a TF32 pair and the products
+ * hi*hi + hi*lo + lo*hi accumulated in FP32 on the tcgen05 tensor cores; relative
+ * error of order 1e-6 of |A| |B|. No reference counterpart (the reference's products
+ * are hmat_tools::Multiply dgemm calls, include/Schur.hpp:97-99). Runs on the calling thread's default
+ * per-thread stream and returns after completion. */
+int hif_gemm_mixed_device(int transA, int transB, int m, int n, int k, double alpha,
+                          const double* dA, long long lda, const double* dB, long long ldb,
+                          double beta, double* dC, long long ldc);
+
 /* ---- Serving: many operators resident on one GPU ------------------------------
  * No reference counterpart (the reference factors one operator per process,
  * tests/HIFDE3D/main.cpp). A server keeps factored operators in device memory and
