@@ -1280,6 +1280,10 @@ class Engine {
 
   // Blocked Householder row compression of the faces with more than
   // kCompressMinN columns: on return idM[f] / idm[f] point at R0 (n x n, ld n).
+  // Two levels of blocking: kQrNB2-column outer panels, each factored by
+  // kQrNB-column sub-panels that update only the rest of the outer panel; the
+  // columns right of the outer panel get one compact-WY update with all of its
+  // kQrNB2 reflectors (T from V^T V).
   static constexpr int kCompressMinN = 64;
   int kGroupMinN = 512;  // faces this wide get a CTA group (HIF_OPT_ID_GROUP_MIN_N)
   void compress_faces(const std::vector<BlockInfo>& blocks,
@@ -1293,89 +1297,174 @@ class Engine {
       const int n = blocks[f].global.size(), m = rows_l[f].size();
       if (n > kCompressMinN && m > n) {
         list.push_back(f);
-        vsz += (long long)m * kQrNB;
-        wsz += (long long)kQrNB * n;
+        vsz += (long long)m * kQrNB2;
+        wsz += (long long)kQrNB2 * n;
         rsz += (long long)n * n;
         maxn = std::max(maxn, n);
       }
     }
     if (list.empty()) return;
     Arena& work = *cur_work;
+    const size_t nl = list.size();
     double* V = work.alloc<double>(vsz);
-    double* Tm = work.alloc<double>((size_t)list.size() * kQrNB * kQrNB);
+    double* Tm = work.alloc<double>(nl * kQrNB * kQrNB);
+    double* T2 = work.alloc<double>(nl * kQrNB2 * kQrNB2);
+    double* Wv = work.alloc<double>(nl * kQrNB2 * kQrNB2);
+    double* tau = work.alloc<double>(nl * kQrNB2);
     double* Z = work.alloc<double>(wsz);
     double* Z2 = work.alloc<double>(wsz);
     double* R0 = work.alloc<double>(rsz);
     std::vector<QrDesc> qd;
     std::vector<long long> o_w, o_r;
     long long ov = 0, ow = 0, orr = 0;
-    for (size_t q = 0; q < list.size(); ++q) {
+    for (size_t q = 0; q < nl; ++q) {
       const int f = list[q];
       const int n = blocks[f].global.size(), m = rows_l[f].size();
-      qd.push_back(QrDesc{dM + o_M[f], V + ov, Tm + (long long)q * kQrNB * kQrNB, m, n});
+      qd.push_back(QrDesc{dM + o_M[f], V + ov, Tm + (long long)q * kQrNB * kQrNB,
+                          tau + (long long)q * kQrNB2, m, n});
       o_w.push_back(ow);
       o_r.push_back(orr);
-      ov += (long long)m * kQrNB;
-      ow += (long long)kQrNB * n;
+      ov += (long long)m * kQrNB2;
+      ow += (long long)kQrNB2 * n;
       orr += (long long)n * n;
     }
     QrDesc* dq = tmp.add(upload(qd, stream));
-    auto tm = [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); };
-    for (int k0 = 0; k0 < maxn; k0 += kQrNB) {
-      std::vector<int> act;
-      std::vector<GemmDesc> g1, g2, g3;
-      for (size_t q = 0; q < qd.size(); ++q) {
-        const QrDesc& d = qd[q];
-        if (d.n <= k0) continue;
-        act.push_back(q);
-        const int kb = std::min(kQrNB, d.n - k0), mt = d.m - k0, nt = d.n - k0 - kb;
-        if (nt <= 0) continue;
-        double* C = d.M + k0 + (long long)(k0 + kb) * d.m;
-        GemmDesc a{};  // Z = V^T C
-        a.C = Z + o_w[q];
-        a.A = d.V + k0;
-        a.B = C;
-        a.ldc = kQrNB;
-        a.lda = d.m;
-        a.ldb = d.m;
-        a.m = kb;
-        a.n = nt;
-        a.k = mt;
-        a.transA = 1;
-        a.alpha = 1.0;
-        a.beta = 0.0;
-        g1.push_back(a);
-        GemmDesc t{};  // Z2 = T^T Z
-        t.C = Z2 + o_w[q];
-        t.A = d.T;
-        t.B = Z + o_w[q];
-        t.ldc = kQrNB;
-        t.lda = kQrNB;
-        t.ldb = kQrNB;
-        t.m = kb;
-        t.n = nt;
-        t.k = kb;
-        t.transA = 1;
-        t.alpha = 1.0;
-        t.beta = 0.0;
-        g2.push_back(t);
-        GemmDesc c{};  // C -= V Z2
-        c.C = C;
-        c.A = d.V + k0;
-        c.B = Z2 + o_w[q];
-        c.ldc = d.m;
-        c.lda = d.m;
-        c.ldb = kQrNB;
-        c.m = mt;
-        c.n = nt;
-        c.k = kb;
-        c.alpha = -1.0;
-        c.beta = 1.0;
-        g3.push_back(c);
+    const int qr_cap = qr_cluster_max_rows();
+    if (verbose) {
+      long long sm = 0, sn = 0;
+      int mm = 0, mn = 0, ncl = 0;
+      for (const QrDesc& d : qd) {
+        sm += d.m;
+        sn += d.n;
+        mm = std::max(mm, d.m);
+        mn = std::max(mn, d.n);
+        ncl += d.m <= qr_cap;
       }
+      std::fprintf(stderr,
+                   "[hif]     compression: %zu faces, m avg %lld max %d, n avg %lld max %d, "
+                   "cluster rows cap %d (%d faces fit from the first panel)\n",
+                   qd.size(), sm / (long long)qd.size(), mm, sn / (long long)qd.size(), mn, qr_cap,
+                   ncl);
+    }
+    auto tm = [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); };
+    // C (rows k.. of columns c0..c1) -= V T^T V^T C with V the kb reflectors at
+    // V + voff (ld m), T ld ldt: three products
+    auto wy_update = [&](std::vector<GemmDesc>& g1, std::vector<GemmDesc>& g2,
+                         std::vector<GemmDesc>& g3, size_t q, const double* Vq, const double* Tq,
+                         int ldt, int k, int kb, int c0, int c1) {
+      const QrDesc& d = qd[q];
+      const int mt = d.m - k, nt = c1 - c0;
+      if (nt <= 0 || kb <= 0) return;
+      double* C = d.M + k + (long long)c0 * d.m;
+      GemmDesc a{};  // Z = V^T C
+      a.C = Z + o_w[q];
+      a.A = Vq;
+      a.B = C;
+      a.ldc = kQrNB2;
+      a.lda = d.m;
+      a.ldb = d.m;
+      a.m = kb;
+      a.n = nt;
+      a.k = mt;
+      a.transA = 1;
+      a.alpha = 1.0;
+      a.beta = 0.0;
+      g1.push_back(a);
+      GemmDesc t{};  // Z2 = T^T Z
+      t.C = Z2 + o_w[q];
+      t.A = Tq;
+      t.B = Z + o_w[q];
+      t.ldc = kQrNB2;
+      t.lda = ldt;
+      t.ldb = kQrNB2;
+      t.m = kb;
+      t.n = nt;
+      t.k = kb;
+      t.transA = 1;
+      t.alpha = 1.0;
+      t.beta = 0.0;
+      g2.push_back(t);
+      GemmDesc c{};  // C -= V Z2
+      c.C = C;
+      c.A = Vq;
+      c.B = Z2 + o_w[q];
+      c.ldc = d.m;
+      c.lda = d.m;
+      c.ldb = kQrNB2;
+      c.m = mt;
+      c.n = nt;
+      c.k = kb;
+      c.alpha = -1.0;
+      c.beta = 1.0;
+      g3.push_back(c);
+    };
+    for (int k0 = 0; k0 < maxn; k0 += kQrNB2) {
+      // sub-panels of the outer panel, each applied to the rest of the panel
+      for (int k1 = k0; k1 < std::min(maxn, k0 + kQrNB2); k1 += kQrNB) {
+        std::vector<int> act, actc;  // single-CTA / cluster panels
+        int maxc = 0;
+        std::vector<GemmDesc> g1, g2, g3;
+        for (size_t q = 0; q < nl; ++q) {
+          const QrDesc& d = qd[q];
+          if (d.n <= k1) continue;
+          if (d.m - k1 <= qr_cap) {
+            actc.push_back(q);
+            maxc = std::max(maxc, d.m - k1);
+          } else {
+            act.push_back(q);
+          }
+          const int kb = std::min(kQrNB, d.n - k1);
+          const double* Vq = d.V + (long long)(k1 - k0) * d.m + k1;
+          wy_update(g1, g2, g3, q, Vq, d.T, kQrNB, k1, kb, k1 + kb, std::min(d.n, k0 + kQrNB2));
+        }
+        BufList step;
+        if (!act.empty()) {
+          int* da = step.add(upload(act, stream));
+          timed(HIF_KCLASS_QR, 0, 0,
+                [&] { launch_qr_panel(dq, da, (int)act.size(), k1, k0, stream); });
+        }
+        if (!actc.empty()) {
+          int* dc = step.add(upload(actc, stream));
+          timed(HIF_KCLASS_QR, 0, 0, [&] {
+            launch_qr_panel_cluster(dq, dc, (int)actc.size(), k1, k0, maxc, stream);
+          });
+        }
+        gemm_batch(g1, step, stream, HIF_KCLASS_QR, tm);
+        gemm_batch(g2, step, stream, HIF_KCLASS_QR, tm);
+        gemm_batch(g3, step, stream, HIF_KCLASS_QR, tm);
+        HIF_CK(cudaGetLastError());
+        step.release(stream);
+      }
+      // outer panel: T from V^T V, then one update of the trailing columns
+      std::vector<GemmDesc> gw, g1, g2, g3;
+      std::vector<TFactorDesc> tf;
+      for (size_t q = 0; q < nl; ++q) {
+        const QrDesc& d = qd[q];
+        const int nb = std::min(kQrNB2, d.n - k0);
+        if (nb <= 0 || d.n <= k0 + kQrNB2) continue;
+        const double* Vq = d.V + k0;
+        double* Wq = Wv + (long long)q * kQrNB2 * kQrNB2;
+        double* Tq = T2 + (long long)q * kQrNB2 * kQrNB2;
+        GemmDesc w{};  // W = V^T V
+        w.C = Wq;
+        w.A = Vq;
+        w.B = Vq;
+        w.ldc = kQrNB2;
+        w.lda = w.ldb = d.m;
+        w.m = w.n = nb;
+        w.k = d.m - k0;
+        w.transA = 1;
+        w.alpha = 1.0;
+        w.beta = 0.0;
+        gw.push_back(w);
+        tf.push_back(TFactorDesc{Wq, d.tau, Tq, nb});
+        wy_update(g1, g2, g3, q, Vq, Tq, kQrNB2, k0, nb, k0 + nb, d.n);
+      }
+      if (tf.empty()) continue;
       BufList step;
-      int* da = step.add(upload(act, stream));
-      timed(HIF_KCLASS_QR, 0, 0, [&] { launch_qr_panel(dq, da, (int)act.size(), k0, stream); });
+      gemm_batch(gw, step, stream, HIF_KCLASS_QR, tm);
+      TFactorDesc* dtf = step.add(upload(tf, stream));
+      timed(HIF_KCLASS_QR, 0, 0, [&] { launch_qr_tfactor(dtf, (int)tf.size(), stream); });
       gemm_batch(g1, step, stream, HIF_KCLASS_QR, tm);
       gemm_batch(g2, step, stream, HIF_KCLASS_QR, tm);
       gemm_batch(g3, step, stream, HIF_KCLASS_QR, tm);

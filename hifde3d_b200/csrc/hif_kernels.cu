@@ -16,6 +16,8 @@
 //   gemv        gather / multiply / scatter sweeps of Apply (Factor.cpp:992-1081).
 #include "hif_kernels.cuh"
 
+#include <cooperative_groups.h>
+
 #include <cfloat>
 #include <climits>
 #include <algorithm>
@@ -1475,9 +1477,11 @@ void launch_copy(const CopyDesc* d_desc, const int* d_tile_off, int nd, int tota
 // Row compression: blocked Householder QR panels (one CTA per face)
 // ===========================================================================
 __global__ void __launch_bounds__(512) k_qr_panel(const QrDesc* __restrict__ descs,
-                                                  const int* __restrict__ active, int k0) {
+                                                  const int* __restrict__ active, int k0,
+                                                  int vrow0) {
   const QrDesc d = descs[active[blockIdx.x]];
   const int m = d.m, kb = min(kQrNB, d.n - k0);
+  double* Vout = d.V + (long long)(k0 - vrow0) * m;  // this sub-panel's columns of V
   double* M = d.M;
   __shared__ double s_tau[kQrNB];
   __shared__ double scratch[64];
@@ -1517,16 +1521,17 @@ __global__ void __launch_bounds__(512) k_qr_panel(const QrDesc* __restrict__ des
     }
     __syncthreads();
   }
-  // explicit V (unit diagonal, zeros above) for rows k0..m-1
-  const int mt = m - k0;
+  // explicit V (unit diagonal, zeros above) for rows vrow0..m-1
+  const int mt = m - vrow0;
   for (long long e = tid; e < (long long)mt * kb; e += nthr) {
     const int rr = (int)(e % mt), j = (int)(e / mt);
-    const int r = k0 + rr;
+    const int r = vrow0 + rr;
     double v = 0.0;
     if (r == k0 + j) v = 1.0;
     else if (r > k0 + j) v = M[r + (long long)(k0 + j) * m];
-    d.V[r + (long long)j * m] = v;
+    Vout[r + (long long)j * m] = v;
   }
+  for (int j = tid; j < kb; j += nthr) d.tau[k0 - vrow0 + j] = s_tau[j];
   __syncthreads();
   // Wd = V^T V in one pass over the rows: lane c holds V[r, c]; the products
   // with every other column come by shuffle. Warps add their partial sums in
@@ -1536,7 +1541,7 @@ __global__ void __launch_bounds__(512) k_qr_panel(const QrDesc* __restrict__ des
 #pragma unroll
     for (int i = 0; i < kQrNB; ++i) acc[i] = 0.0;
     for (int r = k0 + warp; r < m; r += nw) {
-      const double v = (lane < kb) ? d.V[r + (long long)lane * m] : 0.0;
+      const double v = (lane < kb) ? Vout[r + (long long)lane * m] : 0.0;
 #pragma unroll
       for (int i = 0; i < kQrNB; ++i) acc[i] = fma(__shfl_sync(0xffffffffu, v, i), v, acc[i]);
     }
@@ -1567,10 +1572,291 @@ __global__ void __launch_bounds__(512) k_qr_panel(const QrDesc* __restrict__ des
   }
 }
 
-void launch_qr_panel(const QrDesc* d_desc, const int* d_active, int nact, int k0,
+// ---------------------------------------------------------------------------
+// The same sub-panel factorization by a thread-block cluster per face: the
+// cluster's CTAs split the panel's rows (at most kQrcRows each) and keep them
+// in shared memory for the whole panel. Per column, every CTA sums over its
+// rows the squared norm below the diagonal and the products of the column with
+// the columns to its right; the owner of the diagonal row adds that row's
+// entries. One cluster barrier, then every CTA adds the CTAs' partial vectors
+// in rank order (identical sums everywhere, deterministic), forms the
+// reflector (beta, tau) exactly as the single-CTA kernel does and updates its
+// rows. Partial vectors alternate between two buffers, so one barrier per
+// column orders both the reads of step j and the writes of step j + 2.
+// ---------------------------------------------------------------------------
+namespace cg = cooperative_groups;
+constexpr int kQrcRows = 768;
+constexpr int kQrcSlots = 2 * kQrNB + 2;  // [norm^2 | x.A_c (32) | alpha | A[col, c] (32)]
+
+__global__ void __launch_bounds__(512) k_qr_panel_cluster(const QrDesc* __restrict__ descs,
+                                                          const int* __restrict__ active,
+                                                          int k1, int vrow0) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const QrDesc d = descs[active[blockIdx.x / C]];
+  const int m = d.m, kb = min(kQrNB, d.n - k1), mt = m - k1;
+  const int chunk = (mt + C - 1) / C;
+  const int r0 = k1 + rank * chunk, r1 = min(m, r0 + chunk), nr = max(0, r1 - r0);
+  const int ld = chunk | 1;  // odd: lanes reading one row of 32 columns hit distinct banks
+  extern __shared__ double P[];  // nr x kQrNB, ld ld (local rows r0..r1)
+  __shared__ double red[2][kQrcSlots];
+  __shared__ double wpart[16][kQrcSlots];
+  __shared__ double tot[kQrcSlots];
+  __shared__ double gram[kQrNB * kQrNB];
+  __shared__ double s_tau[kQrNB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthr = blockDim.x;
+  double* M = d.M;
+  for (int e = tid; e < nr * kQrNB; e += nthr) {
+    const int i = e % nr, c = e / nr;
+    P[i + c * ld] = (c < kb) ? M[(r0 + i) + (long long)(k1 + c) * m] : 0.0;
+  }
+  __syncthreads();
+  for (int j = 0; j < kb; ++j) {
+    const int col = k1 + j;
+    // partial sums over local rows below the diagonal
+    double acc[kQrNB + 1];
+#pragma unroll
+    for (int c = 0; c <= kQrNB; ++c) acc[c] = 0.0;
+    for (int i = tid; i < nr; i += nthr) {
+      if (r0 + i <= col) continue;
+      const double x = P[i + j * ld];
+      acc[0] = fma(x, x, acc[0]);
+#pragma unroll
+      for (int c = 0; c < kQrNB; ++c)
+        if (c > j) acc[1 + c] = fma(x, P[i + c * ld], acc[1 + c]);
+    }
+    // warp reduce-scatter of acc[1..32] (5 halving exchanges, 31 shuffles):
+    // afterwards lane c holds the warp's total of acc[1 + c]; acc[0] by warp_sum
+    {
+      const double n2 = warp_sum(acc[0]);
+      if (lane == 0) wpart[warp][0] = n2;
+#pragma unroll
+      for (int h = 16; h >= 1; h >>= 1) {
+        const bool upper = (lane & h) != 0;
+#pragma unroll
+        for (int c = 0; c < h; ++c) {
+          // keep the half selected by this lane's bit, send the other half
+          const double send = upper ? acc[1 + c] : acc[1 + c + h];
+          const double keep = upper ? acc[1 + c + h] : acc[1 + c];
+          acc[1 + c] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+      }
+      // the kept halves follow the lane's bits from high to low: acc[1] of lane c
+      // is the warp's total for column c
+      wpart[warp][1 + lane] = acc[1];
+    }
+    __syncthreads();
+    double* rb = red[j & 1];
+    if (tid <= kQrNB) {
+      double sacc = 0.0;
+      for (int w = 0; w < (nthr >> 5); ++w) sacc += wpart[w][tid];
+      rb[tid] = sacc;
+    } else if (tid <= 2 * kQrNB + 1) {
+      // diagonal-row entries (alpha and A[col, c]) from the CTA that owns the row
+      const int c = tid - (kQrNB + 1);  // 0 -> alpha, 1 + c' -> A[col, c']
+      double v = 0.0;
+      if (col >= r0 && col < r1) {
+        const int cc = (c == 0) ? j : c - 1;
+        if (c == 0 || (cc > j && cc < kb)) v = P[(col - r0) + cc * ld];
+      }
+      rb[tid] = v;
+    }
+    cl.sync();
+    if (tid < kQrcSlots) {
+      double v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = (q < C) ? cl.map_shared_rank(rb, q)[tid] : 0.0;
+      double sacc = 0.0;
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (q < C) sacc += v[q];
+      tot[tid] = sacc;
+    }
+    __syncthreads();
+    const double xnorm = sqrt(tot[0]);
+    const double alpha = tot[kQrNB + 1];
+    double tau = 0.0, beta = alpha, scal = 1.0;
+    if (xnorm != 0.0) {
+      beta = -copysign(hypot(alpha, xnorm), alpha);
+      tau = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    // update the local rows: v = x * scal below the diagonal, w_c = tau (A[col, c] + v . A_c)
+    for (int i = tid; i < nr; i += nthr) {
+      const int r = r0 + i;
+      if (r < col) continue;
+      if (r == col) {
+        P[i + j * ld] = beta;
+        for (int c = j + 1; c < kb; ++c) {
+          const double w = tau * (tot[kQrNB + 2 + c] + scal * tot[1 + c]);
+          P[i + c * ld] -= w;
+        }
+      } else {
+        const double v = (xnorm != 0.0) ? P[i + j * ld] * scal : P[i + j * ld];
+        P[i + j * ld] = v;
+        for (int c = j + 1; c < kb; ++c) {
+          const double w = tau * (tot[kQrNB + 2 + c] + scal * tot[1 + c]);
+          P[i + c * ld] = fma(-w, v, P[i + c * ld]);
+        }
+      }
+    }
+    if (tid == 0) s_tau[j] = tau;
+    __syncthreads();
+  }
+  // results: the panel back to M, V (unit diagonal, zeros above) for rows
+  // vrow0.., tau
+  double* Vout = d.V + (long long)(k1 - vrow0) * m;
+  for (int e = tid; e < nr * kb; e += nthr) {
+    const int i = e % nr, c = e / nr;
+    const int r = r0 + i;
+    const double p = P[i + c * ld];
+    M[r + (long long)(k1 + c) * m] = p;
+    Vout[r + (long long)c * m] = (r == k1 + c) ? 1.0 : (r > k1 + c ? p : 0.0);
+  }
+  if (rank == 0) {
+    for (int e = tid; e < (k1 - vrow0) * kb; e += nthr) {
+      const int i = e % (k1 - vrow0), c = e / (k1 - vrow0);
+      Vout[vrow0 + i + (long long)c * m] = 0.0;
+    }
+    for (int j = tid; j < kb; j += nthr) d.tau[k1 - vrow0 + j] = s_tau[j];
+  }
+  // W = V^T V: local partial Gram (lane c holds column c; products with every
+  // other column by shuffle), warps added in warp order, CTAs summed by rank 0
+  // in rank order
+  {
+    double accg[kQrNB];
+#pragma unroll
+    for (int a = 0; a < kQrNB; ++a) accg[a] = 0.0;
+    for (int i = warp; i < nr; i += (nthr >> 5)) {
+      const int r = r0 + i;
+      const double v = (lane < kb) ? (r == k1 + lane ? 1.0 : (r > k1 + lane ? P[i + lane * ld] : 0.0))
+                                   : 0.0;
+#pragma unroll
+      for (int a = 0; a < kQrNB; ++a) accg[a] = fma(__shfl_sync(0xffffffffu, v, a), v, accg[a]);
+    }
+    for (int e = tid; e < kQrNB * kQrNB; e += nthr) gram[e] = 0.0;
+    __syncthreads();
+    for (int w = 0; w < (nthr >> 5); ++w) {
+      if (warp == w) {
+#pragma unroll
+        for (int a = 0; a < kQrNB; ++a) gram[a + lane * kQrNB] += accg[a];
+      }
+      __syncthreads();
+    }
+  }
+  cl.sync();
+  if (rank == 0) {
+    // the panel rows are no longer needed: W and T live in their space
+    double* Wsum = P;
+    double* Tl = P + kQrNB * kQrNB;
+    for (int e = tid; e < kQrNB * kQrNB; e += nthr) {
+      double g = 0.0;
+      for (int q = 0; q < C; ++q) g += cl.map_shared_rank(gram, q)[e];
+      Wsum[e] = g;
+      Tl[e] = 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+      if (tid < j) {
+        double a = 0.0;
+        for (int l = tid; l < j; ++l) a = fma(Tl[tid + l * kQrNB], Wsum[l + j * kQrNB], a);
+        Tl[tid + j * kQrNB] = -s_tau[j] * a;
+      }
+      if (tid == 0) Tl[j + j * kQrNB] = s_tau[j];
+      __syncthreads();
+    }
+    for (int e = tid; e < kQrNB * kQrNB; e += nthr) d.T[e] = Tl[e];
+  }
+  cl.sync();  // no CTA leaves while rank 0 reads its shared memory
+}
+
+void launch_qr_panel(const QrDesc* d_desc, const int* d_active, int nact, int k1, int k0,
                      cudaStream_t s) {
   if (nact <= 0) return;
-  k_qr_panel<<<nact, 512, 0, s>>>(d_desc, d_active, k0);
+  k_qr_panel<<<nact, 512, 0, s>>>(d_desc, d_active, k1, k0);
+}
+
+int qr_cluster_max_rows() {
+  static int cap = -1;
+  if (cap < 0) {
+    cudaFuncSetAttribute(k_qr_panel_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (kQrcRows + 1) * kQrNB * 8);
+    cudaFuncSetAttribute(k_qr_panel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    // the largest cluster the device can place with this kernel's footprint
+    int best = 1;
+    for (int c : {16, 8}) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(c, 1, 1);
+      cfg.blockDim = dim3(512, 1, 1);
+      cfg.dynamicSmemBytes = (kQrcRows + 1) * kQrNB * 8;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = c;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, k_qr_panel_cluster, &cfg) == cudaSuccess && n > 0) {
+        best = c;
+        break;
+      }
+      cudaGetLastError();
+    }
+    cap = best * kQrcRows;
+  }
+  return cap;
+}
+
+void launch_qr_panel_cluster(const QrDesc* d_desc, const int* d_active, int nact, int k1,
+                             int k0, int max_rows, cudaStream_t s) {
+  if (nact <= 0) return;
+  const int C = std::max(1, (max_rows + kQrcRows - 1) / kQrcRows);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nact * C, 1, 1);
+  cfg.blockDim = dim3(512, 1, 1);
+  cfg.dynamicSmemBytes = (kQrcRows + 1) * kQrNB * 8;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_qr_panel_cluster, d_desc, d_active, k1, k0);
+}
+
+// One CTA per outer panel: the forward column recurrence for T over kQrNB2
+// reflectors (T kept in shared memory, 128 KB).
+__global__ void __launch_bounds__(256) k_qr_tfactor(const TFactorDesc* __restrict__ descs) {
+  const TFactorDesc d = descs[blockIdx.x];
+  extern __shared__ double Ts[];  // kQrNB2 x kQrNB2
+  const int nb = d.nb, tid = threadIdx.x;
+  for (int e = tid; e < kQrNB2 * kQrNB2; e += blockDim.x) Ts[e] = 0.0;
+  __syncthreads();
+  for (int j = 0; j < nb; ++j) {
+    const double tj = d.tau[j];
+    for (int i = tid; i < j; i += blockDim.x) {
+      double acc = 0.0;
+      for (int l = i; l < j; ++l) acc = fma(Ts[i + l * kQrNB2], d.W[l + j * kQrNB2], acc);
+      Ts[i + j * kQrNB2] = -tj * acc;
+    }
+    if (tid == 0) Ts[j + j * kQrNB2] = tj;
+    __syncthreads();
+  }
+  for (int e = tid; e < kQrNB2 * kQrNB2; e += blockDim.x) d.T[e] = Ts[e];
+}
+
+void launch_qr_tfactor(const TFactorDesc* d_desc, int nd, cudaStream_t s) {
+  if (nd <= 0) return;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_qr_tfactor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kQrNB2 * kQrNB2 * 8);
+    attr = true;
+  }
+  k_qr_tfactor<<<nd, 256, kQrNB2 * kQrNB2 * 8, s>>>(d_desc);
 }
 
 __global__ void k_triu(const TriuDesc* __restrict__ descs) {

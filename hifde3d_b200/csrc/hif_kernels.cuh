@@ -228,14 +228,36 @@ cudaError_t launch_id_group(const IdGroupDesc* d_desc, int nd, int group, double
 // Q = I - V T V^T (32 x 32, ld 32). The trailing columns C are then updated by
 // batched GEMMs: Z = V^T C, Z = T^T Z, C -= V Z.
 constexpr int kQrNB = 32;
+// Two-level blocked Householder: outer panels of kQrNB2 columns, each
+// factored by kQrNB-wide sub-panels.
+constexpr int kQrNB2 = 128;
 struct QrDesc {
-  double* M;  // m x n, ld m
-  double* V;  // m x kQrNB, ld m
-  double* T;  // kQrNB x kQrNB
+  double* M;    // m x n, ld m
+  double* V;    // m x kQrNB2, ld m: reflectors of the current outer panel
+  double* T;    // kQrNB x kQrNB: compact-WY factor of the current sub-panel
+  double* tau;  // kQrNB2: Householder scalars of the current outer panel
   int m, n;
 };
-void launch_qr_panel(const QrDesc* d_desc, const int* d_active, int nact, int k0,
+// Sub-panel at columns [k1, k1 + kQrNB) of the outer panel starting at k0: V's
+// columns k1 - k0 .. are written for rows k0 .. m - 1 (zeros above the unit
+// diagonal), tau likewise, T for the sub-panel.
+void launch_qr_panel(const QrDesc* d_desc, const int* d_active, int nact, int k1, int k0,
                      cudaStream_t s);
+// The same by one thread-block cluster per face with the panel rows held in
+// shared memory: for faces with at most qr_cluster_max_rows() rows below k1;
+// max_rows = the largest m - k1 among the active faces (sets the cluster size).
+int qr_cluster_max_rows();
+void launch_qr_panel_cluster(const QrDesc* d_desc, const int* d_active, int nact, int k1,
+                             int k0, int max_rows, cudaStream_t s);
+// T (nb x nb, ld kQrNB2) of the outer panel from W = V^T V (ld kQrNB2) and tau:
+// T[j, j] = tau_j, T[0:j, j] = -tau_j T[0:j, 0:j] W[0:j, j].
+struct TFactorDesc {
+  const double* W;
+  const double* tau;
+  double* T;
+  int nb;
+};
+void launch_qr_tfactor(const TFactorDesc* d_desc, int nd, cudaStream_t s);
 // dst (n x n, ld ldd) = upper triangle of src (ld lds), zeros below.
 struct TriuDesc {
   const double* src;
