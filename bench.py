@@ -257,10 +257,12 @@ def run_serving(hb, synth, prec: int, nreq: int, rate: float, budget_gb: float =
             sids.append((srv.submit_solve(op, rhs(n, nrhs, seed), tol=1e-10, maxit=100), n,
                          nrhs))
     lat_s, lat_f, iters, worst, rhs_total, fails = [], [], [], 0.0, 0, 0
+    errors = []
     for rid, n, nrhs in sids:
         r = srv.wait(rid)
         if r["status"] != hb.HIF_OK:
             fails += 1
+            errors.append(f"solve n={n}: {r.get('error', r['status'])}")
             continue
         lat_s.append(r["latency_ms"])
         iters.append(r["iters"])
@@ -270,6 +272,7 @@ def run_serving(hb, synth, prec: int, nreq: int, rate: float, budget_gb: float =
         r = srv.wait(rid)
         if r["status"] != hb.HIF_OK:
             fails += 1
+            errors.append(f"factor n={n}: {r.get('error', r['status'])}")
             continue
         lat_f.append(r["latency_ms"])
     makespan = time.perf_counter() - t0
@@ -285,7 +288,7 @@ def run_serving(hb, synth, prec: int, nreq: int, rate: float, budget_gb: float =
             "factor_p50_ms": pct(lat_f, 50), "factor_p99_ms": pct(lat_f, 99),
             "pcg_iters_max": max(iters) if iters else None, "relres_max": worst,
             "server_iterations": st["iterations"], "batched_launches": st["batched_launches"],
-            "peak_resident_ops": max_resident}
+            "peak_resident_ops": max_resident, "errors": errors[:4]}
 
 
 def run_ours(args, rank: int, world: int):
@@ -503,6 +506,10 @@ def run_ours(args, rank: int, world: int):
                           "solves_per_s": 1e3 / r["solve_ms"], "pcg_iters": r["pcg_iters"],
                           "pcg_relres": r["pcg_relres"]}
     if not args.no_serving:
+        # the n = 128 operator and its pool memory leave the device first
+        f.close()
+        torch.cuda.synchronize()
+        hb.trim_device_pool()
         serve = {}
         for name, prec in (("fp64", hb.PRECISION_FP64), ("mixed", hb.PRECISION_MIXED)):
             if prec in runs:

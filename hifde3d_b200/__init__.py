@@ -76,6 +76,7 @@ _SIGNATURES = {
     "hif_kernel_stats": [_p, _i, _llp, _dp, _dp, _dp],
     "hif_memory": [_p, _llp, _llp],
     "hif_trim": [_p],
+    "hif_trim_device_pool": [],
     "hif_schur": [_dp, _i, _ll, _ip, _i, _ip, _i, _dp, _dp, _dp, _dp],
     "hif_schur_device": [_p, _i, _i, _p, _p, _p],
     "hif_schur_device_noalloc": [_p, _i, _i, _p, _p, _p, _p],
@@ -331,6 +332,11 @@ class HIFFactor:
         d = {k: v.value for k, v in zip(keys, vals)}
         d["device_bytes"] = nb.value
         return d
+
+
+def trim_device_pool() -> None:
+    """Return the unused reserved memory of the current device's default pool."""
+    _check(lib().hif_trim_device_pool())
 
 
 def GemmMixedDevice(transA: int, transB: int, m: int, n: int, k: int, alpha: float, dA: int,

@@ -2524,6 +2524,18 @@ int hif_trim(hif_handle h) {
   });
 }
 
+int hif_trim_device_pool(void) {
+  if (int e = check_device()) return e;
+  return guarded([&] {
+    int dev = 0;
+    HIF_CK(cudaGetDevice(&dev));
+    HIF_CK(cudaDeviceSynchronize());
+    cudaMemPool_t pool;
+    HIF_CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    HIF_CK(cudaMemPoolTrimTo(pool, 0));
+  });
+}
+
 int hif_memory(hif_handle h, long long* factor_bytes, long long* workspace_bytes) {
   if (!h) return HIF_ERR_ARG;
   if (factor_bytes) *factor_bytes = (long long)h->e->arena_factor.reserved();

@@ -206,6 +206,10 @@ int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, 
  * factorizations; hif_trim returns it to the device). */
 int hif_memory(hif_handle h, long long* factor_bytes, long long* workspace_bytes);
 int hif_trim(hif_handle h);
+/* Temporaries freed by any handle stay reserved in the current device's default
+ * memory pool for reuse (handles raise its release threshold); this returns the
+ * unused part to the device. Synchronises the device. */
+int hif_trim_device_pool(void);
 
 /* Mixed-precision GEMM on device pointers, the kernel of the HIF_PRECISION_MIXED
  * Schur-complement updates: C = alpha op(A) op(B) + beta C (column-major; op(A) is
