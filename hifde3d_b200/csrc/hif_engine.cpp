@@ -1060,7 +1060,10 @@ class Engine {
       idM[f] = dM + o_M[f];
       idm[f] = rows_l[f].size();
     }
-    compress_faces(blocks, rows_l, dM, o_M, idM, idm, tmp);
+    // mixed precision: tall faces go to the pivoted Cholesky ID instead (no
+    // compression; replayed pivot orders keep the QR path)
+    const bool chol = precision == HIF_PRECISION_MIXED && d_ord == nullptr;
+    if (!chol) compress_faces(blocks, rows_l, dM, o_M, idM, idm, tmp);
     mark("skel row compression", level);
     std::vector<IdDesc> idd(nf);
     for (int f = 0; f < nf; ++f) {
@@ -1077,12 +1080,16 @@ class Engine {
     }
     // small faces: one CTA each (k_id); compressed faces: grouped ID, several
     // CTAs per face for the largest ones
-    std::vector<IdDesc> small_id;
+    std::vector<IdDesc> small_id, chol_id;
     std::vector<IdGroupDesc> g1, gbig;
     int small_n = 0, g1_m = 0, g1_n = 0, big_m = 0, big_n = 0;
     for (int f = 0; f < nf; ++f) {
       const bool compressed = idM[f] != dM + o_M[f];
       const int n = idd[f].n;
+      if (chol && n > kCompressMinN && idd[f].m > n) {
+        chol_id.push_back(idd[f]);
+        continue;
+      }
       if (!compressed) {
         small_id.push_back(idd[f]);
         small_n = std::max(small_n, n);
@@ -1124,6 +1131,7 @@ class Engine {
             [&] { launch_id(d_idd, (int)small_id.size(), small_n, eps, d_status, stream); });
       idfl = 0;
     }
+    if (!chol_id.empty()) id_cholesky(chol_id, tmp);
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<IdGroupDesc>& v = pass == 0 ? g1 : gbig;
       if (v.empty()) continue;
@@ -1276,6 +1284,139 @@ class Engine {
     tmp.release(stream);
     steps.push_back(std::move(st));
     t_host += wall() - th;
+  }
+
+  // ID of the tall faces in mixed precision: G = M^T M (FP64 product), then a
+  // pivoted Cholesky of G by panels of kPcholNB steps (one CTA per face per
+  // panel, the trailing G updated by an FP64 product after each panel) until
+  // R_ii <= eps R_00, then W = R11^{-1} R12 by blocks of kTrsmNB rows. Pivot
+  // choices equal column-pivoted QR's in exact arithmetic (InterpDecomp.cpp:
+  // 86-138); the skeleton test is the reference's |R_ii| > eps |R_00|.
+  static constexpr int kPcholNB = 32;
+  void id_cholesky(const std::vector<IdDesc>& v, BufList& tmp) {
+    Arena& work = *cur_work;
+    const int nd = (int)v.size();
+    long long gsz = 0, isz = 0;
+    int max_n = 0;
+    for (const IdDesc& d : v) {
+      gsz += (long long)d.n * d.n;
+      isz += 2LL * d.n;
+      max_n = std::max(max_n, d.n);
+    }
+    double* G = work.alloc<double>(gsz);
+    double* R = work.alloc<double>(gsz);
+    int* ibuf = work.alloc<int>(isz + 2LL * nd);
+    double* d0 = work.alloc<double>(nd);
+    HIF_CK(cudaMemsetAsync(ibuf + isz, 0, 2 * nd * sizeof(int), stream));
+    std::vector<PcholDesc> pd(nd);
+    std::vector<GemmDesc> gram;
+    long long og = 0, oi = 0;
+    for (int q = 0; q < nd; ++q) {
+      const IdDesc& d = v[q];
+      PcholDesc& p = pd[q];
+      p.G = G + og;
+      p.R = R + og;
+      p.chosen = ibuf + oi;
+      p.piv = ibuf + oi + d.n;
+      p.info = ibuf + isz + 2 * q;
+      p.d0 = d0 + q;
+      p.id = d;
+      og += (long long)d.n * d.n;
+      oi += 2LL * d.n;
+      GemmDesc g{};  // G = M^T M
+      g.C = p.G;
+      g.ldc = d.n;
+      g.A = d.M;
+      g.lda = d.m;
+      g.B = d.M;
+      g.ldb = d.m;
+      g.m = g.n = d.n;
+      g.k = d.m;
+      g.transA = 1;
+      g.alpha = 1.0;
+      g.beta = 0.0;
+      gram.push_back(g);
+    }
+    auto tm = [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); };
+    gemm_batch(gram, tmp, stream, HIF_KCLASS_QR, tm);
+    PcholDesc* dpd = tmp.add(upload(pd, stream));
+    std::vector<int> active(nd), info(2 * nd);
+    for (int q = 0; q < nd; ++q) active[q] = q;
+    for (int i0 = 0; !active.empty(); i0 += kPcholNB) {
+      BufList step;
+      int* da = step.add(upload(active, stream));
+      timed(HIF_KCLASS_ID, 0, 0, [&] {
+        launch_pchol_panel(dpd, da, (int)active.size(), i0, kPcholNB, eps, max_n, d_status,
+                           stream);
+      });
+      HIF_CK(cudaGetLastError());
+      HIF_CK(cudaMemcpyAsync(info.data(), ibuf + isz, 2 * nd * sizeof(int),
+                             cudaMemcpyDeviceToHost, stream));
+      sync();
+      std::vector<int> next;
+      std::vector<GemmDesc> upd;
+      for (int q : active) {
+        if (info[2 * q + 1]) continue;
+        next.push_back(q);
+        const int n = pd[q].id.n;
+        GemmDesc g{};  // G -= Y Y^T, Y = the panel's rows of R as an n x nb matrix
+        g.C = pd[q].G;
+        g.ldc = n;
+        g.A = pd[q].R + (long long)i0 * n;
+        g.lda = n;
+        g.B = g.A;
+        g.ldb = n;
+        g.transB = 1;
+        g.m = g.n = n;
+        g.k = kPcholNB;
+        g.alpha = -1.0;
+        g.beta = 1.0;
+        upd.push_back(g);
+      }
+      gemm_batch(upd, step, stream, HIF_KCLASS_ID, tm);
+      HIF_CK(cudaGetLastError());
+      step.release(stream);
+      active.swap(next);
+    }
+    timed(HIF_KCLASS_ID, 0, 0, [&] { launch_pchol_finish(dpd, nd, max_n, stream); });
+    HIF_CK(cudaGetLastError());
+    // W := R11^{-1} R12, diagonal blocks from the bottom, products above them
+    int kmax = 0;
+    for (int q = 0; q < nd; ++q) kmax = std::max(kmax, info[2 * q]);
+    for (int b = 0; b * kTrsmNB < kmax; ++b) {
+      std::vector<TrsmBlockDesc> tb;
+      std::vector<GemmDesc> up;
+      int maxc = 0;
+      for (int q = 0; q < nd; ++q) {
+        const int k = info[2 * q], nc = pd[q].id.n - k;
+        const int a1 = k - b * kTrsmNB, a0 = std::max(0, a1 - kTrsmNB);
+        if (a1 <= 0 || nc <= 0) continue;
+        tb.push_back(TrsmBlockDesc{pd[q].G, pd[q].id.W, k, nc, a0, a1});
+        maxc = std::max(maxc, nc);
+        if (a0 > 0) {
+          GemmDesc g{};
+          g.C = pd[q].id.W;
+          g.ldc = k;
+          g.A = pd[q].G + (long long)a0 * k;
+          g.lda = k;
+          g.B = pd[q].id.W + a0;
+          g.ldb = k;
+          g.m = a0;
+          g.n = nc;
+          g.k = a1 - a0;
+          g.alpha = -1.0;
+          g.beta = 1.0;
+          up.push_back(g);
+        }
+      }
+      if (tb.empty()) continue;
+      BufList step;
+      TrsmBlockDesc* dtb = step.add(upload(tb, stream));
+      timed(HIF_KCLASS_ID, 0, 0, [&] { launch_trsm_block(dtb, (int)tb.size(), maxc, stream); });
+      gemm_batch(up, step, stream, HIF_KCLASS_ID, tm);
+      HIF_CK(cudaGetLastError());
+      step.release(stream);
+    }
   }
 
   // Blocked Householder row compression of the faces with more than

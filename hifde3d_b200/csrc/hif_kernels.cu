@@ -1894,6 +1894,210 @@ void launch_trsm_upper(const double* R, long long ldr, int k, double* B, long lo
 }
 
 // ===========================================================================
+// Pivoted Cholesky ID (mixed precision mode), one CTA per face.
+// ===========================================================================
+__global__ void __launch_bounds__(512) k_pchol_panel(const PcholDesc* __restrict__ descs,
+                                                     const int* __restrict__ active, int i0,
+                                                     int nb, double eps, int* __restrict__ status) {
+  const PcholDesc P = descs[active[blockIdx.x]];
+  const int n = P.id.n, tid = threadIdx.x, nthr = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = nthr >> 5;
+  extern __shared__ double pc_sm[];
+  double* d = pc_sm;                              // current Schur diagonal
+  int* ch = reinterpret_cast<int*>(pc_sm + n);    // chosen flags
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  __shared__ double pcol[64];                     // R[l, p] for the panel's rows
+  __shared__ int s_p, s_stop;
+  __shared__ double s_dp, s_d0;
+  const double* G = P.G;
+  double* R = P.R;
+  if (P.info[1]) return;
+  if (i0 == 0) {
+    double mx = 0.0;
+    for (int j = tid; j < n; j += nthr) {
+      const double v = G[j + (long long)j * n];
+      d[j] = v;
+      ch[j] = 0;
+      mx = fmax(mx, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red_v[warp] = mx;
+    __syncthreads();
+    if (tid == 0) {
+      double m0 = 0.0;
+      for (int w = 0; w < nw; ++w) m0 = fmax(m0, red_v[w]);
+      s_d0 = m0;
+      *P.d0 = m0;
+      if (!(m0 > 0.0)) atomicOr(status, kStatusIdZero);
+    }
+  } else {
+    for (int j = tid; j < n; j += nthr) {
+      const int c = P.chosen[j];
+      ch[j] = c;
+      d[j] = c ? 0.0 : G[j + (long long)j * n];
+    }
+    if (tid == 0) s_d0 = *P.d0;
+  }
+  if (tid == 0) s_stop = 0;
+  __syncthreads();
+  const double thr = eps * eps * s_d0;
+  const int iend = min(n, i0 + nb);
+  int i = i0;
+  for (; i < iend; ++i) {
+    // pivot: largest remaining diagonal, smallest index on ties
+    double best = -1.0;
+    int bi = INT_MAX;
+    for (int j = tid; j < n; j += nthr)
+      if (!ch[j] && (d[j] > best || (d[j] == best && j < bi))) { best = d[j]; bi = j; }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (lane == 0) { red_v[warp] = best; red_i[warp] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double b = red_v[0];
+      int bb = red_i[0];
+      for (int w = 1; w < nw; ++w)
+        if (red_v[w] > b || (red_v[w] == b && red_i[w] < bb)) { b = red_v[w]; bb = red_i[w]; }
+      s_p = bb;
+      s_dp = b;
+      // R_ii <= eps R_00 (or nothing left): the rank is i
+      if (bb == INT_MAX || !(b > thr)) s_stop = 1;
+      else P.piv[i] = bb;
+    }
+    __syncthreads();
+    if (s_stop) break;
+    const int p = s_p;
+    const double rii = sqrt(s_dp);
+    for (int l = tid; l < i - i0; l += nthr) pcol[l] = R[(long long)(i0 + l) * n + p];
+    __syncthreads();
+    double* Ri = R + (long long)i * n;
+    for (int j = tid; j < n; j += nthr) {
+      if (ch[j]) { Ri[j] = 0.0; continue; }
+      if (j == p) { Ri[j] = rii; continue; }
+      double sacc = G[j + (long long)p * n];
+      for (int l = 0; l < i - i0; ++l) sacc = fma(-pcol[l], R[(long long)(i0 + l) * n + j], sacc);
+      const double r = sacc / rii;
+      Ri[j] = r;
+      d[j] = fma(-r, r, d[j]);
+    }
+    __syncthreads();
+    if (tid == 0) ch[p] = 1;
+    __syncthreads();
+  }
+  for (int j = tid; j < n; j += nthr) P.chosen[j] = ch[j];
+  if (tid == 0) {
+    P.info[0] = i;
+    if (s_stop || i == n) P.info[1] = 1;
+  }
+}
+
+void launch_pchol_panel(const PcholDesc* d_desc, const int* d_active, int nact, int i0, int nb,
+                        double eps, int max_n, int* d_status, cudaStream_t s) {
+  if (nact <= 0) return;
+  const size_t smem = (size_t)max_n * (sizeof(double) + sizeof(int));
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    cudaFuncSetAttribute(k_pchol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = smem;
+  }
+  k_pchol_panel<<<nact, 512, smem, s>>>(d_desc, d_active, i0, nb, eps, d_status);
+}
+
+__global__ void __launch_bounds__(512) k_pchol_finish(const PcholDesc* __restrict__ descs) {
+  const PcholDesc P = descs[blockIdx.x];
+  const int n = P.id.n, tid = threadIdx.x, nthr = blockDim.x;
+  extern __shared__ int pf_sm[];  // order: n
+  __shared__ int s_k;
+  if (tid == 0) {
+    const int k = P.info[0];
+    int q = 0;
+    for (int i = 0; i < k; ++i) pf_sm[q++] = P.piv[i];
+    for (int j = 0; j < n; ++j)
+      if (!P.chosen[j]) pf_sm[q++] = j;
+    s_k = k;
+    *P.id.rank = k;
+  }
+  __syncthreads();
+  const int k = s_k;
+  const double* R = P.R;
+  for (int i = tid; i < n; i += nthr) {
+    P.id.jpvt[i] = pf_sm[i];
+    P.id.keep[i] = i < k;
+    P.id.rdiag[i] = (i < k) ? R[(long long)i * n + pf_sm[i]] : 0.0;
+  }
+  // R11 (k x k, ld k, upper) into G's space; R12 into W (k x (n - k), ld k)
+  double* R11 = P.G;
+  for (long long e = tid; e < (long long)k * k; e += nthr) {
+    const int a = (int)(e % k), b = (int)(e / k);
+    R11[e] = (b >= a) ? R[(long long)a * n + pf_sm[b]] : 0.0;
+  }
+  const int nr = n - k;
+  for (long long e = tid; e < (long long)k * nr; e += nthr) {
+    const int a = (int)(e % k), c = (int)(e / k);
+    P.id.W[e] = R[(long long)a * n + pf_sm[k + c]];
+  }
+}
+
+void launch_pchol_finish(const PcholDesc* d_desc, int nd, int max_n, cudaStream_t s) {
+  if (nd <= 0) return;
+  const size_t smem = (size_t)max_n * sizeof(int);
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    cudaFuncSetAttribute(k_pchol_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = smem;
+  }
+  k_pchol_finish<<<nd, 512, smem, s>>>(d_desc);
+}
+
+// One CTA per (face, 128 columns): the diagonal block of R11 in shared memory,
+// one column of W per thread, back substitution over the block's rows.
+__global__ void __launch_bounds__(128) k_trsm_block(const TrsmBlockDesc* __restrict__ descs,
+                                                    int chunks) {
+  const TrsmBlockDesc t = descs[blockIdx.x / chunks];
+  const int c = (blockIdx.x % chunks) * 128 + threadIdx.x;
+  const int bs = t.a1 - t.a0;
+  extern __shared__ double tb_sm[];
+  double* Rb = tb_sm;                    // kTrsmNB x kTrsmNB
+  double* X = tb_sm + kTrsmNB * kTrsmNB;  // kTrsmNB x 128
+  if (bs <= 0) return;
+  for (int e = threadIdx.x; e < bs * bs; e += blockDim.x) {
+    const int a = e % bs, b = e / bs;
+    Rb[a + b * kTrsmNB] = t.R[(t.a0 + a) + (long long)(t.a0 + b) * t.k];
+  }
+  const bool live = c < t.ncols;
+  if (live)
+    for (int a = 0; a < bs; ++a)
+      X[a * 128 + threadIdx.x] = t.W[(t.a0 + a) + (long long)c * t.k];
+  __syncthreads();
+  if (!live) return;
+  for (int a = bs - 1; a >= 0; --a) {
+    const double xa = X[a * 128 + threadIdx.x] / Rb[a + a * kTrsmNB];
+    X[a * 128 + threadIdx.x] = xa;
+    for (int r = 0; r < a; ++r)
+      X[r * 128 + threadIdx.x] = fma(-Rb[r + a * kTrsmNB], xa, X[r * 128 + threadIdx.x]);
+  }
+  for (int a = 0; a < bs; ++a) t.W[(t.a0 + a) + (long long)c * t.k] = X[a * 128 + threadIdx.x];
+}
+
+void launch_trsm_block(const TrsmBlockDesc* d_desc, int nd, int max_cols, cudaStream_t s) {
+  if (nd <= 0 || max_cols <= 0) return;
+  const int chunks = (max_cols + 127) / 128;
+  const int smem = (kTrsmNB * kTrsmNB + kTrsmNB * 128) * (int)sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_trsm_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  k_trsm_block<<<nd * chunks, 128, smem, s>>>(d_desc, chunks);
+}
+
+// ===========================================================================
 // Apply: batched gather - GEMV - scatter over right-hand sides.
 // trans = 0: 256 output rows per CTA, one row per thread (coalesced along M's
 //            columns); trans = 1: 32 output columns per CTA, one warp per

@@ -85,6 +85,38 @@ struct IdDesc {
   int m, n;
 };
 
+// ---- Interpolative decomposition by pivoted Cholesky of G = M^T M (mixed
+// precision mode). Column-pivoted QR of M and pivoted Cholesky of M^T M choose
+// the same pivots and the same R in exact arithmetic (the pivot is the column
+// with the largest norm orthogonal to the chosen ones, i.e. the largest
+// remaining Schur diagonal); the factorization stops at the first pivot with
+// R_ii <= eps R_00, so only the skeleton rows of R are formed.
+struct PcholDesc {
+  double* G;       // n x n, ld n: M^T M, updated after every panel
+  double* R;       // n x n row-major: row i of R at R + i * n (original column order)
+  int* chosen;     // n
+  int* piv;        // n: pivot of step i
+  int* info;       // [0] steps done, [1] 1 once the rank is known
+  double* d0;      // R_00^2
+  IdDesc id;       // outputs (jpvt, rdiag, keep, rank, W) and n
+};
+// nb steps from step i0 for the active faces; dynamic smem n doubles + n ints.
+void launch_pchol_panel(const PcholDesc* d_desc, const int* d_active, int nact, int i0, int nb,
+                        double eps, int max_n, int* d_status, cudaStream_t s);
+// Outputs after the last panel: jpvt (skeleton pivots, then the redundant
+// columns in increasing order), keep, rdiag, rank; R11 (k x k, ld k, upper) into
+// G's space and R12 into W (k x (n - k), ld k) for the triangular solve.
+void launch_pchol_finish(const PcholDesc* d_desc, int nd, int max_n, cudaStream_t s);
+// Diagonal-block step of W := R11^{-1} W by blocks of kTrsmNB rows from the
+// bottom: rows [a0, a1) of every face's W solved with R11's diagonal block.
+constexpr int kTrsmNB = 64;
+struct TrsmBlockDesc {
+  const double* R;  // k x k, ld k, upper triangular
+  double* W;        // k x ncols, ld k
+  int k, ncols, a0, a1;
+};
+void launch_trsm_block(const TrsmBlockDesc* d_desc, int nd, int max_cols, cudaStream_t s);
+
 // Apply: y = op(M) x[in] with x, y gathered / scattered through DOF lists.
 struct GemvDesc {
   const double* M;
