@@ -801,46 +801,103 @@ void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_statu
 //   update:   B[i, j] -= B[i, K] B[K, j]       for i, j outside K (dgemm)
 //   colpanel: B[i, K] = -B[i, K] Dinv           for red rows i outside K
 //   setdiag:  B[K, K] = Dinv
-__global__ void __launch_bounds__(256) k_sweep_diag(const SweepDesc* __restrict__ descs,
+// Register-resident Gauss-Jordan inverse of the pivot block: thread (tx, ty)
+// of a 16 x 32 grid holds the 4 x 8 sub-block rows 4 ty.., columns 8 tx.. in
+// registers. At step k the owners of the old row k and column k publish them
+// to shared memory (two buffers, alternating, so one barrier per step orders
+// both the reads of step k and the writes of step k + 2); every thread then
+// updates its 32 entries with the same operations as the in-place sweep:
+// row k * (1 / p), column k * (-1 / p), the rest a - a_ik (a_kj / p).
+__global__ void __launch_bounds__(512) k_sweep_diag(const SweepDesc* __restrict__ descs,
                                                     const int* __restrict__ active, int k0,
                                                     double* __restrict__ dinv,
                                                     int* __restrict__ status) {
   const int di = active[blockIdx.x];
   const SweepDesc d = descs[di];
   const int nb = min(kSweepNB, d.r - k0);
-  extern __shared__ double S[];  // nb x nb
-  __shared__ double s_ip;
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    S[e] = d.B[(k0 + i) + (long long)(k0 + j) * d.n];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  __shared__ double rowk[2][kSweepNB], colk[2][kSweepNB];
+  extern __shared__ double dg_sm[];  // kSweepNB x kSweepNB staging (coalesced load / store)
+  for (int e = threadIdx.x; e < kSweepNB * kSweepNB; e += blockDim.x) {
+    const int i = e & (kSweepNB - 1), j = e / kSweepNB;
+    dg_sm[e] = (i < nb && j < nb) ? d.B[(k0 + i) + (long long)(k0 + j) * d.n] : 0.0;
   }
   __syncthreads();
+  double a[4][8];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[r][c] = dg_sm[(4 * ty + r) + (8 * tx + c) * kSweepNB];
   int bad = 0;
   for (int k = 0; k < nb; ++k) {
-    if (threadIdx.x == 0) {
-      const double p = S[k + k * nb];
-      if (!(fabs(p) > 1e-300) || !isfinite(p)) bad = 1;
-      s_ip = 1.0 / p;
+    const int buf = k & 1;
+    if (ty == (k >> 2)) {
+      const int kr = k & 3;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        double v = a[0][c];
+#pragma unroll
+        for (int r = 1; r < 4; ++r)
+          if (r == kr) v = a[r][c];
+        rowk[buf][8 * tx + c] = v;
+      }
+    }
+    if (tx == (k >> 3)) {
+      const int kc = k & 7;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double v = a[r][0];
+#pragma unroll
+        for (int c = 1; c < 8; ++c)
+          if (c == kc) v = a[r][c];
+        colk[buf][4 * ty + r] = v;
+      }
     }
     __syncthreads();
-    const double ip = s_ip;
-    for (int j = threadIdx.x; j < nb; j += blockDim.x)
-      if (j != k) S[k + j * nb] *= ip;
-    __syncthreads();
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-      const int i = e % nb, j = e / nb;
-      if (i == k || j == k) continue;
-      S[e] = fma(-S[i + k * nb], S[k + j * nb], S[e]);
+    const double p = rowk[buf][k];
+    if (threadIdx.x == 0 && (!(fabs(p) > 1e-300) || !isfinite(p))) bad = 1;
+    const double ip = 1.0 / p;
+    double rj[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) rj[c] = rowk[buf][8 * tx + c] * ip;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const double cir = colk[buf][4 * ty + r];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) a[r][c] = fma(-cir, rj[c], a[r][c]);
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nb; i += blockDim.x)
-      if (i != k) S[i + k * nb] *= -ip;
-    if (threadIdx.x == 0) S[k + k * nb] = ip;
-    __syncthreads();
+    // row k, column k and the pivot replace what the general update wrote there
+    if (ty == (k >> 2)) {
+      const int kr = k & 3;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (r == kr) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c) a[r][c] = rj[c];
+        }
+    }
+    if (tx == (k >> 3)) {
+      const int kc = k & 7;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c == kc) {
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            a[r][c] = (4 * ty + r == k) ? ip : colk[buf][4 * ty + r] * -ip;
+        }
+    }
   }
   if (bad) atomicOr(status, kStatusTinyPivot);
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) dg_sm[(4 * ty + r) + (8 * tx + c) * kSweepNB] = a[r][c];
+  __syncthreads();
   double* out = dinv + (long long)di * kSweepNB * kSweepNB;
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) out[e] = S[e];
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int i = e % nb, j = e / nb;
+    out[e] = dg_sm[i + j * kSweepNB];
+  }
 }
 
 void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
@@ -852,7 +909,7 @@ void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, i
     cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     attr = true;
   }
-  k_sweep_diag<<<nact, 256, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
+  k_sweep_diag<<<nact, 512, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
 }
 
 // Row panel: tile of up to 64 columns [lo, hi) of rows K.
