@@ -80,10 +80,66 @@ void dfree(void* p, cudaStream_t s) {
   if (p) cudaFreeAsync(p, s);
 }
 
+// Pinned host staging for the host -> device copies of a factorization. A copy
+// from pageable memory may make the driver wait for the stream before staging
+// it, which would stall the host behind the GPU at every descriptor upload;
+// from pinned memory the copy is queued and the host goes on. The staging is
+// bump-allocated in chunks kept for the owner's life and reused from the start
+// once the owner has synchronised (its copies are then complete).
+struct PinnedStage {
+  struct Chunk {
+    char* p;
+    size_t size, used;
+  };
+  std::vector<Chunk> chunks;
+  size_t cur = 0;
+  static constexpr size_t kMinChunk = size_t(32) << 20;
+  void* get(size_t bytes) {
+    bytes = (bytes + 255) & ~size_t(255);
+    for (; cur < chunks.size(); ++cur) {
+      Chunk& c = chunks[cur];
+      if (c.size - c.used >= bytes) {
+        void* r = c.p + c.used;
+        c.used += bytes;
+        return r;
+      }
+    }
+    const size_t sz = std::max(bytes, kMinChunk);
+    void* p = nullptr;
+    HIF_CK(cudaHostAlloc(&p, sz, cudaHostAllocDefault));
+    chunks.push_back(Chunk{static_cast<char*>(p), sz, bytes});
+    cur = chunks.size() - 1;
+    return p;
+  }
+  void reset() {
+    for (Chunk& c : chunks) c.used = 0;
+    cur = 0;
+  }
+  void release() {
+    for (Chunk& c : chunks) cudaFreeHost(c.p);
+    chunks.clear();
+    cur = 0;
+  }
+  ~PinnedStage() { release(); }
+};
+// Staging used by upload() on this thread (set while a factorization runs).
+thread_local PinnedStage* t_stage = nullptr;
+
+void copy_to_device(void* d, const void* h, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return;
+  if (t_stage) {
+    void* p = t_stage->get(bytes);
+    std::memcpy(p, h, bytes);
+    HIF_CK(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, s));
+  } else {
+    HIF_CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s));
+  }
+}
+
 template <class T>
 T* upload(const std::vector<T>& v, cudaStream_t s) {
   T* d = dalloc<T>(v.size(), s);
-  if (!v.empty()) HIF_CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  copy_to_device(d, v.data(), v.size() * sizeof(T), s);
   return d;
 }
 
@@ -159,8 +215,7 @@ struct Arena {
   template <class T>
   T* upload(const std::vector<T>& v, cudaStream_t s) {
     T* d = alloc<T>(v.size());
-    if (!v.empty())
-      HIF_CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    copy_to_device(d, v.data(), v.size() * sizeof(T), s);
     return d;
   }
   void reset() {
@@ -238,7 +293,8 @@ struct ApplyPlan {
 struct Sources {
   std::vector<SourceDesc> desc;
   std::vector<int> owner;      // target cell (next Schur phase) that sums this source
-  std::vector<int> dof_src;    // 6 x NC^3 membership arrays (see GatherTarget)
+  // the 6 x NC^3 membership arrays (see GatherTarget) live on the device,
+  // in Engine::d_dof_src, one set at a time
   std::vector<int> cell_src;   // cell index -> source id (T_c), -1 if none
   BufList bufs;                // device memory holding the blocks
 };
@@ -526,6 +582,7 @@ class Engine {
   double t_total = 0, t_gather = 0, t_elim = 0, t_id = 0, t_host = 0, t_plan = 0;
   long long peak_bytes = 0, cur_bytes = 0;
   int* d_status = nullptr;
+  int* d_dof_src = nullptr;  // source membership, 6 x NC^3 (see Sources)
 
   // ---- per-kernel-class timing (HIF_OPT_PROFILE): CUDA events on the engine
   // stream around each launch, with the launch's algorithmic flops / bytes.
@@ -634,6 +691,7 @@ class Engine {
     arena_work[1].release();
     dfree(d_band, stream);
     dfree(d_status, stream);
+    dfree(d_dof_src, stream);
     cudaStreamSynchronize(stream);
     cudaStreamSynchronize(own_stream);
     cudaStreamDestroy(own_stream);
@@ -751,14 +809,16 @@ class Engine {
                       int** d_dof) {
     *d_desc = tmp.add(upload(s.desc, stream));
     *d_owner = tmp.add(upload(s.owner, stream));
-    *d_dof = tmp.add(upload(s.dof_src, stream));
+    *d_dof = d_dof_src;
   }
 
+  // Stream-ordered after every gather that read the previous membership.
   void empty_sources(Sources& s, int ncells) {
     s.desc.clear();
     s.owner.clear();
-    s.dof_src.assign(6 * n3, -1);
     s.cell_src.assign(ncells, -1);
+    if (!d_dof_src) d_dof_src = dalloc<int>(6 * n3, stream);
+    HIF_CK(cudaMemsetAsync(d_dof_src, 0xFF, 6 * n3 * sizeof(int), stream));
   }
 
   // ---- Schur phase (LevelFactorSchur, src/Factor.cpp:184-213) ------------
@@ -791,6 +851,7 @@ class Engine {
     st.o_skel.resize(ncell);
     std::vector<int> rows_all;
     std::vector<long long> o_rows(ncell);
+    long long nred = 0, nskel = 0;
     for (int b = 0; b < ncell; ++b) {
       const BlockInfo& bi = st.blocks[b];
       const long long n = bi.global.size(), r = bi.r(), s = bi.s();
@@ -802,18 +863,29 @@ class Engine {
       asz += r * r;
       st.o_x[b] = asz;
       asz += r * s;
-      st.o_red[b] = red_all.size();
-      st.o_skel[b] = skel_all.size();
-      o_rows[b] = rows_all.size();
-      for (int p : bi.red_pos) {
-        red_all.push_back(bi.global[p]);
-        rows_all.push_back(bi.global[p]);
-      }
-      for (int p : bi.skel_pos) {
-        skel_all.push_back(bi.global[p]);
-        rows_all.push_back(bi.global[p]);
-      }
+      st.o_red[b] = nred;
+      st.o_skel[b] = nskel;
+      o_rows[b] = nred + nskel;
+      nred += r;
+      nskel += s;
     }
+    red_all.resize(nred);
+    skel_all.resize(nskel);
+    rows_all.resize(nred + nskel);
+    parallel_for(ncell, [&](int b) {
+      const BlockInfo& bi = st.blocks[b];
+      long long q = o_rows[b];
+      for (size_t t = 0; t < bi.red_pos.size(); ++t) {
+        const int g = bi.global[bi.red_pos[t]];
+        red_all[st.o_red[b] + t] = g;
+        rows_all[q++] = g;
+      }
+      for (size_t t = 0; t < bi.skel_pos.size(); ++t) {
+        const int g = bi.global[bi.skel_pos[t]];
+        skel_all[st.o_skel[b] + t] = g;
+        rows_all[q++] = g;
+      }
+    });
     st.n_red = red_all.size();
     st.n_skel = skel_all.size();
     t_host += wall() - th;
@@ -917,16 +989,14 @@ class Engine {
       const int parent = cpd_next > 0 ? ((ci / 2) * cpd_next + cj / 2) * cpd_next + ck / 2 : -1;
       out.owner.push_back(parent);
       out.cell_src[b] = id;
-      const int c[3] = {ci, cj, ck};
-      for (int t = 0; t < s; ++t) {
-        const int p = bi.global[bi.skel_pos[t]];
-        const int x[3] = {p % NC, (p / NC) % NC, p / (NC * NC)};
-        int slot = 1;  // high face
-        for (int a = 0; a < 3; ++a)
-          if (x[a] % w == 0 && x[a] == w * c[a]) slot = 0;  // low face
-        out.dof_src[(2 * slot) * n3 + p] = id;
-        out.dof_src[(2 * slot + 1) * n3 + p] = t;
-      }
+    }
+    {
+      std::vector<long long> off(st.o_skel.begin(), st.o_skel.end());
+      off.push_back(st.n_skel);
+      long long* d_off = tmp.add(upload(off, stream));
+      int* d_src = tmp.add(upload(out.cell_src, stream));
+      launch_member_cells(st.d_skel, d_off, d_src, ncell, cpd, w, NC, d_dof_src, stream);
+      HIF_CK(cudaGetLastError());
     }
     // remove eliminated DOFs (UpdateRemainingDOFs, src/Factor.cpp:91-111)
     for (int p : red_all) rem[p] = 0;
@@ -974,17 +1044,15 @@ class Engine {
     }
     const int nf = (int)blocks.size();
     // M blocks (rows x cols) and ID workspace
-    std::vector<int> idx_all;
     std::vector<long long> o_rows(nf), o_cols(nf), o_M(nf), o_W(nf), o_i(nf);
-    long long msz = 0, wsz = 0, isz = 0;
+    long long msz = 0, wsz = 0, isz = 0, xsz = 0;
     int max_n = 0;
     for (int f = 0; f < nf; ++f) {
       const int m = rows_l[f].size(), n = blocks[f].global.size();
       if (m < n) throw Error{HIF_ERR_STATE, "face with fewer interaction rows than columns"};
-      o_rows[f] = idx_all.size();
-      idx_all.insert(idx_all.end(), rows_l[f].begin(), rows_l[f].end());
-      o_cols[f] = idx_all.size();
-      idx_all.insert(idx_all.end(), blocks[f].global.begin(), blocks[f].global.end());
+      o_rows[f] = xsz;
+      o_cols[f] = xsz + m;
+      xsz += m + n;
       o_M[f] = msz;
       msz += (long long)m * n;
       o_W[f] = wsz;
@@ -993,6 +1061,12 @@ class Engine {
       isz += n;
       max_n = std::max(max_n, n);
     }
+    // row and column lists of every face, filled in parallel
+    std::vector<int> idx_all(xsz);
+    parallel_for(nf, [&](int f) {
+      std::copy(rows_l[f].begin(), rows_l[f].end(), idx_all.begin() + o_rows[f]);
+      std::copy(blocks[f].global.begin(), blocks[f].global.end(), idx_all.begin() + o_cols[f]);
+    });
     t_host += wall() - th;
 
     BufList tmp;
@@ -1168,7 +1242,7 @@ class Engine {
     st.o_w.resize(nf);
     st.o_red.resize(nf);
     st.o_skel.resize(nf);
-    for (int f = 0; f < nf; ++f) {
+    parallel_for(nf, [&](int f) {
       BlockInfo& b = blocks[f];
       const int n = b.global.size();
       b.jpvt.assign(h_jp.begin() + o_i[f], h_jp.begin() + o_i[f] + n);
@@ -1177,6 +1251,11 @@ class Engine {
         if (h_keep[o_i[f] + i]) b.skel_pos.push_back(b.jpvt[i]);
         else b.red_pos.push_back(b.jpvt[i]);
       }
+    });
+    long long nred = 0, nskel = 0;
+    for (int f = 0; f < nf; ++f) {
+      const BlockInfo& b = blocks[f];
+      const int n = b.global.size();
       const long long r = b.r(), k = b.s();
       o_B[f] = bsz;
       bsz += (long long)n * n;
@@ -1188,18 +1267,29 @@ class Engine {
       asz += r * k;
       st.o_w[f] = asz;
       asz += k * r;
-      st.o_red[f] = red_all.size();
-      st.o_skel[f] = skel_all.size();
-      o_r2[f] = rows2.size();
-      for (int p : b.red_pos) {
-        red_all.push_back(b.global[p]);
-        rows2.push_back(b.global[p]);
-      }
-      for (int p : b.skel_pos) {
-        skel_all.push_back(b.global[p]);
-        rows2.push_back(b.global[p]);
-      }
+      st.o_red[f] = nred;
+      st.o_skel[f] = nskel;
+      o_r2[f] = nred + nskel;
+      nred += r;
+      nskel += k;
     }
+    red_all.resize(nred);
+    skel_all.resize(nskel);
+    rows2.resize(nred + nskel);
+    parallel_for(nf, [&](int f) {
+      const BlockInfo& b = blocks[f];
+      long long q = o_r2[f];
+      for (size_t t = 0; t < b.red_pos.size(); ++t) {
+        const int g = b.global[b.red_pos[t]];
+        red_all[st.o_red[f] + t] = g;
+        rows2[q++] = g;
+      }
+      for (size_t t = 0; t < b.skel_pos.size(); ++t) {
+        const int g = b.global[b.skel_pos[t]];
+        skel_all[st.o_skel[f] + t] = g;
+        rows2[q++] = g;
+      }
+    });
     st.n_red = red_all.size();
     st.n_skel = skel_all.size();
     t_host += wall() - th;
@@ -1259,10 +1349,12 @@ class Engine {
     // new sources: S_f of faces that eliminated something
     th = wall();
     const int cpd_next = cells_per_dir(level + 1);
-    out.dof_src = std::move(cells.dof_src);  // cell memberships stay (T_c are still live)
+    // cell memberships stay (T_c are still live): slots 0-3 of d_dof_src
     out.desc = cells.desc;
     out.owner = cells.owner;
     out.cell_src = cells.cell_src;
+    std::vector<long long> mo;
+    std::vector<int> mc, ms;
     for (int f : act) {
       const BlockInfo& b = blocks[f];
       const int r = b.r(), k = b.s(), n = b.global.size();
@@ -1271,11 +1363,16 @@ class Engine {
       out.desc.push_back(SourceDesc{dB + o_B[f] + r + (long long)r * n, (long long)n});
       const int ci = b.cell / (cpd * cpd), cj = (b.cell / cpd) % cpd, ck = b.cell % cpd;
       out.owner.push_back(((ci / 2) * cpd_next + cj / 2) * cpd_next + ck / 2);
-      for (int t = 0; t < k; ++t) {
-        const int p = b.global[b.skel_pos[t]];
-        out.dof_src[4 * n3 + p] = id;
-        out.dof_src[5 * n3 + p] = t;
-      }
+      mo.push_back(st.o_skel[f]);
+      mc.push_back(k);
+      ms.push_back(id);
+    }
+    if (!mo.empty()) {
+      long long* d_mo = tmp.add(upload(mo, stream));
+      int* d_mc = tmp.add(upload(mc, stream));
+      int* d_ms = tmp.add(upload(ms, stream));
+      launch_member_faces(st.d_skel, d_mo, d_mc, d_ms, (int)mo.size(), n3, d_dof_src, stream);
+      HIF_CK(cudaGetLastError());
     }
     // T_c buffers move to the output set; add this phase's B
     out.bufs.p = cells.bufs.p;
@@ -1718,8 +1815,20 @@ class Engine {
   }
 
   // ---- Factor (src/Factor.cpp:41-63) --------------------------------------
+  PinnedStage stage;  // host staging of this handle's factorization uploads
+  struct StageScope {
+    PinnedStage* prev;
+    explicit StageScope(PinnedStage* s) : prev(t_stage) { t_stage = s; }
+    ~StageScope() { t_stage = prev; }
+  };
+
   void factor() {
     if (!have_op) throw Error{HIF_ERR_STATE, "no operator: call hif_setup_stencil first"};
+    // the previous factorization ended with a synchronisation: its staged
+    // copies are complete
+    sync();
+    stage.reset();
+    StageScope scope(&stage);
     if (partition == HIF_PARTITION_CLIPPED && NC % P != 0)
       throw Error{HIF_ERR_ARG, "clipped partition needs (N+1) divisible by P"};
     initialize();

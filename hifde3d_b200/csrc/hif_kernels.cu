@@ -2155,6 +2155,53 @@ void launch_trsm_block(const TrsmBlockDesc* d_desc, int nd, int max_cols, cudaSt
 }
 
 // ===========================================================================
+// Source membership (one CTA per cell / face)
+// ===========================================================================
+__global__ void k_member_cells(const int* __restrict__ skel, const long long* __restrict__ off,
+                               const int* __restrict__ src, int cpd, int w, int NC,
+                               int* __restrict__ dof_src) {
+  const int b = blockIdx.x;
+  const int id = src[b];
+  if (id < 0) return;
+  const long long n3 = (long long)NC * NC * NC;
+  const int c[3] = {b / (cpd * cpd), (b / cpd) % cpd, b % cpd};
+  const long long o = off[b], s = off[b + 1] - o;
+  for (long long t = threadIdx.x; t < s; t += blockDim.x) {
+    const int p = skel[o + t];
+    const int x[3] = {p % NC, (p / NC) % NC, p / (NC * NC)};
+    int slot = 1;  // high face
+    for (int a = 0; a < 3; ++a)
+      if (x[a] % w == 0 && x[a] == w * c[a]) slot = 0;  // low face
+    dof_src[(2 * slot) * n3 + p] = id;
+    dof_src[(2 * slot + 1) * n3 + p] = (int)t;
+  }
+}
+
+void launch_member_cells(const int* d_skel, const long long* d_off, const int* d_src, int ncell,
+                         int cpd, int w, int NC, int* d_dof_src, cudaStream_t s) {
+  if (ncell <= 0) return;
+  k_member_cells<<<ncell, 128, 0, s>>>(d_skel, d_off, d_src, cpd, w, NC, d_dof_src);
+}
+
+__global__ void k_member_faces(const int* __restrict__ skel, const long long* __restrict__ off,
+                               const int* __restrict__ cnt, const int* __restrict__ src,
+                               long long n3, int* __restrict__ dof_src) {
+  const int q = blockIdx.x;
+  const long long o = off[q];
+  for (int t = threadIdx.x; t < cnt[q]; t += blockDim.x) {
+    const int p = skel[o + t];
+    dof_src[4 * n3 + p] = src[q];
+    dof_src[5 * n3 + p] = t;
+  }
+}
+
+void launch_member_faces(const int* d_skel, const long long* d_off, const int* d_cnt,
+                         const int* d_src, int nq, long long n3, int* d_dof_src, cudaStream_t s) {
+  if (nq <= 0) return;
+  k_member_faces<<<nq, 128, 0, s>>>(d_skel, d_off, d_cnt, d_src, n3, d_dof_src);
+}
+
+// ===========================================================================
 // Apply: batched gather - GEMV - scatter over right-hand sides.
 // trans = 0: 256 output rows per CTA, one row per thread (coalesced along M's
 //            columns); trans = 1: 32 output columns per CTA, one warp per

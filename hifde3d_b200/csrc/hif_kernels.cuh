@@ -117,6 +117,15 @@ struct TrsmBlockDesc {
 };
 void launch_trsm_block(const TrsmBlockDesc* d_desc, int nd, int max_cols, cudaStream_t s);
 
+// Source membership of the DOFs (the 6 x NC^3 arrays read by k_gather), built
+// on the device. Cells: skeleton DOF t of cell b (cell_ids[b] >= 0) gets
+// (source, t) in slot pair 0 (on the cell's low face along some axis) or 1.
+void launch_member_cells(const int* d_skel, const long long* d_off, const int* d_src, int ncell,
+                         int cpd, int w, int NC, int* d_dof_src, cudaStream_t s);
+// Faces: skeleton DOF t of listed face q gets (d_src[q], t) in slot pair 2.
+void launch_member_faces(const int* d_skel, const long long* d_off, const int* d_cnt,
+                         const int* d_src, int nq, long long n3, int* d_dof_src, cudaStream_t s);
+
 // Apply: y = op(M) x[in] with x, y gathered / scattered through DOF lists.
 struct GemvDesc {
   const double* M;

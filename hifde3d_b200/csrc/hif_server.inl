@@ -211,6 +211,7 @@ class Server {
         e->sync();
         peak = (long long)(e->arena_factor.reserved() + e->arena_work[0].reserved() +
                            e->arena_work[1].reserved());
+        e->stage.release();
         e->arena_work[0].release();
         e->arena_work[1].release();
         e->release_workspace();  // solves use their own vectors
