@@ -310,17 +310,43 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
   if (gin.empty()) return;
   if (mixed_status) {  // split-TF32 tensor-core path (Schur-complement updates)
     double fl = 0;
-    std::vector<int> toff(1, 0);
+    long long tiles = 0;
     for (const GemmDesc& x : gin) {
+      if (x.m <= 0 || x.n <= 0) continue;
+      const long long kt = (x.k + 31) / 32;
+      tiles += ((x.m + 127) / 128 + (x.n + 127) / 128) * kt;
+    }
+    unsigned char* cbuf = tmp.add(dalloc<unsigned char>(std::max(1LL, tiles) * kTcTileBytes, stream));
+    std::vector<TcOperand> ops;
+    std::vector<int> ooff(1, 0);
+    std::vector<TcGemm> tg;
+    std::vector<int> toff(1, 0);
+    long long used = 0;
+    for (const GemmDesc& x : gin) {
+      if (x.m <= 0 || x.n <= 0) continue;
       fl += 2.0 * x.m * x.n * x.k;
-      toff.push_back(toff.back() + dgemm_tiles(x.m, x.n, 128));
+      const int kt = (x.k + 31) / 32;
+      const int ta = (x.m + 127) / 128 * kt, tb = (x.n + 127) / 128 * kt;
+      unsigned char* pa = cbuf + used * kTcTileBytes;
+      unsigned char* pb = cbuf + (used + ta) * kTcTileBytes;
+      used += ta + tb;
+      // A: element (i, kk) = op(A)[i, kk]; B: element (j, kk) = op(B)[kk, j]
+      ops.push_back(TcOperand{x.A, x.lda, x.transA, x.m, x.k, pa});
+      ooff.push_back(ooff.back() + ta);
+      ops.push_back(TcOperand{x.B, x.ldb, x.transB ? 0 : 1, x.n, x.k, pb});
+      ooff.push_back(ooff.back() + tb);
+      tg.push_back(TcGemm{pa, pb, x.C, x.ldc, x.m, x.n, x.k, x.alpha, x.beta});
+      toff.push_back(toff.back() + (x.m + 127) / 128 * ((x.n + 127) / 128));
     }
     if (toff.back() == 0) return;
-    GemmDesc* dg = tmp.add(upload(gin, stream));
+    TcOperand* dops = tmp.add(upload(ops, stream));
+    int* doo = tmp.add(upload(ooff, stream));
+    TcGemm* dg = tmp.add(upload(tg, stream));
     int* dt = tmp.add(upload(toff, stream));
-    timed(HIF_KCLASS_GEMM_MIXED, fl, 0.0,
-          [&] { launch_gemm_mixed(dg, dt, (int)gin.size(), toff.back(), mixed_status, stream); },
-          1);
+    timed(HIF_KCLASS_GEMM_MIXED, fl, 0.0, [&] {
+      launch_tc_convert(dops, doo, (int)ops.size(), ooff.back(), stream);
+      launch_gemm_tc(dg, dt, (int)tg.size(), toff.back(), mixed_status, stream);
+    }, 2);
     HIF_CK(cudaGetLastError());
     return;
   }

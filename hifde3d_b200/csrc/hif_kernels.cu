@@ -455,28 +455,36 @@ __device__ __forceinline__ unsigned tf32_of(float x) {
 }
 
 // ===========================================================================
-// Split-TF32 GEMM on the 5th-generation tensor cores (tcgen05). One CTA per
-// 128 x 128 tile of C; k runs in stages of 32. All 8 warps load the FP64
-// operands of a stage, split each value into a TF32 pair (hi = rn(x),
-// lo = rn(x - hi)) and store the four parts (A hi / lo, B hi / lo) in shared
-// memory in the K-major canonical layout without swizzle: 8-row x 16-byte
-// core matrices, 128 bytes each, K-adjacent core matrices 128 bytes apart
-// (LBO), 8-row groups 1024 bytes apart (SBO). One thread issues, per k-step of
-// 8, the products lo*hi, hi*lo, hi*hi (M = 128, N = 128, K = 8, FP32
-// accumulation in tensor memory) and commits them to the stage's mbarrier,
-// which the loaders wait on before refilling that stage. After every 256
-// values of k the accumulator is read with tcgen05.ld (warp w reads lanes
-// 32 (w % 4) .. + 31, columns 64 (w / 4) .. + 63) and added to C in FP64
-// (the first chunk writes alpha acc + beta C), so FP32 sums never run over
-// more than 256 terms.
-// Every mbarrier wait is bounded (globaltimer, 2 s): on timeout the status
-// word gets kStatusTimeout, the tile is not written and the CTA still frees
-// its tensor memory.
+// Split-TF32 GEMM on the 5th-generation tensor cores (tcgen05).
+//
+// 1. k_tc_convert splits every FP64 operand value into a TF32 pair
+//    (hi = rn(x), lo = rn(x - hi)) and stores the pairs as tiles of 128 rows
+//    x 32 values of k in the K-major canonical layout without swizzle that the
+//    tensor cores read from shared memory: 8-row x 16-byte core matrices of
+//    128 bytes, K-adjacent ones 128 bytes apart (LBO), 8-row groups 1024 bytes
+//    apart (SBO); a tile is 16 KB of hi followed by 16 KB of lo.
+// 2. k_gemm_tc computes one 128 x 128 tile of C per CTA with warp roles:
+//    one thread of warp 0 brings the A and B tiles of each k step into a
+//    3-stage ring with bulk asynchronous copies (cp.async.bulk, completion
+//    counted in bytes on the stage's mbarrier); one thread of warp 1 issues,
+//    per k-step of 8, the products lo*hi, hi*lo, hi*hi (M = N = 128, K = 8,
+//    FP32 accumulation in tensor memory) and releases the stage with
+//    tcgen05.commit; warps 4-7 read the accumulator (warp w: lanes
+//    32 (w - 4) .. + 31) every 256 values of k and add it to an FP64
+//    accumulator that also lives in tensor memory (two 32-bit columns per
+//    value), so no FP32 sum runs over more than 256 terms and C is read and
+//    written once (alpha acc + beta C). Two FP32 accumulators alternate, so
+//    the products of the next chunk proceed while one is read; the CTA holds
+//    all 512 tensor-memory columns (one CTA per SM by its shared memory).
+// Every mbarrier wait is bounded (globaltimer, 2 s); a wait that runs out
+// marks the CTA aborted (every role stops waiting), records kStatusTimeout and
+// leaves the tile unwritten; the CTA still frees its tensor memory.
 // ===========================================================================
-constexpr int kTcM = 128, kTcN = 128, kTcK = 32, kTcStages = 2, kTcChunk = 256;
-constexpr int kTcPart = kTcM * kTcK * 4;             // bytes of one operand part per stage
-constexpr int kTcStage = 4 * kTcPart;                // A hi, A lo, B hi, B lo
-constexpr int kTcSmem = kTcStages * kTcStage + 128;  // + mbarriers, tensor memory address
+constexpr int kTcM = 128, kTcN = 128, kTcK = 32, kTcStages = 3, kTcChunk = 256;
+constexpr int kTcPart = kTcM * kTcK * 4;             // bytes of one operand part (hi or lo)
+constexpr int kTcTile = 2 * kTcPart;                 // one converted operand tile (hi, lo)
+constexpr int kTcStage = 2 * kTcTile;                // A tile, B tile
+constexpr int kTcSmem = kTcStages * kTcStage + 256;  // + mbarriers, tensor memory address
 constexpr unsigned long long kTcWaitNs = 2000000000ull;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -489,8 +497,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Bounded wait for the completion of the mbarrier phase with the given parity.
-__device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity) {
+// Bounded wait for the completion of the mbarrier phase with the given parity;
+// gives up at once when *abort is set, and sets it when the time runs out.
+__device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity,
+                                          volatile int* abort = nullptr) {
   const unsigned long long t0 = global_ns();
   for (;;) {
     unsigned done;
@@ -502,7 +512,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity) {
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
-    if (global_ns() - t0 > kTcWaitNs) return false;
+    if (abort && *abort) return false;
+    if (global_ns() - t0 > kTcWaitNs) {
+      if (abort) *abort = 1;
+      return false;
+    }
   }
 }
 
@@ -526,29 +540,84 @@ __device__ __forceinline__ int tc_off(int row, int kc) {
   return (((row >> 3) * (kTcK / 4) + kc) << 7) + ((row & 7) << 4);
 }
 
-__global__ void __launch_bounds__(256, 1) k_gemm_tc(const GemmDesc* __restrict__ descs,
+__global__ void __launch_bounds__(256) k_tc_convert(const TcOperand* __restrict__ ops,
+                                                    const int* __restrict__ tile_off, int nops) {
+  const int oi = find_desc(tile_off, nops, blockIdx.x);
+  const TcOperand o = ops[oi];
+  const int local = blockIdx.x - tile_off[oi];
+  const int kt_n = (o.kdim + kTcK - 1) / kTcK;
+  const int rt = local / kt_n, kt = local % kt_n;
+  unsigned char* dst = o.out + (size_t)local * kTcTile;
+  const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
+  const int gi = rt * kTcM + row;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int kc = half + 2 * i;
+    uint4 h, l;
+    unsigned* ph = &h.x;
+    unsigned* pl = &l.x;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int gk = kt * kTcK + 4 * kc + e;
+      const double x = (gi < o.rows && gk < o.kdim)
+                           ? (o.trans ? o.X[gk + (long long)gi * o.ld] : o.X[gi + (long long)gk * o.ld])
+                           : 0.0;
+      const float f = (float)x;
+      const unsigned fh = tf32_of(f);
+      ph[e] = fh;
+      pl[e] = tf32_of(f - __uint_as_float(fh));
+    }
+    const int off = tc_off(row, kc);
+    *reinterpret_cast<uint4*>(dst + off) = h;
+    *reinterpret_cast<uint4*>(dst + kTcPart + off) = l;
+  }
+}
+
+void launch_tc_convert(const TcOperand* d_ops, const int* d_tile_off, int nops, int total_tiles,
+                       cudaStream_t s) {
+  if (total_tiles <= 0) return;
+  k_tc_convert<<<total_tiles, 256, 0, s>>>(d_ops, d_tile_off, nops);
+}
+
+__global__ void __launch_bounds__(256, 1) k_gemm_tc(const TcGemm* __restrict__ descs,
                                                     const int* __restrict__ tile_off, int nd,
                                                     int* __restrict__ status) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tc_smem + kTcStages * kTcStage);
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(tc_smem + kTcStages * kTcStage + 64);
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(tc_smem + kTcStages * kTcStage);
+  unsigned long long* full = bars;                  // [kTcStages]
+  unsigned long long* empty = bars + kTcStages;     // [kTcStages]
+  unsigned long long* tfull = bars + 2 * kTcStages;  // [2]
+  unsigned long long* tempty = tfull + 2;            // [2]
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(tempty + 2);
+  volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int di = find_desc(tile_off, nd, blockIdx.x);
-  const GemmDesc g = descs[di];
+  const TcGemm g = descs[di];
   const int local = blockIdx.x - tile_off[di];
   const int tiles_m = (g.m + kTcM - 1) / kTcM;
-  const int m0 = (local % tiles_m) * kTcM, n0 = (local / tiles_m) * kTcN;
+  const int mt = local % tiles_m, nt = local / tiles_m;
+  const int m0 = mt * kTcM, n0 = nt * kTcN;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kt_n = (g.k + kTcK - 1) / kTcK;
+  constexpr int spc = kTcChunk / kTcK;  // k steps per chunk
+  const int nchunk = (kt_n + spc - 1) / spc;
 
-  if (warp == 0) {
+  if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(kTcN)
+                 "r"(4 * kTcN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
+    for (int q = 0; q < kTcStages; ++q) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[q])) : "memory");
+    }
+    for (int q = 0; q < 2; ++q) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&tfull[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&tempty[q])) : "memory");
+    }
+    *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -556,107 +625,42 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const GemmDesc* __restrict__
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const unsigned tmem = *tmem_slot;
 
-  // loader mapping: row = tid % 128 of the tile, k chunks (4 values) half, half + 2, ...
-  const int lr = tid & 127, lh = tid >> 7;
-  double ra[16], rb[16];
-  auto load = [&](int k0) {
-    const int gm = m0 + lr, gn = n0 + lr;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int kc = lh + 2 * i;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int gk = k0 + 4 * kc + e;
-        const bool ka = gk < g.k;
-        ra[4 * i + e] = (ka && gm < g.m) ? (g.transA == 0 ? g.A[gm + (long long)gk * g.lda]
-                                                         : g.A[gk + (long long)gm * g.lda])
-                                         : 0.0;
-        rb[4 * i + e] = (ka && gn < g.n) ? (g.transB == 0 ? g.B[gk + (long long)gn * g.ldb]
-                                                         : g.B[gn + (long long)gk * g.ldb])
-                                         : 0.0;
-      }
-    }
-  };
-  auto store = [&](int s) {
-    unsigned char* st = tc_smem + s * kTcStage;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int off = tc_off(lr, lh + 2 * i);
-      uint4 ah, al, bh, bl;
-      unsigned* pah = &ah.x;
-      unsigned* pal = &al.x;
-      unsigned* pbh = &bh.x;
-      unsigned* pbl = &bl.x;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const float x = (float)ra[4 * i + e];
-        const unsigned xh = tf32_of(x);
-        pah[e] = xh;
-        pal[e] = tf32_of(x - __uint_as_float(xh));
-        const float y = (float)rb[4 * i + e];
-        const unsigned yh = tf32_of(y);
-        pbh[e] = yh;
-        pbl[e] = tf32_of(y - __uint_as_float(yh));
-      }
-      *reinterpret_cast<uint4*>(st + 0 * kTcPart + off) = ah;
-      *reinterpret_cast<uint4*>(st + 1 * kTcPart + off) = al;
-      *reinterpret_cast<uint4*>(st + 2 * kTcPart + off) = bh;
-      *reinterpret_cast<uint4*>(st + 3 * kTcPart + off) = bl;
-    }
-  };
-
-  // C (FP64) accumulates the FP32 tensor-memory sums chunk by chunk
-  // (kTcChunk values of k each), so no FP32 sum runs over more terms.
-  const int q4 = warp & 3, h2 = warp >> 2;
-  const int em = m0 + 32 * q4 + lane;
-  auto drain = [&](bool first) {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      unsigned v[16];
-      const unsigned taddr = tmem + ((unsigned)(32 * q4) << 16) + (unsigned)(64 * h2 + 16 * c);
+  if (warp == 0 && lane == 0) {
+    // producer: bulk copies of the converted A and B tiles
+    const unsigned char* a_src = g.A + (size_t)mt * kt_n * kTcTile;
+    const unsigned char* b_src = g.B + (size_t)nt * kt_n * kTcTile;
+    for (int kt = 0; kt < kt_n; ++kt) {
+      const int s = kt % kTcStages;
+      if (kt >= kTcStages &&
+          !mbar_wait(smem_u32(&empty[s]), (unsigned)((kt / kTcStages - 1) & 1), abort))
+        break;
+      const unsigned fb = smem_u32(&full[s]);
+      const unsigned dst = smem_u32(tc_smem + s * kTcStage);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                   "r"(kTcStage)
+                   : "memory");
       asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
-          "%13,%14,%15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(taddr)
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+          "[%3];" ::"r"(dst),
+          "l"(a_src + (size_t)kt * kTcTile), "r"(kTcTile), "r"(fb)
           : "memory");
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (em < g.m) {
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-          const int gn = n0 + 64 * h2 + 16 * c + e;
-          if (gn < g.n) {
-            double* cp = g.C + em + (long long)gn * g.ldc;
-            const double val = g.alpha * (double)__uint_as_float(v[e]);
-            if (first) *cp = (g.beta == 0.0) ? val : fma(g.beta, *cp, val);
-            else *cp += val;
-          }
-        }
-      }
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+          "[%3];" ::"r"(dst + kTcTile),
+          "l"(b_src + (size_t)kt * kTcTile), "r"(kTcTile), "r"(fb)
+          : "memory");
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  };
-
-  const int nk = (g.k + kTcK - 1) / kTcK;
-  constexpr int spc = kTcChunk / kTcK;  // stages per chunk
-  bool failed = false;
-  if (nk > 0) load(0);
-  for (int t = 0; t < nk; ++t) {
-    const int s = t % kTcStages;
-    bool late = false;
-    if (t >= kTcStages) late = !mbar_wait(smem_u32(&mbar[s]), (unsigned)((t / kTcStages - 1) & 1));
-    if (!late) store(s);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (__syncthreads_or(late)) {
-      failed = true;
-      break;
-    }
-    if (tid == 0) {
+  } else if (warp == 1 && lane == 0) {
+    // tensor-core issue
+    for (int kt = 0; kt < kt_n; ++kt) {
+      const int s = kt % kTcStages, c = kt / spc, buf = c & 1;
+      if (kt % spc == 0 && c >= 2 &&
+          !mbar_wait(smem_u32(&tempty[buf]), (unsigned)((c / 2 - 1) & 1), abort))
+        break;
+      if (!mbar_wait(smem_u32(&full[s]), (unsigned)((kt / kTcStages) & 1), abort)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const unsigned base = smem_u32(tc_smem + s * kTcStage);
+      const unsigned dacc = tmem + (unsigned)(buf * kTcN);
 #pragma unroll
       for (int j = 0; j < kTcK / 8; ++j) {
         const unsigned long long dah = tc_desc(base + 0 * kTcPart + 256 * j);
@@ -666,53 +670,129 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const GemmDesc* __restrict__
         const unsigned long long da[3] = {dal, dah, dah}, db[3] = {dbh, dbl, dbh};
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
-          const unsigned acc = (t % spc > 0 || j > 0 || p > 0) ? 1u : 0u;
+          const unsigned acc = (kt % spc > 0 || j > 0 || p > 0) ? 1u : 0u;
           asm volatile(
               "{\n\t.reg .pred q;\n\t"
               "setp.ne.b32 q, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, q;\n\t}\n" ::"r"(tmem),
+              "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, q;\n\t}\n" ::"r"(dacc),
               "l"(da[p]), "l"(db[p]), "r"(kTcIdesc), "r"(acc)
               : "memory");
         }
       }
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(&mbar[s]))
+              smem_u32(&empty[s]))
           : "memory");
+      if (kt % spc == spc - 1 || kt == kt_n - 1)
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(&tfull[buf]))
+            : "memory");
     }
-    if (t + 1 < nk) load((t + 1) * kTcK);
-    if ((t + 1) % spc == 0 || t + 1 == nk) {
-      // end of a chunk: its products are done once this stage's commit arrived
-      const bool ok = mbar_wait(smem_u32(&mbar[s]), (unsigned)((t / kTcStages) & 1));
-      if (__syncthreads_or(!ok)) {
-        failed = true;
-        break;
+  } else if (warp >= 4) {
+    // epilogue: every chunk's FP32 sums are added to an FP64 accumulator kept
+    // in tensor memory (columns 2 kTcN + 2 j, + 1: low and high words of
+    // column j's value); C is read and written once, after the last chunk
+    const int q = warp - 4;
+    const int gm = m0 + 32 * q + lane;
+    const unsigned lanes = (unsigned)(32 * q) << 16;
+    for (int c = 0; c < nchunk; ++c) {
+      const int buf = c & 1;
+      const bool last = c == nchunk - 1;
+      if (!mbar_wait(smem_u32(&tfull[buf]), (unsigned)((c / 2) & 1), abort)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+      for (int cc = 0; cc < kTcN / 16; ++cc) {
+        unsigned v[16], w[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+            "%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+              "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(tmem + lanes + (unsigned)(buf * kTcN + 16 * cc))
+            : "memory");
+        const unsigned a64 = tmem + lanes + (unsigned)(2 * kTcN + 32 * cc);
+        if (c > 0) {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+              "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, "
+              "[%32];"
+              : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]),
+                "=r"(w[6]), "=r"(w[7]), "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]),
+                "=r"(w[12]), "=r"(w[13]), "=r"(w[14]), "=r"(w[15]), "=r"(w[16]), "=r"(w[17]),
+                "=r"(w[18]), "=r"(w[19]), "=r"(w[20]), "=r"(w[21]), "=r"(w[22]), "=r"(w[23]),
+                "=r"(w[24]), "=r"(w[25]), "=r"(w[26]), "=r"(w[27]), "=r"(w[28]), "=r"(w[29]),
+                "=r"(w[30]), "=r"(w[31])
+              : "r"(a64)
+              : "memory");
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        double acc[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const double x = (double)__uint_as_float(v[e]);
+          acc[e] = (c > 0) ? __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]) + x : x;
+        }
+        if (!last) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            w[2 * e] = (unsigned)__double2loint(acc[e]);
+            w[2 * e + 1] = (unsigned)__double2hiint(acc[e]);
+          }
+          asm volatile(
+              "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+              "%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+              "%32};" ::"r"(a64),
+              "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]),
+              "r"(w[7]), "r"(w[8]), "r"(w[9]), "r"(w[10]), "r"(w[11]), "r"(w[12]), "r"(w[13]),
+              "r"(w[14]), "r"(w[15]), "r"(w[16]), "r"(w[17]), "r"(w[18]), "r"(w[19]),
+              "r"(w[20]), "r"(w[21]), "r"(w[22]), "r"(w[23]), "r"(w[24]), "r"(w[25]),
+              "r"(w[26]), "r"(w[27]), "r"(w[28]), "r"(w[29]), "r"(w[30]), "r"(w[31])
+              : "memory");
+          asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        } else if (gm < g.m) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int gn = n0 + 16 * cc + e;
+            if (gn < g.n) {
+              double* cp = g.C + gm + (long long)gn * g.ldc;
+              const double val = g.alpha * acc[e];
+              *cp = (g.beta == 0.0) ? val : fma(g.beta, *cp, val);
+            }
+          }
+        }
       }
-      drain(t < spc);
+      // this chunk's accumulator has been read: release it to the next chunk but one
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0)
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[buf]))
+                     : "memory");
     }
-  }
-  if (failed) {
-    if (tid == 0) atomicOr(status, kStatusTimeout);
-  } else if (nk == 0 && em < g.m) {
-    for (int c = 0; c < 64; ++c) {
-      const int gn = n0 + 64 * h2 + c;
-      if (gn < g.n) {
-        double* cp = g.C + em + (long long)gn * g.ldc;
-        *cp = (g.beta == 0.0) ? 0.0 : g.beta * *cp;
+    if (kt_n == 0 && gm < g.m) {
+      for (int e = 0; e < kTcN; ++e) {
+        const int gn = n0 + e;
+        if (gn < g.n) {
+          double* cp = g.C + gm + (long long)gn * g.ldc;
+          *cp = (g.beta == 0.0) ? 0.0 : g.beta * *cp;
+        }
       }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) {
+  if (tid == 0 && *abort) atomicOr(status, kStatusTimeout);
+  if (warp == 2) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(4 * kTcN)
                  : "memory");
   }
 }
 
-void launch_gemm_mixed(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
-                       int* d_status, cudaStream_t s) {
+void launch_gemm_tc(const TcGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                    int* d_status, cudaStream_t s) {
   if (total_tiles <= 0) return;
   static bool attr = false;
   if (!attr) {

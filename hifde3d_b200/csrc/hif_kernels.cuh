@@ -207,11 +207,35 @@ void launch_splitk_reduce(const SplitKDesc* d_desc, int nd, cudaStream_t s);
 // (x = hi + lo); hi*hi + hi*lo + lo*hi run on the tensor cores (mma.sync
 // m16n8k8, FP32 accumulation), then C (FP64) = beta C + alpha acc.
 // 128 x 128 x 16 tiles; tile offsets from dgemm_tiles(m, n, 128).
-// Split-TF32 tensor-core GEMM (tcgen05, FP32 accumulation in tensor memory):
-// C = alpha op(A) op(B) + beta C over the descriptors, 128 x 128 tiles counted
-// by d_tile_off; bounded waits report kStatusTimeout in d_status.
-void launch_gemm_mixed(const GemmDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
-                       int* d_status, cudaStream_t s);
+// Split-TF32 tensor-core GEMM (tcgen05, FP32 accumulation in tensor memory).
+// Operands are first converted to TF32 (hi, lo) pairs in 128 x 32 tiles of
+// kTcTileBytes each: element (i, kk) of an operand is op(X)[i, kk] for A and
+// op(B)[kk, i] for B; tile (rt, kt) at out + (rt * ceil(kdim / 32) + kt) *
+// kTcTileBytes.
+constexpr int kTcTileBytes = 32768;
+struct TcOperand {
+  const double* X;
+  long long ld;
+  int trans;  // 0: element (i, kk) at X[i + kk ld]; 1: at X[kk + i ld]
+  int rows, kdim;
+  unsigned char* out;
+};
+// d_tile_off: prefix over operands of ceil(rows / 128) * ceil(kdim / 32).
+void launch_tc_convert(const TcOperand* d_ops, const int* d_tile_off, int nops, int total_tiles,
+                       cudaStream_t s);
+// C = alpha A B^T-style product of converted operands (A rows m, B rows n,
+// common kdim k) + beta C; 128 x 128 tiles counted by d_tile_off; bounded
+// waits report kStatusTimeout in d_status.
+struct TcGemm {
+  const unsigned char* A;
+  const unsigned char* B;
+  double* C;
+  long long ldc;
+  int m, n, k;
+  double alpha, beta;
+};
+void launch_gemm_tc(const TcGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                    int* d_status, cudaStream_t s);
 
 // In-shared-memory Gauss-Jordan sweep of the first r pivots (n <= kSmallSweepN).
 constexpr int kSmallSweepN = 160;
