@@ -418,7 +418,7 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
 // `timed(kernel class, flops, bytes, launch, launches)` wraps every launch.
 template <class Timed>
 void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t stream,
-                int* d_status, Timed&& timed, bool mixed = false) {
+                int* d_status, Timed&& timed, bool mixed = false, bool sym = false) {
   std::vector<SweepDesc> small, large;
   int max_small = 0;
   for (const SweepDesc& d : descs) {
@@ -455,84 +455,226 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
   double* dinv = tmp.add(dalloc<double>((size_t)nl * kSweepNB * kSweepNB, stream));
   int maxr = 0;
   for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
-  for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
-    std::vector<int> active;
-    std::vector<GemmDesc> gd, rowg, colg;
+  if (sym) {
+    // Symmetric A22 (the face operator): only the block-lower triangle is
+    // kept. After the pivot blocks before K, entry (i, j) equals +(j, i) when
+    // i and j are both pivoted or both not, -(j, i) otherwise. Step K with
+    // Q = the old column block K (rows above K from row block K, negated),
+    // W = -Q D^{-1}: new column block K = W (rows below K), new row block K
+    // = W^T (columns left of K), and lower tile (I, J) += tau_J W_I Q_J^T with
+    // tau_J = -1 left of K, +1 right of K. At the end every pivot is taken,
+    // the inverse is symmetric and the upper tiles are mirrored from the lower.
+    // 2r^3 -> r^3 flops.
+    std::vector<long long> oq(nl);
+    long long qsz = 0;
     for (int b = 0; b < nl; ++b) {
-      const SweepDesc& d = large[b];
-      if (d.r <= k0) continue;
-      active.push_back(b);
-      const int k1 = std::min(d.r, k0 + kSweepNB);
-      const int nbk = k1 - k0;
-      const double* Dv = dinv + (long long)b * kSweepNB * kSweepNB;  // nbk x nbk, ld nbk
-      // row panel B[K, c0:c1) = Dinv B[K, c0:c1), in place: one 128-row tile
-      auto rowp = [&](int c0, int c1) {
-        if (c1 <= c0) return;
-        GemmDesc g{};
-        g.C = d.B + k0 + (long long)c0 * d.n;
-        g.A = Dv;
-        g.B = g.C;
-        g.ldc = g.ldb = d.n;
-        g.lda = nbk;
-        g.m = nbk;
-        g.n = c1 - c0;
-        g.k = nbk;
-        g.alpha = 1.0;
-        g.beta = 0.0;
-        rowg.push_back(g);
-      };
-      // column panel B[r0:r1, K] = -B[r0:r1, K] Dinv, in place: one 128-column tile
-      auto colp = [&](int r0, int r1) {
-        if (r1 <= r0) return;
-        GemmDesc g{};
-        g.C = d.B + r0 + (long long)k0 * d.n;
-        g.A = g.C;
-        g.B = Dv;
-        g.ldc = g.lda = d.n;
-        g.ldb = nbk;
-        g.m = r1 - r0;
-        g.n = nbk;
-        g.k = nbk;
-        g.alpha = -1.0;
-        g.beta = 0.0;
-        colg.push_back(g);
-      };
-      rowp(0, k0);
-      rowp(k1, d.r);
-      colp(0, k0);
-      colp(k1, d.r);
-      auto gemm = [&](int r0, int r1, int c0, int c1) {
-        if (r1 <= r0 || c1 <= c0) return;
-        GemmDesc g{};
-        g.C = d.B + r0 + (long long)c0 * d.n;
-        g.A = d.B + r0 + (long long)k0 * d.n;
-        g.B = d.B + k0 + (long long)c0 * d.n;
-        g.ldc = g.lda = g.ldb = d.n;
-        g.m = r1 - r0;
-        g.n = c1 - c0;
-        g.k = nbk;
-        g.alpha = -1.0;
-        g.beta = 1.0;
-        gd.push_back(g);
-      };
-      gemm(0, k0, 0, k0);
-      gemm(0, k0, k1, d.r);
-      gemm(k1, d.r, 0, k0);
-      gemm(k1, d.r, k1, d.r);
+      oq[b] = qsz;
+      qsz += (long long)large[b].r * kSweepNB;
     }
-    BufList step;
-    int* dact = step.add(upload(active, stream));
-    timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
-      launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
-    });
-    gemm_batch(rowg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
-    gemm_batch(gd, step, stream, HIF_KCLASS_GEMM, timed);
-    gemm_batch(colg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
-    timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
-      launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
-    });
-    HIF_CK(cudaGetLastError());
-    step.release(stream);
+    double* Qb = tmp.add(dalloc<double>(qsz, stream));
+    double* Wb = tmp.add(dalloc<double>(qsz, stream));
+    for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
+      std::vector<int> active;
+      std::vector<CopyDesc> cq, cw;
+      std::vector<int> ocq(1, 0), ocw(1, 0);
+      std::vector<TCopyDesc> tq, tw;
+      std::vector<int> otq(1, 0), otw(1, 0);
+      std::vector<GemmDesc> gw, gu;
+      for (int b = 0; b < nl; ++b) {
+        const SweepDesc& d = large[b];
+        if (d.r <= k0) continue;
+        active.push_back(b);
+        const int k1 = std::min(d.r, k0 + kSweepNB), nbk = k1 - k0, r = d.r;
+        const double* Dv = dinv + (long long)b * kSweepNB * kSweepNB;
+        double* Q = Qb + oq[b];
+        double* W = Wb + oq[b];
+        if (r > k1) {
+          cq.push_back(CopyDesc{d.B + k1 + (long long)k0 * d.n, Q + k1, d.n, r, r - k1, nbk});
+          ocq.push_back(ocq.back() + copy_tiles(r - k1, nbk));
+          cw.push_back(CopyDesc{W + k1, d.B + k1 + (long long)k0 * d.n, r, d.n, r - k1, nbk});
+          ocw.push_back(ocw.back() + copy_tiles(r - k1, nbk));
+        }
+        if (k0 > 0) {
+          tq.push_back(TCopyDesc{d.B + k0, Q, d.n, r, k0, nbk, -1.0});
+          otq.push_back(otq.back() + copy_tiles(k0, nbk));
+          tw.push_back(TCopyDesc{W, d.B + k0, r, d.n, nbk, k0, 1.0});
+          otw.push_back(otw.back() + copy_tiles(nbk, k0));
+        }
+        auto wg = [&](int r0, int r1) {
+          if (r1 <= r0) return;
+          GemmDesc g{};
+          g.C = W + r0;
+          g.ldc = r;
+          g.A = Q + r0;
+          g.lda = r;
+          g.B = Dv;
+          g.ldb = nbk;
+          g.m = r1 - r0;
+          g.n = nbk;
+          g.k = nbk;
+          g.alpha = -1.0;
+          g.beta = 0.0;
+          gw.push_back(g);
+        };
+        wg(0, k0);
+        wg(k1, r);
+        for (int j0 = 0; j0 < r; j0 += kSweepNB) {
+          if (j0 == k0) continue;
+          const int j1 = std::min(r, j0 + kSweepNB);
+          const double tau = j0 < k0 ? -1.0 : 1.0;
+          auto ug = [&](int r0, int r1) {
+            if (r1 <= r0) return;
+            GemmDesc g{};
+            g.C = d.B + r0 + (long long)j0 * d.n;
+            g.ldc = d.n;
+            g.A = W + r0;
+            g.lda = r;
+            g.B = Q + j0;
+            g.ldb = r;
+            g.transB = 1;
+            g.m = r1 - r0;
+            g.n = j1 - j0;
+            g.k = nbk;
+            g.alpha = tau;
+            g.beta = 1.0;
+            gu.push_back(g);
+          };
+          if (j0 < k0) {
+            ug(j0, k0);
+            ug(k1, r);
+          } else {
+            ug(j0, r);
+          }
+        }
+      }
+      BufList step;
+      int* dact = step.add(upload(active, stream));
+      timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+        launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream, 1);
+      });
+      if (!cq.empty()) {
+        CopyDesc* dq = step.add(upload(cq, stream));
+        int* doq = step.add(upload(ocq, stream));
+        timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dq, doq, (int)cq.size(), ocq.back(), stream); });
+      }
+      if (!tq.empty()) {
+        TCopyDesc* dq = step.add(upload(tq, stream));
+        int* doq = step.add(upload(otq, stream));
+        timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_tcopy(dq, doq, (int)tq.size(), otq.back(), stream); });
+      }
+      gemm_batch(gw, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+      gemm_batch(gu, step, stream, HIF_KCLASS_GEMM, timed);
+      if (!cw.empty()) {
+        CopyDesc* dw = step.add(upload(cw, stream));
+        int* dow = step.add(upload(ocw, stream));
+        timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dw, dow, (int)cw.size(), ocw.back(), stream); });
+      }
+      if (!tw.empty()) {
+        TCopyDesc* dw = step.add(upload(tw, stream));
+        int* dow = step.add(upload(otw, stream));
+        timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_tcopy(dw, dow, (int)tw.size(), otw.back(), stream); });
+      }
+      timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+        launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
+      });
+      HIF_CK(cudaGetLastError());
+      step.release(stream);
+    }
+    // upper tiles of A22^{-1} from the lower ones
+    std::vector<TCopyDesc> tm;
+    std::vector<int> otm(1, 0);
+    for (const SweepDesc& d : large)
+      for (int j0 = kSweepNB; j0 < d.r; j0 += kSweepNB) {
+        const int j1 = std::min(d.r, j0 + kSweepNB);
+        tm.push_back(TCopyDesc{d.B + j0, d.B + (long long)j0 * d.n, d.n, d.n, j0, j1 - j0, 1.0});
+        otm.push_back(otm.back() + copy_tiles(j0, j1 - j0));
+      }
+    if (!tm.empty()) {
+      TCopyDesc* dm = tmp.add(upload(tm, stream));
+      int* dom = tmp.add(upload(otm, stream));
+      timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_tcopy(dm, dom, (int)tm.size(), otm.back(), stream); });
+      HIF_CK(cudaGetLastError());
+    }
+  } else {
+    for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
+      std::vector<int> active;
+      std::vector<GemmDesc> gd, rowg, colg;
+      for (int b = 0; b < nl; ++b) {
+        const SweepDesc& d = large[b];
+        if (d.r <= k0) continue;
+        active.push_back(b);
+        const int k1 = std::min(d.r, k0 + kSweepNB);
+        const int nbk = k1 - k0;
+        const double* Dv = dinv + (long long)b * kSweepNB * kSweepNB;  // nbk x nbk, ld nbk
+        // row panel B[K, c0:c1) = Dinv B[K, c0:c1), in place: one 128-row tile
+        auto rowp = [&](int c0, int c1) {
+          if (c1 <= c0) return;
+          GemmDesc g{};
+          g.C = d.B + k0 + (long long)c0 * d.n;
+          g.A = Dv;
+          g.B = g.C;
+          g.ldc = g.ldb = d.n;
+          g.lda = nbk;
+          g.m = nbk;
+          g.n = c1 - c0;
+          g.k = nbk;
+          g.alpha = 1.0;
+          g.beta = 0.0;
+          rowg.push_back(g);
+        };
+        // column panel B[r0:r1, K] = -B[r0:r1, K] Dinv, in place: one 128-column tile
+        auto colp = [&](int r0, int r1) {
+          if (r1 <= r0) return;
+          GemmDesc g{};
+          g.C = d.B + r0 + (long long)k0 * d.n;
+          g.A = g.C;
+          g.B = Dv;
+          g.ldc = g.lda = d.n;
+          g.ldb = nbk;
+          g.m = r1 - r0;
+          g.n = nbk;
+          g.k = nbk;
+          g.alpha = -1.0;
+          g.beta = 0.0;
+          colg.push_back(g);
+        };
+        rowp(0, k0);
+        rowp(k1, d.r);
+        colp(0, k0);
+        colp(k1, d.r);
+        auto gemm = [&](int r0, int r1, int c0, int c1) {
+          if (r1 <= r0 || c1 <= c0) return;
+          GemmDesc g{};
+          g.C = d.B + r0 + (long long)c0 * d.n;
+          g.A = d.B + r0 + (long long)k0 * d.n;
+          g.B = d.B + k0 + (long long)c0 * d.n;
+          g.ldc = g.lda = g.ldb = d.n;
+          g.m = r1 - r0;
+          g.n = c1 - c0;
+          g.k = nbk;
+          g.alpha = -1.0;
+          g.beta = 1.0;
+          gd.push_back(g);
+        };
+        gemm(0, k0, 0, k0);
+        gemm(0, k0, k1, d.r);
+        gemm(k1, d.r, 0, k0);
+        gemm(k1, d.r, k1, d.r);
+      }
+      BufList step;
+      int* dact = step.add(upload(active, stream));
+      timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+        launch_sweep_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
+      });
+      gemm_batch(rowg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
+      gemm_batch(gd, step, stream, HIF_KCLASS_GEMM, timed);
+      gemm_batch(colg, step, stream, HIF_KCLASS_SWEEP_PANEL, timed, 128);
+      timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+        launch_sweep_setdiag(dd, dact, (int)active.size(), k0, dinv, stream);
+      });
+      HIF_CK(cudaGetLastError());
+      step.release(stream);
+    }
   }
   // X = A22^{-1} A21 and S = A11 - A12 X
   std::vector<GemmDesc> gx, gs;
@@ -609,6 +751,9 @@ class Engine {
   long long peak_bytes = 0, cur_bytes = 0;
   int* d_status = nullptr;
   int* d_dof_src = nullptr;  // source membership, 6 x NC^3 (see Sources)
+  // the operator is symmetric (face-coefficient form): eliminations keep only
+  // the lower triangle of A22
+  bool symmetric = false;
 
   // ---- per-kernel-class timing (HIF_OPT_PROFILE): CUDA events on the engine
   // stream around each launch, with the launch's algorithmic flops / bytes.
@@ -781,6 +926,7 @@ class Engine {
     launch_setup_node(dA, dV, N, hstep, d_band, stream);
     HIF_CK(cudaGetLastError());
     have_op = true;
+    symmetric = false;  // the node form is not symmetric for variable A
   }
 
   // ---- Initialize (src/Factor.cpp:6-39) -----------------------------------
@@ -807,7 +953,7 @@ class Engine {
   void run_sweep(const std::vector<SweepDesc>& descs, BufList& tmp) {
     sweep_blocks(descs, tmp, stream, d_status,
                  [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); },
-                 precision == HIF_PRECISION_MIXED);
+                 precision == HIF_PRECISION_MIXED, symmetric);
   }
 
   void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
@@ -2317,6 +2463,7 @@ int hif_setup_stencil_faces(hif_handle h, int N, double hstep, const double* ax,
     hif::dfree(dz, e.stream);
     hif::dfree(dv, e.stream);
     e.have_op = true;
+    e.symmetric = true;
     e.sync();
   });
 }
@@ -2331,6 +2478,7 @@ int hif_setup_stencil_faces_device(hif_handle h, int N, double hstep, const doub
     });
     HIF_CK(cudaGetLastError());
     e.have_op = true;
+    e.symmetric = true;
   });
 }
 

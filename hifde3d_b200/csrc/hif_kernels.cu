@@ -891,16 +891,20 @@ void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_statu
 __global__ void __launch_bounds__(512) k_sweep_diag(const SweepDesc* __restrict__ descs,
                                                     const int* __restrict__ active, int k0,
                                                     double* __restrict__ dinv,
-                                                    int* __restrict__ status) {
+                                                    int* __restrict__ status, int sym) {
   const int di = active[blockIdx.x];
   const SweepDesc d = descs[di];
   const int nb = min(kSweepNB, d.r - k0);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   __shared__ double rowk[2][kSweepNB], colk[2][kSweepNB];
   extern __shared__ double dg_sm[];  // kSweepNB x kSweepNB staging (coalesced load / store)
+  // sym: the block is taken from its lower triangle (mirrored), so that the
+  // inverse of a symmetric elimination stays consistent when the input carries
+  // an asymmetric rounding error
   for (int e = threadIdx.x; e < kSweepNB * kSweepNB; e += blockDim.x) {
     const int i = e & (kSweepNB - 1), j = e / kSweepNB;
-    dg_sm[e] = (i < nb && j < nb) ? d.B[(k0 + i) + (long long)(k0 + j) * d.n] : 0.0;
+    const int ii = (sym && i < j) ? j : i, jj = (sym && i < j) ? i : j;
+    dg_sm[e] = (i < nb && j < nb) ? d.B[(k0 + ii) + (long long)(k0 + jj) * d.n] : 0.0;
   }
   __syncthreads();
   double a[4][8];
@@ -981,7 +985,7 @@ __global__ void __launch_bounds__(512) k_sweep_diag(const SweepDesc* __restrict_
 }
 
 void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
-                       double* d_dinv, int* d_status, cudaStream_t s) {
+                       double* d_dinv, int* d_status, cudaStream_t s, int sym) {
   if (nact <= 0) return;
   const int smem = kSweepNB * kSweepNB * (int)sizeof(double);
   static bool attr = false;
@@ -989,7 +993,7 @@ void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, i
     cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     attr = true;
   }
-  k_sweep_diag<<<nact, 512, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
+  k_sweep_diag<<<nact, 512, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status, sym);
 }
 
 // Row panel: tile of up to 64 columns [lo, hi) of rows K.
@@ -1608,6 +1612,35 @@ void launch_copy(const CopyDesc* d_desc, const int* d_tile_off, int nd, int tota
                  cudaStream_t s) {
   if (total_tiles <= 0) return;
   k_copy<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
+}
+
+// Transposing copy through a shared-memory tile (coalesced on both sides).
+__global__ void __launch_bounds__(256) k_tcopy(const TCopyDesc* __restrict__ descs,
+                                               const int* __restrict__ tile_off, int nd) {
+  const int di = find_desc(tile_off, nd, blockIdx.x);
+  const TCopyDesc c = descs[di];
+  const int local = blockIdx.x - tile_off[di];
+  const int tm = (c.m + 31) / 32;
+  const int i0 = (local % tm) * 32, j0 = (local / tm) * 32;
+  __shared__ double t[32][33];
+  // read: consecutive threads take consecutive j (contiguous in src)
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+    const int jj = e & 31, ii = e >> 5;
+    const int i = i0 + ii, j = j0 + jj;
+    t[jj][ii] = (i < c.m && j < c.n) ? c.src[j + (long long)i * c.lds] : 0.0;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+    const int ii = e & 31, jj = e >> 5;
+    const int i = i0 + ii, j = j0 + jj;
+    if (i < c.m && j < c.n) c.dst[i + (long long)j * c.ldd] = c.alpha * t[jj][ii];
+  }
+}
+
+void launch_tcopy(const TCopyDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                  cudaStream_t s) {
+  if (total_tiles <= 0) return;
+  k_tcopy<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
 }
 
 // ===========================================================================

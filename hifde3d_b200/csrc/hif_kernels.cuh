@@ -175,6 +175,16 @@ struct CopyDesc {
   long long lds, ldd;
   int m, n;
 };
+// dst (m x n, ld ldd) = alpha * src^T, src n x m (ld lds); 32 x 32 tiles.
+struct TCopyDesc {
+  const double* src;
+  double* dst;
+  long long lds, ldd;
+  int m, n;
+  double alpha;
+};
+void launch_tcopy(const TCopyDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                  cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Launchers. Descriptor arrays live in device memory; tile_off (device) is
@@ -246,7 +256,7 @@ void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_statu
 constexpr int kSweepNB = 128;
 constexpr int kPanelTile = 64;  // rows / columns per panel tile
 void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
-                       double* d_dinv, int* d_status, cudaStream_t s);
+                       double* d_dinv, int* d_status, cudaStream_t s, int sym = 0);
 // Panel tile maps hold 4 ints per tile: {descriptor, lo, hi, unused} with
 // hi - lo <= kPanelTile; the row panel covers columns [lo, hi) of pivot rows,
 // the column panel rows [lo, hi) of pivot columns. d_dinv holds kSweepNB^2

@@ -206,6 +206,7 @@ class Server {
                            e->stream);
         HIF_CK(cudaGetLastError());
         e->have_op = true;
+        e->symmetric = true;
         dfree(d, e->stream);
         e->factor();
         e->sync();
