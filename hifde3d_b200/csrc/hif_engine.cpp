@@ -335,7 +335,7 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
       ooff.push_back(ooff.back() + ta);
       ops.push_back(TcOperand{x.B, x.ldb, x.transB ? 0 : 1, x.n, x.k, pb});
       ooff.push_back(ooff.back() + tb);
-      tg.push_back(TcGemm{pa, pb, x.C, x.ldc, x.m, x.n, x.k, x.alpha, x.beta});
+      tg.push_back(TcGemm{pa, pb, x.C, x.ldc, x.m, x.n, x.k, x.alpha, x.beta, x.lower});
       toff.push_back(toff.back() + (x.m + 127) / 128 * ((x.n + 127) / 128));
     }
     if (toff.back() == 0) return;
@@ -363,7 +363,7 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
     const GemmDesc& x = gin[q];
     fl += 2.0 * x.m * x.n * x.k;
     const int big = std::max(x.m, x.n);
-    if (force_tile == 0 && x.k >= 2048 && x.k >= 8 * big) {
+    if (force_tile == 0 && !x.lower && x.k >= 2048 && x.k >= 8 * big) {
       const int S = std::min(32, (x.k + 1023) / 1024);
       splits.push_back(Split{q, S});
       psz += (long long)S * x.m * x.n;
@@ -397,7 +397,9 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
     all += w;
     if (x.m >= 96 && x.n >= 96) big += w;
   }
-  const int tile = force_tile ? force_tile : ((big >= 0.5 * all) ? 128 : 64);
+  bool lower = false;  // lower-triangle products are tiled by 128 x 128
+  for (const GemmDesc& x : g) lower = lower || x.lower;
+  const int tile = force_tile ? force_tile : ((lower || big >= 0.5 * all) ? 128 : 64);
   std::vector<int> toff(1, 0);
   for (const GemmDesc& x : g) toff.push_back(toff.back() + dgemm_tiles(x.m, x.n, tile));
   if (toff.back() == 0 && red.empty()) return;
@@ -706,13 +708,33 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
     y.k = r;
     y.alpha = -1.0;
     y.beta = 1.0;
+    y.lower = sym ? 1 : 0;  // S is symmetric: the tiles above the diagonal are mirrored
     gs.push_back(y);
   }
   // X stays FP64: it comes from the explicit inverse, whose entries exceed X's by
   // about cond(A22), so a TF32-level product would lose that factor in X.
   gemm_batch(gx, tmp, stream, HIF_KCLASS_GEMM, timed);
   if (mixed) gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM_MIXED, timed, 128, d_status);
-  else gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM, timed);
+  else gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM, timed, sym ? 128 : 0);
+  if (sym) {
+    std::vector<TCopyDesc> tm;
+    std::vector<int> otm(1, 0);
+    for (const SweepDesc& d : large) {
+      const int sk = d.n - d.r;
+      double* S = d.B + d.r + (long long)d.r * d.n;
+      for (int j0 = 128; j0 < sk; j0 += 128) {
+        const int j1 = std::min(sk, j0 + 128);
+        tm.push_back(TCopyDesc{S + j0, S + (long long)j0 * d.n, d.n, d.n, j0, j1 - j0, 1.0});
+        otm.push_back(otm.back() + copy_tiles(j0, j1 - j0));
+      }
+    }
+    if (!tm.empty()) {
+      TCopyDesc* dm = tmp.add(upload(tm, stream));
+      int* dom = tmp.add(upload(otm, stream));
+      timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_tcopy(dm, dom, (int)tm.size(), otm.back(), stream); });
+      HIF_CK(cudaGetLastError());
+    }
+  }
   // compact copy of A22^{-1}
   std::vector<CopyDesc> cd;
   std::vector<int> coff(1, 0);

@@ -308,6 +308,7 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
   const GemmDesc g = descs[di];
   const int local = blockIdx.x - tile_off[di];
   const int tiles_m = (g.m + kLBM - 1) / kLBM;
+  if (g.lower && local % tiles_m < local / tiles_m) return;
   const int m0 = (local % tiles_m) * kLBM, n0 = (local / tiles_m) * kLBN;
   const int tid = threadIdx.x;
 
@@ -595,6 +596,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const TcGemm* __restrict__ d
   const int local = blockIdx.x - tile_off[di];
   const int tiles_m = (g.m + kTcM - 1) / kTcM;
   const int mt = local % tiles_m, nt = local / tiles_m;
+  if (g.lower && mt < nt) return;  // whole CTA, before any barrier or allocation
   const int m0 = mt * kTcM, n0 = nt * kTcN;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int kt_n = (g.k + kTcK - 1) / kTcK;

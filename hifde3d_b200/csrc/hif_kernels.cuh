@@ -63,6 +63,7 @@ struct GemmDesc {
   int m, n, k;
   int transA, transB;
   double alpha, beta;
+  int lower;  // 128 x 128 tiles only: skip the tiles above the diagonal (row tile < column tile)
 };
 
 // Dense elimination block: B (n x n, ld n) in assembly order [red | skel].
@@ -243,6 +244,7 @@ struct TcGemm {
   long long ldc;
   int m, n, k;
   double alpha, beta;
+  int lower;  // skip the tiles above the diagonal
 };
 void launch_gemm_tc(const TcGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
                     int* d_status, cudaStream_t s);
