@@ -1626,10 +1626,11 @@ class Engine {
       g.transA = 1;
       g.alpha = 1.0;
       g.beta = 0.0;
+      g.lower = 1;  // G is symmetric: the panels read its lower triangle only
       gram.push_back(g);
     }
     auto tm = [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); };
-    gemm_batch(gram, tmp, stream, HIF_KCLASS_QR, tm);
+    gemm_batch(gram, tmp, stream, HIF_KCLASS_QR, tm, 128);
     PcholDesc* dpd = tmp.add(upload(pd, stream));
     std::vector<int> active(nd), info(2 * nd);
     for (int q = 0; q < nd; ++q) active[q] = q;
@@ -1662,9 +1663,10 @@ class Engine {
         g.k = kPcholNB;
         g.alpha = -1.0;
         g.beta = 1.0;
+        g.lower = 1;
         upd.push_back(g);
       }
-      gemm_batch(upd, step, stream, HIF_KCLASS_ID, tm);
+      gemm_batch(upd, step, stream, HIF_KCLASS_ID, tm, 128);
       HIF_CK(cudaGetLastError());
       step.release(stream);
       active.swap(next);

@@ -2152,7 +2152,8 @@ __global__ void __launch_bounds__(512) k_pchol_panel(const PcholDesc* __restrict
     for (int j = tid; j < n; j += nthr) {
       if (ch[j]) { Ri[j] = 0.0; continue; }
       if (j == p) { Ri[j] = rii; continue; }
-      double sacc = G[j + (long long)p * n];
+      // only the lower triangle of G is kept: G[j, p] for j > p, G[p, j] above
+      double sacc = (j > p) ? G[j + (long long)p * n] : G[p + (long long)j * n];
       for (int l = 0; l < i - i0; ++l) sacc = fma(-pcol[l], R[(long long)(i0 + l) * n + j], sacc);
       const double r = sacc / rii;
       Ri[j] = r;
