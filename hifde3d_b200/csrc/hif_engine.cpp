@@ -766,6 +766,7 @@ class Engine {
   Arena arena_factor, arena_work[2];
   Arena* cur_work = &arena_work[0];
   bool keep_schur = false, verbose = false;
+  int verbose_mode = 0;
   int precision = HIF_PRECISION_FP64;
   long long budget_mb = 0;
   std::map<int, std::vector<std::vector<int>>> replay;
@@ -893,12 +894,40 @@ class Engine {
   void sync() { HIF_CK(cudaStreamSynchronize(stream)); }
   // verbose: print the time since the last mark (after a stream sync)
   double mark_t = 0;
+  // verbose 1: synchronise at every mark and print the phase's wall time;
+  // verbose 2: no synchronisation; an event per mark, and at the end of the
+  // factorization each phase's host time (issue) beside its device time
+  struct Mark {
+    const char* what;
+    int level;
+    double host;
+    cudaEvent_t ev;
+  };
+  std::vector<Mark> marks;
   void mark(const char* what, int level) {
     if (!verbose) return;
+    if (verbose_mode == 2) {
+      Mark m{what, level, wall(), get_event()};
+      HIF_CK(cudaEventRecord(m.ev, stream));
+      marks.push_back(m);
+      return;
+    }
     sync();
     const double t = wall();
     if (mark_t > 0) std::fprintf(stderr, "[hif]   L%d %-22s %9.3f ms\n", level, what, 1e3 * (t - mark_t));
     mark_t = t;
+  }
+  void report_marks() {
+    if (marks.empty()) return;
+    sync();
+    for (size_t q = 1; q < marks.size(); ++q) {
+      float ms = 0;
+      HIF_CK(cudaEventElapsedTime(&ms, marks[q - 1].ev, marks[q].ev));
+      std::fprintf(stderr, "[hif]   L%d %-22s host %9.3f ms  device %9.3f ms\n", marks[q].level,
+                   marks[q].what, 1e3 * (marks[q].host - marks[q - 1].host), ms);
+    }
+    for (Mark& m : marks) ev_pool.push_back(m.ev);
+    marks.clear();
   }
   void sync_quiet() { cudaStreamSynchronize(stream); }
 
@@ -1117,7 +1146,7 @@ class Engine {
     }
     mark("schur partition+upload", level);
     gather(tg, in, d_own, d_sd, d_dof, tmp);
-    if (verbose) sync();
+    if (verbose && verbose_mode != 2) sync();
     t_gather += wall() - tg0;
     mark("schur gather", level);
 
@@ -1153,7 +1182,7 @@ class Engine {
       sd.push_back(d);
     }
     run_sweep(sd, tmp);
-    if (verbose) sync();
+    if (verbose && verbose_mode != 2) sync();
     t_elim += wall() - te0;
     mark("schur eliminate", level);
 
@@ -1298,7 +1327,7 @@ class Engine {
     }
     mark("skel partition+upload", level);
     gather(tg, cells, d_own, d_sd, d_dof, tmp);
-    if (verbose) sync();
+    if (verbose && verbose_mode != 2) sync();
     t_gather += wall() - tg0;
     mark("skel gather M", level);
 
@@ -1518,7 +1547,7 @@ class Engine {
       tg2.push_back(g);
     }
     gather(tg2, cells, d_own, d_sd, d_dof, tmp);
-    if (verbose) sync();
+    if (verbose && verbose_mode != 2) sync();
     t_gather += wall() - tg0;
     mark("skel gather A_ff", level);
 
@@ -1632,25 +1661,17 @@ class Engine {
     auto tm = [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); };
     gemm_batch(gram, tmp, stream, HIF_KCLASS_QR, tm, 128);
     PcholDesc* dpd = tmp.add(upload(pd, stream));
-    std::vector<int> active(nd), info(2 * nd);
-    for (int q = 0; q < nd; ++q) active[q] = q;
-    for (int i0 = 0; !active.empty(); i0 += kPcholNB) {
-      BufList step;
-      int* da = step.add(upload(active, stream));
-      timed(HIF_KCLASS_ID, 0, 0, [&] {
-        launch_pchol_panel(dpd, da, (int)active.size(), i0, kPcholNB, eps, max_n, d_status,
-                           stream);
-      });
-      HIF_CK(cudaGetLastError());
-      HIF_CK(cudaMemcpyAsync(info.data(), ibuf + isz, 2 * nd * sizeof(int),
-                             cudaMemcpyDeviceToHost, stream));
-      sync();
-      std::vector<int> next;
+    // a fixed sequence of panels without host synchronisation: a face whose
+    // rank is known skips its later panels and updates on the device
+    std::vector<int> info(2 * nd);
+    for (int i0 = 0; i0 < max_n; i0 += kPcholNB) {
+      std::vector<int> active;
       std::vector<GemmDesc> upd;
-      for (int q : active) {
-        if (info[2 * q + 1]) continue;
-        next.push_back(q);
+      for (int q = 0; q < nd; ++q) {
         const int n = pd[q].id.n;
+        if (n <= i0) continue;
+        active.push_back(q);
+        if (n <= i0 + kPcholNB) continue;  // no columns left after this panel
         GemmDesc g{};  // G -= Y Y^T, Y = the panel's rows of R as an n x nb matrix
         g.C = pd[q].G;
         g.ldc = n;
@@ -1664,13 +1685,23 @@ class Engine {
         g.alpha = -1.0;
         g.beta = 1.0;
         g.lower = 1;
+        g.skip = pd[q].info + 1;
         upd.push_back(g);
       }
+      BufList step;
+      int* da = step.add(upload(active, stream));
+      timed(HIF_KCLASS_ID, 0, 0, [&] {
+        launch_pchol_panel(dpd, da, (int)active.size(), i0, kPcholNB, eps, max_n, d_status,
+                           stream);
+      });
+      HIF_CK(cudaGetLastError());
       gemm_batch(upd, step, stream, HIF_KCLASS_ID, tm, 128);
       HIF_CK(cudaGetLastError());
       step.release(stream);
-      active.swap(next);
     }
+    HIF_CK(cudaMemcpyAsync(info.data(), ibuf + isz, 2 * nd * sizeof(int), cudaMemcpyDeviceToHost,
+                           stream));
+    sync();
     timed(HIF_KCLASS_ID, 0, 0, [&] { launch_pchol_finish(dpd, nd, max_n, stream); });
     HIF_CK(cudaGetLastError());
     // W := R11^{-1} R12, diagonal blocks from the bottom, products above them
@@ -2006,7 +2037,7 @@ class Engine {
       sd.push_back(d);
     }
     run_sweep(sd, tmp);
-    if (verbose) sync();
+    if (verbose && verbose_mode != 2) sync();
     t_elim += wall() - te0;
   }
 
@@ -2044,13 +2075,15 @@ class Engine {
       } else {
         b.bufs.release(stream);
       }
-      if (verbose) {
+      if (verbose && verbose_mode != 2) {
         sync();
         std::fprintf(stderr, "[hif] level %d: %.3f ms\n", level, 1e3 * (wall() - tl));
       }
     }
+    mark("end", L);
     sync();
     t_total = wall() - t0;
+    report_marks();
     int st = 0;
     HIF_CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
     factored = true;
@@ -2679,7 +2712,10 @@ int hif_set_option(hif_handle h, int option, long long value) {
   if (!h) return HIF_ERR_ARG;
   switch (option) {
     case HIF_OPT_KEEP_SCHUR: h->e->keep_schur = value != 0; return HIF_OK;
-    case HIF_OPT_VERBOSE: h->e->verbose = value != 0; return HIF_OK;
+    case HIF_OPT_VERBOSE:
+      h->e->verbose = value != 0;
+      h->e->verbose_mode = (int)value;
+      return HIF_OK;
     case HIF_OPT_MEM_BUDGET_MB: h->e->budget_mb = value; return HIF_OK;
     case HIF_OPT_PRECISION:
       if (value != HIF_PRECISION_FP64 && value != HIF_PRECISION_MIXED) return HIF_ERR_ARG;

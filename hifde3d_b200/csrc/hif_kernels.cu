@@ -180,6 +180,7 @@ __global__ void __launch_bounds__(256) k_dgemm(const GemmDesc* __restrict__ desc
   const GemmDesc g = descs[di];
   const int local = blockIdx.x - tile_off[di];
   const int tiles_m = (g.m + kBM - 1) / kBM;
+  if (g.skip && *g.skip) return;
   const int m0 = (local % tiles_m) * kBM, n0 = (local / tiles_m) * kBN;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
 
@@ -309,6 +310,7 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
   const int local = blockIdx.x - tile_off[di];
   const int tiles_m = (g.m + kLBM - 1) / kLBM;
   if (g.lower && local % tiles_m < local / tiles_m) return;
+  if (g.skip && *g.skip) return;
   const int m0 = (local % tiles_m) * kLBM, n0 = (local / tiles_m) * kLBN;
   const int tid = threadIdx.x;
 

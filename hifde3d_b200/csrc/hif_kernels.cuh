@@ -64,6 +64,7 @@ struct GemmDesc {
   int transA, transB;
   double alpha, beta;
   int lower;  // 128 x 128 tiles only: skip the tiles above the diagonal (row tile < column tile)
+  const int* skip;  // optional: the product is skipped when *skip != 0 (read on the device)
 };
 
 // Dense elimination block: B (n x n, ld n) in assembly order [red | skel].
