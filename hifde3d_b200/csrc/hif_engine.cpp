@@ -125,6 +125,11 @@ struct PinnedStage {
 // Staging used by upload() on this thread (set while a factorization runs).
 thread_local PinnedStage* t_stage = nullptr;
 
+struct Arena;
+// Arena for the large temporaries of gemm_batch on this thread (the engine's
+// current level workspace while a factorization runs), else the pool.
+thread_local Arena* t_scratch = nullptr;
+
 void copy_to_device(void* d, const void* h, size_t bytes, cudaStream_t s) {
   if (bytes == 0) return;
   if (t_stage) {
@@ -192,6 +197,7 @@ struct Arena {
   };
   std::vector<Chunk> chunks;
   size_t cur = 0;
+  double grow_s = 0;  // host time spent in cudaMalloc for new chunks
   static constexpr size_t kMinChunk = size_t(256) << 20;
 
   template <class T>
@@ -207,7 +213,9 @@ struct Arena {
     }
     const size_t sz = std::max(bytes, kMinChunk);
     void* p = nullptr;
+    const double t0 = wall();
     HIF_CK(cudaMalloc(&p, sz));
+    grow_s += wall() - t0;
     chunks.push_back(Chunk{static_cast<char*>(p), sz, bytes});
     cur = chunks.size() - 1;
     return static_cast<T*>(p);
@@ -221,6 +229,18 @@ struct Arena {
   void reset() {
     for (Chunk& c : chunks) c.used = 0;
     cur = 0;
+  }
+  // Stack discipline for temporaries: everything allocated after mark() is
+  // given back by rewind(). Users are on one stream, so memory handed out
+  // again after a rewind is written only by work ordered after the old users.
+  struct Mark {
+    size_t cur, used;
+  };
+  Mark mark() const { return Mark{cur, chunks.empty() ? 0 : chunks[cur].used}; }
+  void rewind(const Mark& m) {
+    for (size_t q = m.cur + 1; q < chunks.size(); ++q) chunks[q].used = 0;
+    if (!chunks.empty()) chunks[m.cur].used = m.used;
+    cur = m.cur;
   }
   size_t reserved() const {
     size_t t = 0;
@@ -304,10 +324,28 @@ struct Sources {
 // a single output tile along the aliased dimension), else 64x64. Problems with
 // a reduction much longer than their output dimensions are split along k into
 // partial products and summed in a fixed order.
+// Temporaries of one call: from t_scratch (given back when the scope ends) or
+// from the pool (released with tmp).
+struct ScratchScope {
+  Arena* a;
+  Arena::Mark m{};
+  ScratchScope() : a(t_scratch) {
+    if (a) m = a->mark();
+  }
+  ~ScratchScope() {
+    if (a) a->rewind(m);
+  }
+};
+template <class T>
+T* scratch_alloc(size_t count, BufList& tmp, cudaStream_t s) {
+  return t_scratch ? t_scratch->alloc<T>(count) : tmp.add(dalloc<T>(count, s));
+}
+
 template <class Timed>
 void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t stream, int cls,
                 Timed&& timed, int force_tile = 0, int* mixed_status = nullptr) {
   if (gin.empty()) return;
+  ScratchScope scope;
   if (mixed_status) {  // split-TF32 tensor-core path (Schur-complement updates)
     double fl = 0;
     long long tiles = 0;
@@ -316,7 +354,8 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
       const long long kt = (x.k + 31) / 32;
       tiles += ((x.m + 127) / 128 + (x.n + 127) / 128) * kt;
     }
-    unsigned char* cbuf = tmp.add(dalloc<unsigned char>(std::max(1LL, tiles) * kTcTileBytes, stream));
+    unsigned char* cbuf =
+        scratch_alloc<unsigned char>(std::max(1LL, tiles) * kTcTileBytes, tmp, stream);
     std::vector<TcOperand> ops;
     std::vector<int> ooff(1, 0);
     std::vector<TcGemm> tg;
@@ -371,7 +410,7 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
       g.push_back(x);
     }
   }
-  double* P = psz ? tmp.add(dalloc<double>(psz, stream)) : nullptr;
+  double* P = psz ? scratch_alloc<double>(psz, tmp, stream) : nullptr;
   long long po = 0;
   for (const Split& sp : splits) {
     const GemmDesc& x = gin[sp.idx];
@@ -420,7 +459,13 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
 // `timed(kernel class, flops, bytes, launch, launches)` wraps every launch.
 template <class Timed>
 void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t stream,
-                int* d_status, Timed&& timed, bool mixed = false, bool sym = false) {
+                int* d_status, Timed&& timed, bool mixed = false, bool sym = false,
+                Arena* scratch = nullptr) {
+  // large per-call scratch from the caller's arena when it has one (no pool
+  // traffic), else from the stream-ordered pool
+  auto big = [&](size_t count) -> double* {
+    return scratch ? scratch->alloc<double>(count) : tmp.add(dalloc<double>(count, stream));
+  };
   std::vector<SweepDesc> small, large;
   int max_small = 0;
   for (const SweepDesc& d : descs) {
@@ -454,7 +499,7 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
   // Product 3 goes to the split-TF32 tensor-core kernel in mixed precision.
   const int nl = (int)large.size();
   SweepDesc* dd = tmp.add(upload(large, stream));
-  double* dinv = tmp.add(dalloc<double>((size_t)nl * kSweepNB * kSweepNB, stream));
+  double* dinv = big((size_t)nl * kSweepNB * kSweepNB);
   int maxr = 0;
   for (const SweepDesc& d : large) maxr = std::max(maxr, d.r);
   if (sym) {
@@ -473,8 +518,8 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
       oq[b] = qsz;
       qsz += (long long)large[b].r * kSweepNB;
     }
-    double* Qb = tmp.add(dalloc<double>(qsz, stream));
-    double* Wb = tmp.add(dalloc<double>(qsz, stream));
+    double* Qb = big(qsz);
+    double* Wb = big(qsz);
     for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
       std::vector<int> active;
       std::vector<CopyDesc> cq, cw;
@@ -928,6 +973,12 @@ class Engine {
     }
     for (Mark& m : marks) ev_pool.push_back(m.ev);
     marks.clear();
+    std::fprintf(stderr, "[hif]   arenas: factor %zu chunks %.1f GB, work %zu + %zu chunks %.1f GB, "
+                 "cudaMalloc %.1f ms so far\n", arena_factor.chunks.size(),
+                 arena_factor.reserved() / 1e9, arena_work[0].chunks.size(),
+                 arena_work[1].chunks.size(),
+                 (arena_work[0].reserved() + arena_work[1].reserved()) / 1e9,
+                 1e3 * (arena_factor.grow_s + arena_work[0].grow_s + arena_work[1].grow_s));
   }
   void sync_quiet() { cudaStreamSynchronize(stream); }
 
@@ -1004,7 +1055,7 @@ class Engine {
   void run_sweep(const std::vector<SweepDesc>& descs, BufList& tmp) {
     sweep_blocks(descs, tmp, stream, d_status,
                  [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); },
-                 precision == HIF_PRECISION_MIXED, symmetric);
+                 precision == HIF_PRECISION_MIXED, symmetric, cur_work);
   }
 
   void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
@@ -1117,6 +1168,8 @@ class Engine {
     // this level's workspace: what it held (level - 2) is no longer read
     Arena& work = arena_work[level & 1];
     work.reset();
+    cur_work = &work;
+    t_scratch = &work;
     double* dB = work.alloc<double>(bsz);
     st.arena = arena_factor.alloc<double>(asz);
     st.d_red = arena_factor.upload(red_all, stream);
@@ -1296,6 +1349,7 @@ class Engine {
     track((msz + wsz) * 8);
     Arena& work = arena_work[level & 1];
     cur_work = &work;
+    t_scratch = &work;
     double* dM = work.alloc<double>(msz);
     double* dWs = work.alloc<double>(wsz);
     int* didx = tmp.add(upload(idx_all, stream));
@@ -2045,8 +2099,12 @@ class Engine {
   PinnedStage stage;  // host staging of this handle's factorization uploads
   struct StageScope {
     PinnedStage* prev;
-    explicit StageScope(PinnedStage* s) : prev(t_stage) { t_stage = s; }
-    ~StageScope() { t_stage = prev; }
+    Arena* prev_scratch;
+    explicit StageScope(PinnedStage* s) : prev(t_stage), prev_scratch(t_scratch) { t_stage = s; }
+    ~StageScope() {
+      t_stage = prev;
+      t_scratch = prev_scratch;
+    }
   };
 
   void factor() {
