@@ -983,6 +983,7 @@ class Engine {
   void sync_quiet() { cudaStreamSynchronize(stream); }
 
   void release_workspace() {
+    drop_graphs();
     dfree(d_ua, stream);
     dfree(d_ub, stream);
     dfree(d_pcg, stream);
@@ -990,7 +991,17 @@ class Engine {
     ws_nrhs = pcg_nrhs = 0;
   }
 
+  // CUDA graphs of the apply sweep (boundary zeroing, output clearing and every
+  // launch of the plan), one per (direction, right-hand-side count); valid
+  // while the plans and the apply workspace stay as they were captured
+  std::map<std::pair<int, int>, cudaGraphExec_t> apply_graphs;
+  void drop_graphs() {
+    for (auto& kv : apply_graphs) cudaGraphExecDestroy(kv.second);
+    apply_graphs.clear();
+  }
+
   void release_plans() {
+    drop_graphs();
     plan_inv.bufs.release(stream);
     plan_fwd.bufs.release(stream);
     plan_inv.launches.clear();
@@ -2340,6 +2351,7 @@ class Engine {
   void ensure_workspace(int nrhs) {
     if (!plans_built || contrib_cap < nrhs) build_plans(std::max(nrhs, contrib_cap));
     if (ws_nrhs >= nrhs && d_ua) return;
+    drop_graphs();
     dfree(d_ua, stream);
     dfree(d_ub, stream);
     d_ua = dalloc<double>(n3 * nrhs, stream);
@@ -2373,10 +2385,36 @@ class Engine {
     for (int c = 0; c < nrhs; ++c)
       HIF_CK(cudaMemcpyAsync(d_ua + c * n3, du + c * ldu, n3 * 8, cudaMemcpyDeviceToDevice,
                              stream));
-    timed(HIF_KCLASS_VECTOR, 0, 8.0 * n3 * nrhs,
-          [&] { launch_zero_boundary(d_ua, NC, nrhs, n3, stream); });
-    HIF_CK(cudaMemsetAsync(d_ub, 0, n3 * nrhs * 8, stream));
-    run_plan(inverse ? plan_inv : plan_fwd, nrhs);
+    auto sweep = [&] {
+      timed(HIF_KCLASS_VECTOR, 0, 8.0 * n3 * nrhs,
+            [&] { launch_zero_boundary(d_ua, NC, nrhs, n3, stream); });
+      HIF_CK(cudaMemsetAsync(d_ub, 0, n3 * nrhs * 8, stream));
+      run_plan(inverse ? plan_inv : plan_fwd, nrhs);
+    };
+    if (profile) {
+      sweep();  // per-launch events: no graph
+    } else {
+      const std::pair<int, int> key(inverse ? 1 : 0, nrhs);
+      auto it = apply_graphs.find(key);
+      if (it == apply_graphs.end()) {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        HIF_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          sweep();
+        } catch (...) {
+          cudaStreamEndCapture(stream, &g);
+          if (g) cudaGraphDestroy(g);
+          throw;
+        }
+        HIF_CK(cudaStreamEndCapture(stream, &g));
+        const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        HIF_CK(ie);
+        it = apply_graphs.emplace(key, ge).first;
+      }
+      HIF_CK(cudaGraphLaunch(it->second, stream));
+    }
     for (int c = 0; c < nrhs; ++c)
       HIF_CK(cudaMemcpyAsync(du + c * ldu, d_ub + c * n3, n3 * 8, cudaMemcpyDeviceToDevice,
                              stream));
