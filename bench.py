@@ -291,6 +291,37 @@ def run_serving(hb, synth, prec: int, nreq: int, rate: float, budget_gb: float =
             "peak_resident_ops": max_resident, "errors": errors[:4]}
 
 
+def run_multi_rhs(hb, synth, torch, dev, prec: int, n: int = 96, nrhs: int = 64):
+    """High-contrast operator with many right-hand sides in one batched solve:
+    a piecewise constant on 8^3 sub-cubes with values 10^U(-3, 3) (seed 1),
+    V = 1e-2, eps = 1e-8, 64 right-hand sides N(0, 1) (seeds 0..63), PCG to
+    1e-10 with every right-hand side in the same preconditioner applies."""
+    N = n - 1
+    ax, ay, az = synth.face_coefficients_blocks(N, 1)
+    V = np.full((n + 1,) * 3, 1e-2)
+    f = hb.HIFFactor(N, 4, 1e-8, hb.PARTITION_CLIPPED)
+    f.set_option(hb.OPT_PRECISION, prec)
+    stream = torch.cuda.Stream(device=dev)
+    hb.set_stream(f, stream.cuda_stream)
+    hb.SetupStencilFaces(f, N, 1.0 / n, ax, ay, az, V)
+    b = np.asfortranarray(np.stack([synth.dof_vector(N, s) for s in range(nrhs)], axis=1))
+    db = torch.from_numpy(np.ascontiguousarray(b.T)).to(dev)  # column c contiguous
+    dx = torch.zeros_like(db)
+    f.Factor()
+    f.solve_pcg_device(db.data_ptr(), dx.data_ptr(), nrhs, n ** 3, 1e-10, 200)  # warm
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    f.Factor()
+    e1.record(stream)
+    it, rr = f.solve_pcg_device(db.data_ptr(), dx.data_ptr(), nrhs, n ** 3, 1e-10, 200)
+    e2.record(stream)
+    e2.synchronize()
+    f.close()
+    return {"factor_s": e0.elapsed_time(e1) / 1e3, "solve_s": e1.elapsed_time(e2) / 1e3,
+            "rhs": nrhs, "pcg_iters_max": int(np.max(it)), "relres_max": float(np.max(rr))}
+
+
 def run_ours(args, rank: int, world: int):
     import torch
     import torch.distributed as dist
@@ -514,11 +545,22 @@ def run_ours(args, rank: int, world: int):
                           "factor_s": r["factor_s"], "solve_ms": r["solve_ms"],
                           "solves_per_s": 1e3 / r["solve_ms"], "pcg_iters": r["pcg_iters"],
                           "pcg_relres": r["pcg_relres"]}
-    if not args.no_serving:
+    if not (args.no_multi_rhs and args.no_serving):
         # the n = 128 operator and its pool memory leave the device first
         f.close()
         torch.cuda.synchronize()
         hb.trim_device_pool()
+    if not args.no_multi_rhs:
+        mr = {}
+        for name, prec in (("fp64", hb.PRECISION_FP64), ("mixed", hb.PRECISION_MIXED)):
+            if prec in runs:
+                mr[name] = run_multi_rhs(hb, synth, torch, dev, prec)
+        line["multi_rhs"] = {
+            "workload": "n=96 (clipped partition), a piecewise constant on 8^3 sub-cubes, "
+                        "10^U(-3,3) seed 1, V=1e-2, eps=1e-8, 64 RHS N(0,1) seeds 0..63 in one "
+                        "batched PCG to 1e-10",
+            **mr}
+    if not args.no_serving:
         serve = {}
         for name, prec in (("fp64", hb.PRECISION_FP64), ("mixed", hb.PRECISION_MIXED)):
             if prec in runs:
@@ -553,6 +595,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling)")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
+    ap.add_argument("--no-multi-rhs", action="store_true", help="skip the 64-RHS workload")
     ap.add_argument("--serve-requests", type=int, default=80)
     ap.add_argument("--serve-rate", type=float, default=8.0, help="arrivals per second")
     args = ap.parse_args()
