@@ -35,6 +35,7 @@
 #include <atomic>
 #include <memory>
 #include <string>
+#include <exception>
 #include <thread>
 #include <vector>
 
@@ -916,6 +917,7 @@ class Engine {
   }
 
   ~Engine() {
+    join_face_partition();
     sync_quiet();
     for (Pending& pd : pending) {
       cudaEventDestroy(pd.a);
@@ -1173,6 +1175,7 @@ class Engine {
     });
     st.n_red = red_all.size();
     st.n_skel = skel_all.size();
+    start_face_partition(level, red_all);
     t_host += wall() - th;
 
     track((bsz + asz) * 8);
@@ -1293,6 +1296,79 @@ class Engine {
   }
 
   // ---- skeletonization phase (LevelFactorSkel, src/Factor.cpp:232-260) -----
+  // SkelInteractionIndexData for every TOP / FRONT / LEFT face of the level
+  // (src/Factor.cpp:645-755), over the given remaining-DOF mask.
+  void partition_faces(int level, const uint8_t* mask, std::vector<BlockInfo>& blocks,
+                       std::vector<std::vector<int>>& rows_l) const {
+    const int cpd = cells_per_dir(level);
+    Partitioner part{N, P, NC, mask};
+    const int ncell = cpd * cpd * cpd;
+    std::vector<std::vector<BlockInfo>> pb(ncell);
+    std::vector<std::vector<std::vector<int>>> pr(ncell);
+    parallel_for(ncell, [&](int idx) {
+      const int c[3] = {idx / (cpd * cpd), (idx / cpd) % cpd, idx % cpd};
+      std::vector<int> rw, cl;
+      for (int face : {TOP, FRONT, LEFT}) {
+        int nb[3];
+        if (!part.skel_interaction(level, c, face, rw, cl, nb)) continue;
+        if (cl.empty()) continue;
+        BlockInfo b;
+        b.face = face;
+        b.global = cl;
+        b.cell = idx;
+        b.nbr = (nb[0] * cpd + nb[1]) * cpd + nb[2];
+        pb[idx].push_back(std::move(b));
+        pr[idx].push_back(rw);
+      }
+    });
+    for (int idx = 0; idx < ncell; ++idx)
+      for (size_t q = 0; q < pb[idx].size(); ++q) {
+        blocks.push_back(std::move(pb[idx][q]));
+        rows_l.push_back(std::move(pr[idx][q]));
+      }
+  }
+
+  // The face partition of a level depends only on the DOFs left after that
+  // level's cell eliminations, which are known once its cell partition is: it
+  // runs on a host thread while the cell phase is assembled and eliminated.
+  struct FacePartition {
+    int level = -1;
+    std::vector<uint8_t> mask;
+    std::vector<BlockInfo> blocks;
+    std::vector<std::vector<int>> rows_l;
+    std::exception_ptr err;
+  };
+  FacePartition face_pre;
+  std::thread face_thread;
+  void start_face_partition(int level, const std::vector<int>& red) {
+    join_face_partition();
+    if (level >= L - 1) return;
+    face_pre = FacePartition{};
+    face_pre.level = level;
+    face_pre.mask = rem;
+    for (int p : red) face_pre.mask[p] = 0;
+    face_thread = std::thread([this, level] {
+      try {
+        partition_faces(level, face_pre.mask.data(), face_pre.blocks, face_pre.rows_l);
+      } catch (...) {
+        face_pre.err = std::current_exception();
+      }
+    });
+  }
+  void join_face_partition() {
+    if (face_thread.joinable()) face_thread.join();
+  }
+  bool take_face_partition(int level, std::vector<BlockInfo>& blocks,
+                           std::vector<std::vector<int>>& rows_l) {
+    join_face_partition();
+    if (face_pre.level != level) return false;
+    face_pre.level = -1;
+    if (face_pre.err) std::rethrow_exception(face_pre.err);
+    blocks = std::move(face_pre.blocks);
+    rows_l = std::move(face_pre.rows_l);
+    return true;
+  }
+
   void skel_phase(int level, Sources& cells, Sources& out) {
     double th = wall();
     const int cpd = cells_per_dir(level);
@@ -1300,35 +1376,10 @@ class Engine {
     st.level = level;
     st.skel = true;
     st.cpd = cpd;
-    Partitioner part{N, P, NC, rem.data()};
     std::vector<std::vector<int>> rows_l;
     std::vector<BlockInfo>& blocks = st.blocks;
-    {
-      const int ncell = cpd * cpd * cpd;
-      std::vector<std::vector<BlockInfo>> pb(ncell);
-      std::vector<std::vector<std::vector<int>>> pr(ncell);
-      parallel_for(ncell, [&](int idx) {
-        const int c[3] = {idx / (cpd * cpd), (idx / cpd) % cpd, idx % cpd};
-        std::vector<int> rw, cl;
-        for (int face : {TOP, FRONT, LEFT}) {
-          int nb[3];
-          if (!part.skel_interaction(level, c, face, rw, cl, nb)) continue;
-          if (cl.empty()) continue;
-          BlockInfo b;
-          b.face = face;
-          b.global = cl;
-          b.cell = idx;
-          b.nbr = (nb[0] * cpd + nb[1]) * cpd + nb[2];
-          pb[idx].push_back(std::move(b));
-          pr[idx].push_back(rw);
-        }
-      });
-      for (int idx = 0; idx < ncell; ++idx)
-        for (size_t q = 0; q < pb[idx].size(); ++q) {
-          blocks.push_back(std::move(pb[idx][q]));
-          rows_l.push_back(std::move(pr[idx][q]));
-        }
-    }
+    if (!take_face_partition(level, blocks, rows_l))
+      partition_faces(level, rem.data(), blocks, rows_l);
     const int nf = (int)blocks.size();
     // M blocks (rows x cols) and ID workspace
     std::vector<long long> o_rows(nf), o_cols(nf), o_M(nf), o_W(nf), o_i(nf);
@@ -2125,6 +2176,8 @@ class Engine {
     sync();
     stage.reset();
     StageScope scope(&stage);
+    join_face_partition();
+    face_pre.level = -1;
     if (partition == HIF_PARTITION_CLIPPED && NC % P != 0)
       throw Error{HIF_ERR_ARG, "clipped partition needs (N+1) divisible by P"};
     initialize();
