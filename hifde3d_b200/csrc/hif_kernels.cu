@@ -300,7 +300,7 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-__global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict__ descs,
+__global__ void __launch_bounds__(512, 1) k_dgemm128(const GemmDesc* __restrict__ descs,
                                                      const int* __restrict__ tile_off, int nd) {
   extern __shared__ double lsm[];
   double* As = lsm;                                  // [stage][k][kLAStride]
@@ -318,8 +318,8 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
     double* as = As + stage * kLBK * kLAStride;
     double* bs = Bs + stage * kLBK * kLBStride;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int e = tid + 256 * q;
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 512 * q;
       int mm, kk;
       if (g.transA == 0) { mm = e % kLBM; kk = e / kLBM; } else { mm = e / kLBK; kk = e % kLBK; }
       const int gm = m0 + mm, gk = k0 + kk;
@@ -330,8 +330,8 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
       cp_async8(as + kk * kLAStride + mm, src, ok);
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int e = tid + 256 * q;
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 512 * q;
       int nn, kk;
       if (g.transB == 0) { kk = e % kLBK; nn = e / kLBK; } else { nn = e % kLBN; kk = e / kLBN; }
       const int gn = n0 + nn, gk = k0 + kk;
@@ -343,23 +343,24 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
     }
   };
 
-  // FP64 tensor cores: mma.sync m8n8k4 (DMMA). 8 warps as 2 (m) x 4 (n), warp
-  // tile 64 x 32 = 8 x 4 MMA tiles. Fragments (PTX ISA, m8n8k4 .f64): with
-  // g = lane / 4, t = lane % 4, A holds (row g, k t), B holds (k t, col g),
-  // C holds (row g, cols 2t and 2t + 1).
+  // FP64 tensor cores: mma.sync m8n8k4 (DMMA). 16 warps as 4 (m) x 4 (n), warp
+  // tile 32 x 32 = 4 x 4 MMA tiles (four warps per SM sub-partition keep the
+  // DMMA pipe fed across the fixed issue spacing of one warp). Fragments (PTX
+  // ISA, m8n8k4 .f64): with g = lane / 4, t = lane % 4, A holds (row g, k t),
+  // B holds (k t, col g), C holds (row g, cols 2t and 2t + 1).
   const int lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
   const int gq = lane >> 2, tq = lane & 3;
-  double acc[8][4][2];
+  double acc[4][4][2];
 #pragma unroll
-  for (int a = 0; a < 8; ++a)
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 
   double* Cs = lsm + kLStages * kLBK * (kLAStride + kLBStride);  // [col][row], 128 x 128
   const bool prefetch_c = g.beta != 0.0;
   if (prefetch_c) {
-    for (int e = tid; e < kLBM * kLBN; e += 256) {
+    for (int e = tid; e < kLBM * kLBN; e += 512) {
       const int i = e % kLBM, j = e / kLBM;
       const bool ok = (m0 + i) < g.m && (n0 + j) < g.n;
       cp_async8(Cs + e, ok ? g.C + (m0 + i) + (long long)(n0 + j) * g.ldc : g.C, ok);
@@ -381,13 +382,13 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
     const double* bs = Bs + (t % kLStages) * kLBK * kLBStride;
 #pragma unroll
     for (int k4 = 0; k4 < kLBK; k4 += 4) {
-      double af[8], bf[4];
+      double af[4], bf[4];
 #pragma unroll
-      for (int a = 0; a < 8; ++a) af[a] = as[(k4 + tq) * kLAStride + wm + a * 8 + gq];
+      for (int a = 0; a < 4; ++a) af[a] = as[(k4 + tq) * kLAStride + wm + a * 8 + gq];
 #pragma unroll
       for (int b = 0; b < 4; ++b) bf[b] = bs[(k4 + tq) * kLBStride + wn + b * 8 + gq];
 #pragma unroll
-      for (int a = 0; a < 8; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b)
           asm volatile(
@@ -399,7 +400,7 @@ __global__ void __launch_bounds__(256, 1) k_dgemm128(const GemmDesc* __restrict_
   cp_async_wait<0>();
   __syncthreads();
 #pragma unroll
-  for (int a = 0; a < 8; ++a) {
+  for (int a = 0; a < 4; ++a) {
     const int gm = m0 + wm + a * 8 + gq;
     if (gm >= g.m) continue;
 #pragma unroll
@@ -425,7 +426,7 @@ void launch_dgemm(const GemmDesc* d_desc, const int* d_tile_off, int nd, int tot
       cudaFuncSetAttribute(k_dgemm128, cudaFuncAttributeMaxDynamicSharedMemorySize, kLSmemC);
       attr = true;
     }
-    k_dgemm128<<<total_tiles, 256, kLSmemC, s>>>(d_desc, d_tile_off, nd);
+    k_dgemm128<<<total_tiles, 512, kLSmemC, s>>>(d_desc, d_tile_off, nd);
   } else {
     k_dgemm<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
   }
