@@ -1000,6 +1000,131 @@ class Engine {
   void drop_graphs() {
     for (auto& kv : apply_graphs) cudaGraphExecDestroy(kv.second);
     apply_graphs.clear();
+    for (auto& kv : gemm_plans) kv.second.bufs.release(stream);
+    gemm_plans.clear();
+  }
+
+  // ---- apply for many right-hand sides: every GEMV launch of a plan as gather /
+  // GEMM / emit, so each factor matrix is read once per apply instead of once
+  // per 4 right-hand sides. Built per (direction, RHS count) from the plan's
+  // descriptors; launches only, so the sweep is still captured in a graph.
+  static constexpr int kGemmApplyMinRhs = 16;
+  struct GemmStage {
+    size_t launch = 0;  // plan launch (reduce-scatter launches are run as they are)
+    ApplyGatherDesc* d_gather = nullptr;
+    long long* d_goff = nullptr;
+    int ng = 0;
+    long long gtotal = 0;
+    GemmDesc* d_gemm = nullptr;
+    int* d_toff = nullptr;
+    int tiles = 0, tile = 64;
+    ApplyEmitDesc* d_emit = nullptr;
+    long long* d_eoff = nullptr;
+    long long etotal = 0;
+    double flops = 0;
+  };
+  struct GemmPlan {
+    std::vector<GemmStage> stages;
+    BufList bufs;
+  };
+  std::map<std::pair<int, int>, GemmPlan> gemm_plans;
+
+  GemmPlan& gemm_plan(ApplyPlan& plan, int inverse, int nrhs) {
+    const std::pair<int, int> key(inverse, nrhs);
+    auto it = gemm_plans.find(key);
+    if (it != gemm_plans.end()) return it->second;
+    GemmPlan gp;
+    long long xmax = 1, ymax = 1;
+    for (const ApplyLaunch& l : plan.launches) {
+      if (l.type != 0) continue;
+      long long xs = 0, ys = 0;
+      for (const GemvDesc& g : l.hdesc) {
+        xs += (long long)(g.trans ? g.m : g.n) * nrhs;
+        ys += (long long)(g.trans ? g.n : g.m) * nrhs;
+      }
+      xmax = std::max(xmax, xs);
+      ymax = std::max(ymax, ys);
+    }
+    double* xin = gp.bufs.add(dalloc<double>(xmax, stream));
+    double* yout = gp.bufs.add(dalloc<double>(ymax, stream));
+    for (size_t q = 0; q < plan.launches.size(); ++q) {
+      const ApplyLaunch& l = plan.launches[q];
+      GemmStage st;
+      st.launch = q;
+      if (l.type == 0) {
+        std::vector<ApplyGatherDesc> gd;
+        std::vector<ApplyEmitDesc> ed;
+        std::vector<GemmDesc> gm;
+        std::vector<long long> goff(1, 0), eoff(1, 0);
+        std::vector<int> toff(1, 0);
+        long long ox = 0, oy = 0;
+        const int tile = nrhs >= 48 ? 128 : 64;
+        for (const GemvDesc& g : l.hdesc) {
+          const int len = g.trans ? g.m : g.n, rows = g.trans ? g.n : g.m;
+          gd.push_back(ApplyGatherDesc{g.in_idx, xin + ox, len});
+          goff.push_back(goff.back() + (long long)len * nrhs);
+          GemmDesc m{};
+          m.C = yout + oy;
+          m.ldc = rows;
+          m.A = g.M;
+          m.lda = g.ld;
+          m.transA = g.trans;
+          m.B = xin + ox;
+          m.ldb = len;
+          m.m = rows;
+          m.n = nrhs;
+          m.k = len;
+          m.alpha = 1.0;
+          m.beta = 0.0;
+          gm.push_back(m);
+          toff.push_back(toff.back() + dgemm_tiles(rows, nrhs, tile));
+          ed.push_back(ApplyEmitDesc{yout + oy, g.out_idx, g.contrib, rows, g.mode, g.alpha});
+          eoff.push_back(eoff.back() + (long long)rows * nrhs);
+          st.flops += 2.0 * rows * len * nrhs;
+          ox += (long long)len * nrhs;
+          oy += (long long)rows * nrhs;
+        }
+        st.d_gather = gp.bufs.add(upload(gd, stream));
+        st.d_goff = gp.bufs.add(upload(goff, stream));
+        st.ng = (int)gd.size();
+        st.gtotal = goff.back();
+        st.d_gemm = gp.bufs.add(upload(gm, stream));
+        st.d_toff = gp.bufs.add(upload(toff, stream));
+        st.tiles = toff.back();
+        st.tile = tile;
+        st.d_emit = gp.bufs.add(upload(ed, stream));
+        st.d_eoff = gp.bufs.add(upload(eoff, stream));
+        st.etotal = eoff.back();
+      }
+      gp.stages.push_back(st);
+    }
+    return gemm_plans.emplace(key, std::move(gp)).first->second;
+  }
+
+  void run_gemm_plan(ApplyPlan& plan, GemmPlan& gp, int nrhs) {
+    double* vec[2] = {d_ua, d_ub};
+    for (GemmStage& st : gp.stages) {
+      ApplyLaunch& l = plan.launches[st.launch];
+      if (l.type == 0) {
+        timed(HIF_KCLASS_VECTOR, 0, 0, [&] {
+          launch_apply_gather(st.d_gather, st.d_goff, st.ng, st.gtotal, vec[l.in_vec], n3,
+                              stream);
+        });
+        timed(HIF_KCLASS_GEMV, st.flops, l.bytes, [&] {
+          launch_dgemm(st.d_gemm, st.d_toff, st.ng, st.tiles, stream, st.tile);
+        });
+        timed(HIF_KCLASS_VECTOR, 0, 0, [&] {
+          launch_apply_emit(st.d_emit, st.d_eoff, st.ng, st.etotal, vec[l.out_vec], n3,
+                            contrib_ld, stream);
+        });
+      } else {
+        timed(HIF_KCLASS_VECTOR, 0, 0, [&] {
+          launch_reduce_scatter(l.d_dof, l.d_off, l.d_slot, d_contrib, l.ndof, contrib_ld,
+                                l.alpha, vec[l.out_vec], nrhs, n3, stream);
+        });
+      }
+      HIF_CK(cudaGetLastError());
+    }
   }
 
   void release_plans() {
@@ -2438,11 +2563,14 @@ class Engine {
     for (int c = 0; c < nrhs; ++c)
       HIF_CK(cudaMemcpyAsync(d_ua + c * n3, du + c * ldu, n3 * 8, cudaMemcpyDeviceToDevice,
                              stream));
+    ApplyPlan& plan = inverse ? plan_inv : plan_fwd;
+    GemmPlan* gp = nrhs >= kGemmApplyMinRhs ? &gemm_plan(plan, inverse ? 1 : 0, nrhs) : nullptr;
     auto sweep = [&] {
       timed(HIF_KCLASS_VECTOR, 0, 8.0 * n3 * nrhs,
             [&] { launch_zero_boundary(d_ua, NC, nrhs, n3, stream); });
       HIF_CK(cudaMemsetAsync(d_ub, 0, n3 * nrhs * 8, stream));
-      run_plan(inverse ? plan_inv : plan_fwd, nrhs);
+      if (gp) run_gemm_plan(plan, *gp, nrhs);
+      else run_plan(plan, nrhs);
     };
     if (profile) {
       sweep();  // per-launch events: no graph

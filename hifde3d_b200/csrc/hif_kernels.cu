@@ -2438,6 +2438,62 @@ __global__ void __launch_bounds__(256) k_gemv_seg(const GemvSeg* __restrict__ se
   gemv_tile(sg.desc[di], t - sg.toff[di], nullptr, nullptr, 0, 0, 0);
 }
 
+__device__ __forceinline__ int find_desc_ll(const long long* __restrict__ off, int nd,
+                                            long long t) {
+  int lo = 0, hi = nd - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void k_apply_gather(const ApplyGatherDesc* __restrict__ descs,
+                               const long long* __restrict__ off, int nd, long long total,
+                               const double* __restrict__ u, long long ldu) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int di = find_desc_ll(off, nd, t);
+    const ApplyGatherDesc d = descs[di];
+    const long long e = t - off[di];
+    const int k = (int)(e % d.len);
+    const long long c = e / d.len;
+    d.dst[e] = u[d.idx[k] + c * ldu];
+  }
+}
+
+void launch_apply_gather(const ApplyGatherDesc* d_desc, const long long* d_off, int nd,
+                         long long total, const double* u, long long ldu, cudaStream_t s) {
+  if (total <= 0) return;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  k_apply_gather<<<blocks, 256, 0, s>>>(d_desc, d_off, nd, total, u, ldu);
+}
+
+__global__ void k_apply_emit(const ApplyEmitDesc* __restrict__ descs,
+                             const long long* __restrict__ off, int nd, long long total,
+                             double* __restrict__ u, long long ldu, long long contrib_ld) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int di = find_desc_ll(off, nd, t);
+    const ApplyEmitDesc d = descs[di];
+    const long long e = t - off[di];
+    const int i = (int)(e % d.rows);
+    const long long c = e / d.rows;
+    const double y = d.Y[e];
+    if (d.mode == 1) d.contrib[i + c * contrib_ld] = y;
+    else if (d.mode == 0) u[d.out_idx[i] + c * ldu] += d.alpha * y;
+    else u[d.out_idx[i] + c * ldu] = d.alpha * y;
+  }
+}
+
+void launch_apply_emit(const ApplyEmitDesc* d_desc, const long long* d_off, int nd,
+                       long long total, double* u, long long ldu, long long contrib_ld,
+                       cudaStream_t s) {
+  if (total <= 0) return;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  k_apply_emit<<<blocks, 256, 0, s>>>(d_desc, d_off, nd, total, u, ldu, contrib_ld);
+}
+
 void launch_gemv_seg(const GemvSeg* d_segs, const int* d_seg_off, int nseg, int total_tiles,
                      cudaStream_t s) {
   if (total_tiles <= 0) return;

@@ -128,6 +128,28 @@ void launch_member_cells(const int* d_skel, const long long* d_off, const int* d
 void launch_member_faces(const int* d_skel, const long long* d_off, const int* d_cnt,
                          const int* d_src, int nq, long long n3, int* d_dof_src, cudaStream_t s);
 
+// Apply for many right-hand sides as gather / GEMM / emit: the input rows of a
+// descriptor are gathered into a dense block (len x nrhs, ld len), multiplied
+// by op(M) with the batched GEMM, and the result (rows x nrhs, ld rows) is
+// emitted like the GEMV's output (mode 0: u[out] += alpha y; 1: contrib = y;
+// 2: u[out] = alpha y). Element counts are prefix sums over descriptors.
+struct ApplyGatherDesc {
+  const int* idx;
+  double* dst;
+  int len;
+};
+struct ApplyEmitDesc {
+  const double* Y;
+  const int* out_idx;
+  double* contrib;
+  int rows, mode;
+  double alpha;
+};
+void launch_apply_gather(const ApplyGatherDesc* d_desc, const long long* d_off, int nd,
+                         long long total, const double* u, long long ldu, cudaStream_t s);
+void launch_apply_emit(const ApplyEmitDesc* d_desc, const long long* d_off, int nd,
+                       long long total, double* u, long long ldu, long long contrib_ld,
+                       cudaStream_t s);
 // Apply: y = op(M) x[in] with x, y gathered / scattered through DOF lists.
 struct GemvDesc {
   const double* M;
