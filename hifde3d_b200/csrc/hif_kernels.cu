@@ -880,12 +880,9 @@ void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_statu
 }
 
 // --- blocked sweep ---------------------------------------------------------
-// Step for pivot block K = [k0, k1): D = B[K, K].
-//   diag:     Dinv = D^{-1} (Gauss-Jordan in shared memory)
-//   rowpanel: B[K, j] = Dinv B[K, j]           for j outside K
-//   update:   B[i, j] -= B[i, K] B[K, j]       for i, j outside K (dgemm)
-//   colpanel: B[i, K] = -B[i, K] Dinv           for red rows i outside K
-//   setdiag:  B[K, K] = Dinv
+// Step for pivot block K = [k0, k1) of A22: Dinv = B[K, K]^{-1} (k_sweep_diag);
+// the row / column panels and the rank-128 update are batched GEMMs issued by
+// the host; B[K, K] = Dinv (k_sweep_setdiag).
 // Register-resident Gauss-Jordan inverse of the pivot block: thread (tx, ty)
 // of a 16 x 32 grid holds the 4 x 8 sub-block rows 4 ty.., columns 8 tx.. in
 // registers. At step k the owners of the old row k and column k publish them
@@ -999,84 +996,6 @@ void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, i
     attr = true;
   }
   k_sweep_diag<<<nact, 512, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status, sym);
-}
-
-// Row panel: tile of up to 64 columns [lo, hi) of rows K.
-__global__ void __launch_bounds__(256) k_sweep_rowpanel(const SweepDesc* __restrict__ descs,
-                                                        const int4* __restrict__ tiles, int k0,
-                                                        const double* __restrict__ dinv) {
-  const int4 t = tiles[blockIdx.x];
-  const SweepDesc d = descs[t.x];
-  const int nb = min(kSweepNB, d.r - k0);
-  const int w = t.z - t.y;
-  extern __shared__ double panel_smem[];
-  double* Ds = panel_smem;
-  double* Ts = panel_smem + kSweepNB * kSweepNB;
-  const double* Dg = dinv + (long long)t.x * kSweepNB * kSweepNB;
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) Ds[e] = Dg[e];
-  for (int e = threadIdx.x; e < nb * w; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    Ts[e] = d.B[(k0 + i) + (long long)(t.y + j) * d.n];
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < nb * w; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    double acc = 0.0;
-    for (int kk = 0; kk < nb; ++kk) acc = fma(Ds[i + kk * nb], Ts[kk + j * nb], acc);
-    d.B[(k0 + i) + (long long)(t.y + j) * d.n] = acc;
-  }
-}
-
-void launch_sweep_rowpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
-                           const double* d_dinv, cudaStream_t s) {
-  if (ntiles <= 0) return;
-  const int smem = (kSweepNB * kSweepNB + kSweepNB * kPanelTile) * (int)sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_sweep_rowpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
-  k_sweep_rowpanel<<<ntiles, 256, smem, s>>>(d_desc, reinterpret_cast<const int4*>(d_tile_map),
-                                             k0, d_dinv);
-}
-
-// Column panel: tile of up to 64 rows [lo, hi) of columns K: B = -B Dinv.
-__global__ void __launch_bounds__(256) k_sweep_colpanel(const SweepDesc* __restrict__ descs,
-                                                        const int4* __restrict__ tiles, int k0,
-                                                        const double* __restrict__ dinv) {
-  const int4 t = tiles[blockIdx.x];
-  const SweepDesc d = descs[t.x];
-  const int nb = min(kSweepNB, d.r - k0);
-  const int h = t.z - t.y;
-  extern __shared__ double panel_smem[];
-  double* Ds = panel_smem;
-  double* Ts = panel_smem + kSweepNB * kSweepNB;
-  const double* Dg = dinv + (long long)t.x * kSweepNB * kSweepNB;
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) Ds[e] = Dg[e];
-  for (int e = threadIdx.x; e < h * nb; e += blockDim.x) {
-    const int i = e % h, j = e / h;
-    Ts[e] = d.B[(t.y + i) + (long long)(k0 + j) * d.n];
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < h * nb; e += blockDim.x) {
-    const int i = e % h, j = e / h;
-    double acc = 0.0;
-    for (int kk = 0; kk < nb; ++kk) acc = fma(Ts[i + kk * h], Ds[kk + j * nb], acc);
-    d.B[(t.y + i) + (long long)(k0 + j) * d.n] = -acc;
-  }
-}
-
-void launch_sweep_colpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
-                           const double* d_dinv, cudaStream_t s) {
-  if (ntiles <= 0) return;
-  const int smem = (kSweepNB * kSweepNB + kSweepNB * kPanelTile) * (int)sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_sweep_colpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
-  k_sweep_colpanel<<<ntiles, 256, smem, s>>>(d_desc, reinterpret_cast<const int4*>(d_tile_map),
-                                             k0, d_dinv);
 }
 
 __global__ void k_sweep_setdiag(const SweepDesc* __restrict__ descs,
@@ -2682,15 +2601,6 @@ void launch_zero_boundary(double* u, int NC, int nrhs, long long ldu, cudaStream
   k_zero_boundary<<<(int)((total + 255) / 256), 256, 0, s>>>(u, NC, nrhs, ldu);
 }
 
-__global__ void k_copy_vec(const double* __restrict__ x, double* __restrict__ y, long long n) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) y[t] = x[t];
-}
-
-void launch_copy_vec(const double* x, double* y, long long n, cudaStream_t s) {
-  if (n <= 0) return;
-  k_copy_vec<<<(int)((n + 255) / 256), 256, 0, s>>>(x, y, n);
-}
 
 // ---- deterministic dot products: fixed grid, fixed-order final sum --------
 __global__ void __launch_bounds__(256) k_dot_partial(const double* __restrict__ x,

@@ -279,17 +279,8 @@ void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_statu
 
 // Blocked sweep, one pivot block [k0, k0+nbk) of every active block.
 constexpr int kSweepNB = 128;
-constexpr int kPanelTile = 64;  // rows / columns per panel tile
 void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
                        double* d_dinv, int* d_status, cudaStream_t s, int sym = 0);
-// Panel tile maps hold 4 ints per tile: {descriptor, lo, hi, unused} with
-// hi - lo <= kPanelTile; the row panel covers columns [lo, hi) of pivot rows,
-// the column panel rows [lo, hi) of pivot columns. d_dinv holds kSweepNB^2
-// doubles per descriptor.
-void launch_sweep_rowpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
-                           const double* d_dinv, cudaStream_t s);
-void launch_sweep_colpanel(const SweepDesc* d_desc, const int* d_tile_map, int ntiles, int k0,
-                           const double* d_dinv, cudaStream_t s);
 void launch_sweep_setdiag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
                           const double* d_dinv, cudaStream_t s);
 
@@ -393,7 +384,6 @@ void launch_setup_faces(const double* d_ax, const double* d_ay, const double* d_
 void launch_stencil_apply(const double* d_band, int NC, const double* x, double* y, int nrhs,
                           long long ldx, int transpose, cudaStream_t s);
 void launch_zero_boundary(double* u, int NC, int nrhs, long long ldu, cudaStream_t s);
-void launch_copy_vec(const double* x, double* y, long long n, cudaStream_t s);
 
 // Deterministic dot products: out[c] = sum_i x[i + c ld] y[i + c ld] (per rhs c).
 void launch_dot(const double* x, const double* y, long long n, int nrhs, long long ld,
