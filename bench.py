@@ -349,6 +349,9 @@ def run_ours(args, rank: int, world: int):
     peak_fp64 = fp64_gemm_peak(torch, dev) if rank == 0 else None
 
     f = hb.HIFFactor(N, 4, eps)
+    # tile shapes of the batched FP64 products are tuned during the warm-up
+    # factorizations (two suffice for every batch signature to decide)
+    f.set_option(hb.OPT_AUTOTUNE, 0 if args.no_autotune else 1)
     stream = torch.cuda.Stream(device=dev)
     hb.set_stream(f, stream.cuda_stream)
     h = 1.0 / NC
@@ -537,6 +540,7 @@ def run_ours(args, rank: int, world: int):
         # profiled step) times the timed steps
         "gpu_launches": int(sum(v["launches"] for v in kst.values())) * args.steps,
         "cpu_baseline": cpu,
+        "autotune": None if args.no_autotune else f.autotune_stats(),
     }
     for name, prec in (("fp64", hb.PRECISION_FP64), ("mixed", hb.PRECISION_MIXED)):
         if prec in runs:
@@ -596,6 +600,7 @@ def main():
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     ap.add_argument("--no-multi-rhs", action="store_true", help="skip the 64-RHS workload")
+    ap.add_argument("--no-autotune", action="store_true", help="fixed tile rules")
     ap.add_argument("--serve-requests", type=int, default=80)
     ap.add_argument("--serve-rate", type=float, default=8.0, help="arrivals per second")
     args = ap.parse_args()

@@ -30,7 +30,7 @@ HIF_OK, HIF_ERR_ARG, HIF_ERR_CUDA, HIF_ERR_NOMEM, HIF_ERR_SINGULAR = 0, 1, 2, 3,
 HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET = 5, 6, 7
 PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
 OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE, OPT_ID_GROUP_MIN_N = 1, 2, 3, 4, 5
-OPT_PRECISION = 6
+OPT_PRECISION, OPT_AUTOTUNE = 6, 7
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 KCLASS_NAMES = ["gather", "gemm", "sweep_small", "sweep_panel", "id", "gemv", "copy", "vector",
                 "qr", "gemm_mixed"]
@@ -74,6 +74,7 @@ _SIGNATURES = {
     "hif_set_replay_pivots": [_p, _i, _i, _ip, _ip],
     "hif_factor_stats": [_p, _dp, _dp, _dp, _dp, _dp, _llp],
     "hif_kernel_stats": [_p, _i, _llp, _dp, _dp, _dp],
+    "hif_autotune_stats": [_p, _ip, _ip, _ip],
     "hif_memory": [_p, _llp, _llp],
     "hif_trim": [_p],
     "hif_trim_device_pool": [],
@@ -314,6 +315,13 @@ class HIFFactor:
                                           ctypes.byref(fl), ctypes.byref(by)))
             out[name] = {"launches": n.value, "ms": ms.value, "flops": fl.value, "bytes": by.value}
         return out
+
+    def autotune_stats(self) -> dict:
+        """OPT_AUTOTUNE tuner: batch signatures seen, decided, and how many chose 128 x 128."""
+        n, d, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().hif_autotune_stats(self._h, ctypes.byref(n), ctypes.byref(d),
+                                        ctypes.byref(c)))
+        return {"signatures": n.value, "decided": d.value, "chose_128": c.value}
 
     def memory(self) -> dict:
         fb, wb = ctypes.c_longlong(), ctypes.c_longlong()

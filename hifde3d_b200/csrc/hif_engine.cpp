@@ -325,6 +325,59 @@ struct Sources {
 // a single output tile along the aliased dimension), else 64x64. Problems with
 // a reduction much longer than their output dimensions are split along k into
 // partial products and summed in a fixed order.
+// Online tile-shape tuner for the batched FP64 products (HIF_OPT_AUTOTUNE).
+// A batch is keyed by its class and the log2 buckets of its work and mean
+// shape; until both candidate tiles (64 x 64 FFMA, 128 x 128 DMMA) have run
+// once for a key, the next untried one runs with events around it; after that
+// the faster is kept. Events are read when the factorization synchronises.
+struct GemmTuner {
+  struct Rec {
+    double ms[2] = {0.0, 0.0};
+    int runs[2] = {0, 0};
+    int choice = -1;
+  };
+  struct Pending {
+    long long key;
+    int cand;
+    cudaEvent_t a, b;
+  };
+  std::map<long long, Rec> recs;
+  std::vector<Pending> pending;
+  static constexpr int kTiles[2] = {64, 128};
+  ~GemmTuner() {
+    for (Pending& p : pending) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+  }
+  void resolve() {
+    for (Pending& p : pending) {
+      float ms = 0;
+      if (cudaEventSynchronize(p.b) == cudaSuccess &&
+          cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+        Rec& r = recs[p.key];
+        r.ms[p.cand] += ms;
+        r.runs[p.cand] += 1;
+        if (r.runs[0] > 0 && r.runs[1] > 0)
+          r.choice = (r.ms[0] / r.runs[0] <= r.ms[1] / r.runs[1]) ? 0 : 1;
+      }
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+    pending.clear();
+  }
+};
+thread_local GemmTuner* t_tuner = nullptr;
+
+int ilog2_bucket(double x) {
+  int b = 0;
+  while (x >= 2.0 && b < 62) {
+    x *= 0.5;
+    ++b;
+  }
+  return b;
+}
+
 // Temporaries of one call: from t_scratch (given back when the scope ends) or
 // from the pool (released with tmp).
 struct ScratchScope {
@@ -439,13 +492,44 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
   }
   bool lower = false;  // lower-triangle products are tiled by 128 x 128
   for (const GemmDesc& x : g) lower = lower || x.lower;
-  const int tile = force_tile ? force_tile : ((lower || big >= 0.5 * all) ? 128 : 64);
+  int tile = force_tile ? force_tile : ((lower || big >= 0.5 * all) ? 128 : 64);
+  GemmTuner::Pending tp{0, -1, nullptr, nullptr};
+  if (t_tuner && !force_tile && !lower && !g.empty()) {
+    double sm = 0, sn = 0, sk = 0;
+    for (const GemmDesc& x : g) {
+      sm += x.m;
+      sn += x.n;
+      sk += x.k;
+    }
+    const double cnt = (double)g.size();
+    const long long key = ((long long)cls << 40) | ((long long)ilog2_bucket(fl) << 30) |
+                          ((long long)ilog2_bucket(sm / cnt) << 20) |
+                          ((long long)ilog2_bucket(sn / cnt) << 10) | ilog2_bucket(sk / cnt);
+    GemmTuner::Rec& r = t_tuner->recs[key];
+    if (r.choice >= 0) {
+      tile = GemmTuner::kTiles[r.choice];
+    } else {
+      const int cand = r.runs[0] == 0 ? 0 : 1;
+      tile = GemmTuner::kTiles[cand];
+      tp.key = key;
+      tp.cand = cand;
+    }
+  }
   std::vector<int> toff(1, 0);
   for (const GemmDesc& x : g) toff.push_back(toff.back() + dgemm_tiles(x.m, x.n, tile));
   if (toff.back() == 0 && red.empty()) return;
   GemmDesc* dg = tmp.add(upload(g, stream));
   int* dt = tmp.add(upload(toff, stream));
+  if (tp.cand >= 0) {
+    HIF_CK(cudaEventCreate(&tp.a));
+    HIF_CK(cudaEventCreate(&tp.b));
+    HIF_CK(cudaEventRecord(tp.a, stream));
+  }
   timed(cls, fl, 0.0, [&] { launch_dgemm(dg, dt, (int)g.size(), toff.back(), stream, tile); }, 1);
+  if (tp.cand >= 0) {
+    HIF_CK(cudaEventRecord(tp.b, stream));
+    t_tuner->pending.push_back(tp);
+  }
   if (!red.empty()) {
     SplitKDesc* dr = tmp.add(upload(red, stream));
     timed(cls, 0.0, 0.0, [&] { launch_splitk_reduce(dr, (int)red.size(), stream); }, 1);
@@ -2284,13 +2368,21 @@ class Engine {
 
   // ---- Factor (src/Factor.cpp:41-63) --------------------------------------
   PinnedStage stage;  // host staging of this handle's factorization uploads
+  GemmTuner tuner;
+  bool autotune = false;
   struct StageScope {
     PinnedStage* prev;
     Arena* prev_scratch;
-    explicit StageScope(PinnedStage* s) : prev(t_stage), prev_scratch(t_scratch) { t_stage = s; }
+    GemmTuner* prev_tuner;
+    StageScope(PinnedStage* s, GemmTuner* tu)
+        : prev(t_stage), prev_scratch(t_scratch), prev_tuner(t_tuner) {
+      t_stage = s;
+      t_tuner = tu;
+    }
     ~StageScope() {
       t_stage = prev;
       t_scratch = prev_scratch;
+      t_tuner = prev_tuner;
     }
   };
 
@@ -2300,7 +2392,7 @@ class Engine {
     // copies are complete
     sync();
     stage.reset();
-    StageScope scope(&stage);
+    StageScope scope(&stage, autotune ? &tuner : nullptr);
     join_face_partition();
     face_pre.level = -1;
     if (partition == HIF_PARTITION_CLIPPED && NC % P != 0)
@@ -2330,6 +2422,7 @@ class Engine {
     mark("end", L);
     sync();
     t_total = wall() - t0;
+    tuner.resolve();
     report_marks();
     int st = 0;
     HIF_CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
@@ -2998,6 +3091,9 @@ int hif_set_option(hif_handle h, int option, long long value) {
       if (value != HIF_PRECISION_FP64 && value != HIF_PRECISION_MIXED) return HIF_ERR_ARG;
       h->e->precision = (int)value;
       return HIF_OK;
+    case HIF_OPT_AUTOTUNE:
+      h->e->autotune = value != 0;
+      return HIF_OK;
     case HIF_OPT_ID_GROUP_MIN_N:
       if (value < 2) return HIF_ERR_ARG;
       h->e->kGroupMinN = (int)value;
@@ -3316,6 +3412,23 @@ int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, 
     if (ms) *ms = k.ms;
     if (flops) *flops = k.flops;
     if (bytes) *bytes = k.bytes;
+  });
+}
+
+int hif_autotune_stats(hif_handle h, int* signatures, int* decided, int* chose_128) {
+  if (!h) return HIF_ERR_ARG;
+  return guarded([&] {
+    h->e->sync();
+    h->e->tuner.resolve();
+    int n = 0, d = 0, c = 0;
+    for (const auto& kv : h->e->tuner.recs) {
+      ++n;
+      if (kv.second.choice >= 0) ++d;
+      if (kv.second.choice == 1) ++c;
+    }
+    if (signatures) *signatures = n;
+    if (decided) *decided = d;
+    if (chose_128) *chose_128 = c;
   });
 }
 

@@ -145,17 +145,22 @@ int hif_block_pivots(hif_handle h, int level, int b, int* jpvt, double* rdiag);
 
 enum hif_option {
   HIF_OPT_KEEP_SCHUR = 1,    /* keep every Schur complement for hif_block_matrix(which=4) */
-  HIF_OPT_VERBOSE = 2,       /* per-phase timings on stderr */
+  HIF_OPT_VERBOSE = 2,       /* 1: per-phase wall times on stderr (synchronising);
+                                2: per-phase host and device times, no synchronisation */
   HIF_OPT_MEM_BUDGET_MB = 3, /* refuse factorizations whose device memory exceeds this */
   HIF_OPT_PROFILE = 4,       /* time every launch with CUDA events (resets the counters) */
   HIF_OPT_ID_GROUP_MIN_N = 5, /* faces with at least this many columns get a CTA group (default 512) */
-  HIF_OPT_PRECISION = 6       /* HIF_PRECISION_FP64 (default) or HIF_PRECISION_MIXED */
+  HIF_OPT_PRECISION = 6,      /* HIF_PRECISION_FP64 (default) or HIF_PRECISION_MIXED */
+  HIF_OPT_AUTOTUNE = 7        /* 1: tune the tile shape of the batched FP64 products online
+                                 (each batch signature tries both tiles on the first
+                                 factorizations, then keeps the faster); results may then
+                                 differ in the last bits between those factorizations */
 };
-/* Arithmetic of the factorization. MIXED: the Schur-complement updates of every
- * elimination (the X and skeleton-row regions) run on the tensor cores as split-TF32
- * products with FP32 accumulation; the pivoted QR, the row compression, the
- * eliminated diagonal blocks (A22 and its inverse), the factor storage, the apply and
- * the PCG residual stay FP64. */
+/* Arithmetic of the factorization. MIXED: the Schur complements S = A11 - A12 X of the
+ * eliminations run on the tcgen05 tensor cores as split-TF32 products with FP64
+ * accumulation every 256 terms; the interpolative decompositions of the large faces
+ * use the pivoted Cholesky of M^T M (FP64) instead of the column-pivoted QR; A22^{-1},
+ * X, the factor storage, the apply and the PCG residual stay FP64. */
 enum hif_precision { HIF_PRECISION_FP64 = 0, HIF_PRECISION_MIXED = 1 };
 int hif_set_option(hif_handle h, int option, long long value);
 
@@ -200,6 +205,10 @@ enum hif_kernel_class {
  * flops and bytes of one kernel class since HIF_OPT_PROFILE was last set. */
 int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, double* flops,
                      double* bytes);
+
+/* State of the HIF_OPT_AUTOTUNE tuner: batch signatures seen, signatures with a
+ * decision, and how many of those chose the 128 x 128 tensor-core tile. */
+int hif_autotune_stats(hif_handle h, int* signatures, int* decided, int* chose_128);
 
 /* Device memory held by the handle: the factor (kept until the next hif_factor or
  * hif_destroy) and the factorization workspace (kept for reuse by later
