@@ -30,10 +30,10 @@ HIF_OK, HIF_ERR_ARG, HIF_ERR_CUDA, HIF_ERR_NOMEM, HIF_ERR_SINGULAR = 0, 1, 2, 3,
 HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET = 5, 6, 7
 PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
 OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE, OPT_ID_GROUP_MIN_N = 1, 2, 3, 4, 5
-OPT_PRECISION, OPT_AUTOTUNE = 6, 7
+OPT_PRECISION, OPT_AUTOTUNE, OPT_SCHUR_SLICES, OPT_X_SLICES = 6, 7, 8, 9
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 KCLASS_NAMES = ["gather", "gemm", "sweep_small", "sweep_panel", "id", "gemv", "copy", "vector",
-                "qr", "gemm_mixed"]
+                "qr", "gemm_mixed", "gemm_int8"]
 TOP, BOTTOM, RIGHT, LEFT, FRONT, BACK = range(6)
 
 
@@ -85,6 +85,7 @@ _SIGNATURES = {
     "hif_pivoted_qr": [_dp, _i, _i, _ll, _ip],
     "hif_triangular_solve": [_dp, _i, _ll, _dp, _i, _ll],
     "hif_gemm_mixed_device": [_i, _i, _i, _i, _i, _d, _p, _ll, _p, _ll, _d, _p, _ll],
+    "hif_gemm_int8_device": [_i, _i, _i, _i, _i, _d, _p, _ll, _p, _ll, _d, _p, _ll, _i],
     "hif_server_create": [_ll, _i, _i, ctypes.POINTER(_p)],
     "hif_server_destroy": [_p],
     "hif_server_submit_factor": [_p, _i, _i, _i, _d, _i, _i, _d, _dp, _dp, _dp, _dp, _llp],
@@ -353,6 +354,15 @@ def GemmMixedDevice(transA: int, transB: int, m: int, n: int, k: int, alpha: flo
     products on the tcgen05 tensor cores with FP32 accumulation."""
     _check(lib().hif_gemm_mixed_device(int(transA), int(transB), m, n, k, float(alpha), _p(dA),
                                        lda, _p(dB), ldb, float(beta), _p(dC), ldc))
+
+
+def GemmInt8Device(transA: int, transB: int, m: int, n: int, k: int, alpha: float, dA: int,
+                   lda: int, dB: int, ldb: int, beta: float, dC: int, ldc: int,
+                   slices: int = 7) -> None:
+    """C = alpha op(A) op(B) + beta C on device pointers (column-major), FP64 from
+    exact int8 slice products on the tcgen05 tensor cores (Ozaki scheme)."""
+    _check(lib().hif_gemm_int8_device(int(transA), int(transB), m, n, k, float(alpha), _p(dA),
+                                      lda, _p(dB), ldb, float(beta), _p(dC), ldc, int(slices)))
 
 
 class Server:

@@ -537,14 +537,106 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
   HIF_CK(cudaGetLastError());
 }
 
+// FP64 products of a batch from int8 slices (Ozaki scheme, `slices` pieces per
+// operand value): the operands are converted once, then products whose k
+// exceeds kOzMaxK run as consecutive launches over k ranges (beta = 1 after
+// the first), which keeps every diagonal sum exact in int32.
+template <class Timed>
+void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t stream,
+                     Timed&& timed, int slices, int* status) {
+  if (gin.empty()) return;
+  ScratchScope scope;
+  const int bn = oz_tile_n(slices);
+  constexpr int kChunkTiles = kOzMaxK / kOzK;
+  long long parts = 0, nexp = 0;
+  for (const GemmDesc& x : gin) {
+    if (x.m <= 0 || x.n <= 0) continue;
+    const long long kt = (x.k + kOzK - 1) / kOzK;
+    parts += ((x.m + 127) / 128 + (x.n + 127) / 128) * kt * slices;
+    nexp += x.m + x.n;
+  }
+  if (nexp == 0) return;
+  signed char* cbuf = scratch_alloc<signed char>(std::max(1LL, parts) * kOzPart, tmp, stream);
+  int* ebuf = scratch_alloc<int>(nexp, tmp, stream);
+  std::vector<OzOperand> ops;
+  std::vector<int> ooff(1, 0);
+  std::vector<std::vector<OzGemm>> launches;
+  long long used = 0, eo = 0;
+  double fl = 0;
+  // work counted as the tensor cores' int8 operations: slices (slices + 1) / 2
+  // products of the padded tile shape, for the tiles computed
+  const double pairs = 0.5 * slices * (slices + 1);
+  for (const GemmDesc& x : gin) {
+    if (x.m <= 0 || x.n <= 0) continue;
+    const int kt = (x.k + kOzK - 1) / kOzK;
+    {
+      const int tm = (x.m + 127) / 128, tn = (x.n + bn - 1) / bn;
+      long long tiles = (long long)tm * tn;
+      if (x.lower) {
+        tiles = 0;
+        for (int i = 0; i < tm; ++i) tiles += std::min(tn, (i * 128 + 128 + bn - 1) / bn);
+      }
+      fl += pairs * 2.0 * 128.0 * bn * kOzK * kt * (double)tiles;
+    }
+    const int ta = (x.m + 127) / 128 * kt, tb = (x.n + 127) / 128 * kt;
+    signed char* pa = cbuf + used * kOzPart;
+    signed char* pb = cbuf + (used + (long long)ta * slices) * kOzPart;
+    used += (long long)(ta + tb) * slices;
+    int* ea = ebuf + eo;
+    int* eb = ea + x.m;
+    eo += x.m + x.n;
+    if (kt > 0) {
+      // A: element (i, kk) = op(A)[i, kk]; B: element (j, kk) = op(B)[kk, j]
+      ops.push_back(OzOperand{x.A, x.lda, x.transA, x.m, x.k, pa, ea});
+      ooff.push_back(ooff.back() + ta);
+      ops.push_back(OzOperand{x.B, x.ldb, x.transB ? 0 : 1, x.n, x.k, pb, eb});
+      ooff.push_back(ooff.back() + tb);
+    }
+    for (int c = 0, kt0 = 0; kt0 < kt || c == 0; ++c, kt0 += kChunkTiles) {
+      if ((int)launches.size() <= c) launches.emplace_back();
+      launches[c].push_back(OzGemm{pa, pb, ea, eb, x.C, x.ldc, x.m, x.n, kt, kt0,
+                                   std::min(kChunkTiles, std::max(0, kt - kt0)), x.alpha,
+                                   c == 0 ? x.beta : 1.0, x.lower});
+    }
+  }
+  timed(HIF_KCLASS_GEMM_INT8, fl, 0.0, [&] {
+    if (!ops.empty()) {
+      OzOperand* dops = tmp.add(upload(ops, stream));
+      int* doo = tmp.add(upload(ooff, stream));
+      launch_oz_convert(dops, doo, (int)ops.size(), ooff.back(), slices, ebuf, nexp, stream);
+    } else {
+      HIF_CK(cudaMemsetAsync(ebuf, 0x80, (size_t)nexp * sizeof(int), stream));
+    }
+    for (const std::vector<OzGemm>& lg : launches) {
+      std::vector<int> toff(1, 0);
+      for (const OzGemm& y : lg)
+        toff.push_back(toff.back() + (y.m + 127) / 128 * ((y.n + bn - 1) / bn));
+      OzGemm* dg = tmp.add(upload(lg, stream));
+      int* dt = tmp.add(upload(toff, stream));
+      launch_gemm_oz(dg, dt, (int)lg.size(), toff.back(), slices, status, stream);
+    }
+  }, (int)launches.size() + (ops.empty() ? 0 : 2));
+  HIF_CK(cudaGetLastError());
+}
+
 // Dense elimination of a batch of blocks: descs[b].B holds [A22 A21; A12 A11]
 // (ld n); on return the compact A22^{-1}, X are written and B's trailing block
 // holds A11 - A12 X. Blocks up to kSmallSweepN are eliminated whole in shared
 // memory; larger ones by 64-wide pivot blocks with batched GEMM updates.
 // `timed(kernel class, flops, bytes, launch, launches)` wraps every launch.
+// Arithmetic of the products of an elimination. schur: S = A11 - A12 X in FP64
+// (-1), split TF32 (0) or from `schur` int8 slices; x: X = A22^{-1} A21 in FP64
+// (0) or from `x` int8 slices. The Gauss-Jordan updates of A22^{-1} are rank-128
+// products, bound by the traffic of their target rather than by arithmetic, and
+// stay FP64.
+struct ElimArith {
+  int schur = -1;
+  int x = 0;
+};
+
 template <class Timed>
 void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t stream,
-                int* d_status, Timed&& timed, bool mixed = false, bool sym = false,
+                int* d_status, Timed&& timed, ElimArith ar = {}, bool sym = false,
                 Arena* scratch = nullptr) {
   // large per-call scratch from the caller's arena when it has one (no pool
   // traffic), else from the stream-ordered pool
@@ -578,10 +670,9 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
   if (large.empty()) return;
   // Large blocks (include/Schur.hpp:72-100 in the reference's order):
   //   1. A22^{-1} in place by a blocked Gauss-Jordan sweep over the r x r block
-  //      only (FP64 in both precisions: the diagonal-block factorization);
+  //      only (FP64 in every arithmetic: the diagonal-block factorization);
   //   2. X = A22^{-1} A21, one product with k = r, written to the compact X;
   //   3. S = A11 - A12 X, one product with k = r, in place in the trailing block.
-  // Product 3 goes to the split-TF32 tensor-core kernel in mixed precision.
   const int nl = (int)large.size();
   SweepDesc* dd = tmp.add(upload(large, stream));
   double* dinv = big((size_t)nl * kSweepNB * kSweepNB);
@@ -841,10 +932,13 @@ void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_
     y.lower = sym ? 1 : 0;  // S is symmetric: the tiles above the diagonal are mirrored
     gs.push_back(y);
   }
-  // X stays FP64: it comes from the explicit inverse, whose entries exceed X's by
-  // about cond(A22), so a TF32-level product would lose that factor in X.
-  gemm_batch(gx, tmp, stream, HIF_KCLASS_GEMM, timed);
-  if (mixed) gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM_MIXED, timed, 128, d_status);
+  // X comes from the explicit inverse, whose entries exceed X's by about
+  // cond(A22): a TF32-level product would lose that factor in X, so it is FP64
+  // or from enough int8 slices to be close to it.
+  if (ar.x > 0) gemm_batch_int8(gx, tmp, stream, timed, ar.x, d_status);
+  else gemm_batch(gx, tmp, stream, HIF_KCLASS_GEMM, timed);
+  if (ar.schur > 0) gemm_batch_int8(gs, tmp, stream, timed, ar.schur, d_status);
+  else if (ar.schur == 0) gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM_MIXED, timed, 128, d_status);
   else gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM, timed, sym ? 128 : 0);
   if (sym) {
     std::vector<TCopyDesc> tm;
@@ -1275,9 +1369,14 @@ class Engine {
   // descs[b].B holds [A22 A21; A12 A11] (ld n); on return the compact
   // A22^{-1}, X are written and B's trailing block holds A11 - A12 X.
   void run_sweep(const std::vector<SweepDesc>& descs, BufList& tmp) {
+    ElimArith ar;
+    if (precision == HIF_PRECISION_MIXED) {
+      ar.schur = schur_slices;
+      ar.x = x_slices;
+    }
     sweep_blocks(descs, tmp, stream, d_status,
                  [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); },
-                 precision == HIF_PRECISION_MIXED, symmetric, cur_work);
+                 ar, symmetric, cur_work);
   }
 
   void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
@@ -2370,6 +2469,9 @@ class Engine {
   PinnedStage stage;  // host staging of this handle's factorization uploads
   GemmTuner tuner;
   bool autotune = false;
+  // HIF_PRECISION_MIXED: int8 slices of the Schur products (0: split TF32) and
+  // of the X products (0: FP64)
+  int schur_slices = 5, x_slices = 7;
   struct StageScope {
     PinnedStage* prev;
     Arena* prev_scratch;
@@ -3094,6 +3196,14 @@ int hif_set_option(hif_handle h, int option, long long value) {
     case HIF_OPT_AUTOTUNE:
       h->e->autotune = value != 0;
       return HIF_OK;
+    case HIF_OPT_SCHUR_SLICES:
+      if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
+      h->e->schur_slices = (int)value;
+      return HIF_OK;
+    case HIF_OPT_X_SLICES:
+      if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
+      h->e->x_slices = (int)value;
+      return HIF_OK;
     case HIF_OPT_ID_GROUP_MIN_N:
       if (value < 2) return HIF_ERR_ARG;
       h->e->kGroupMinN = (int)value;
@@ -3237,6 +3347,39 @@ int hif_gemm_mixed_device(int transA, int transB, int m, int n, int k, double al
     g.beta = beta;
     hif::gemm_batch(std::vector<hif::GemmDesc>{g}, c.bufs, c.stream, HIF_KCLASS_GEMM_MIXED,
                     [&](int, double, double, auto&& f, int = 1) { f(); }, 128, c.d_status);
+    if (c.status() & hif::kStatusTimeout)
+      throw hif::Error{HIF_ERR_CUDA, "tensor-core pipeline wait timed out"};
+  });
+}
+
+int hif_gemm_int8_device(int transA, int transB, int m, int n, int k, double alpha,
+                         const double* dA, long long lda, const double* dB, long long ldb,
+                         double beta, double* dC, long long ldc, int slices) {
+  if (m < 0 || n < 0 || k < 0 || slices < 2 || slices > hif::kOzMaxS ||
+      (m && n && (!dC || ldc < m)) ||
+      (m && n && k && (!dA || !dB || lda < (transA ? k : m) || ldb < (transB ? n : k))))
+    return HIF_ERR_ARG;
+  if (int e = check_device()) return e;
+  return guarded([&] {
+    if (m == 0 || n == 0) return;
+    FreeCtx c;
+    hif::GemmDesc g{};
+    g.C = dC;
+    g.A = dA;
+    g.B = dB;
+    g.ldc = ldc;
+    g.lda = lda;
+    g.ldb = ldb;
+    g.m = m;
+    g.n = n;
+    g.k = k;
+    g.transA = transA ? 1 : 0;
+    g.transB = transB ? 1 : 0;
+    g.alpha = alpha;
+    g.beta = beta;
+    hif::gemm_batch_int8(std::vector<hif::GemmDesc>{g}, c.bufs, c.stream,
+                         [&](int, double, double, auto&& f, int = 1) { f(); }, slices,
+                         c.d_status);
     if (c.status() & hif::kStatusTimeout)
       throw hif::Error{HIF_ERR_CUDA, "tensor-core pipeline wait timed out"};
   });

@@ -808,6 +808,342 @@ void launch_gemm_tc(const TcGemm* d_desc, const int* d_tile_off, int nd, int tot
 }
 
 // ===========================================================================
+// FP64 products on the int8 tensor cores (Ozaki scheme).
+//
+// C = op(A) op(B) is computed from exact integer pieces of the operands.
+// Every operand row (row i of op(A), column j of op(B)) is scaled by a power
+// of two into (-1, 1) and cut into S signed 7-bit slices by truncation
+// (v <- 128 v; q = trunc(v); v <- v - q, exact in FP64):
+//   x_ik = 2^{e_i} sum_{s<S} q_s(i, k) 2^{-7(s+1)} + r_ik,  |r_ik| < 2^{e_i - 7S}.
+// Then
+//   C_ij = 2^{e_i + f_j - 14} sum_{d<S} 2^{-7d} P_d(i, j),  P_d = sum_{s+t=d} Q_s R_t^T,
+// the slice pairs with s + t >= S being dropped (they weigh less than the
+// representation error). |P_d| <= (d + 1) k 127^2 < 2^31 for k <= kOzMaxK, so
+// each diagonal sum is exact in int32 and accumulates over the whole k range
+// in its own tensor-memory accumulator (tcgen05.mma kind::i8, M = 128,
+// N = BN, K = 32); the epilogue reads each once, sums them in FP64 (Horner in
+// 2^-7) and scales by 2^{e_i + f_j - 14}. Integer accumulation makes the
+// result independent of the order of the products. The error is of order
+// k 2^{-7S} max_k |a_ik| max_k |b_kj| (an FP64 product's scales with
+// u sum_k |a_ik| |b_kj|).
+// A converted tile holds S slices of 128 rows x 64 bytes, each in the K-major
+// canonical layout without swizzle: 8-row x 16-byte core matrices of 128 B,
+// K-adjacent ones 128 B apart (LBO), 8-row groups 512 B apart (SBO), so rows
+// 64..127 of a slice are its second 4 KB and a 64-row B tile is a contiguous
+// half of each slice.
+// Roles as in k_gemm_tc: one thread of warp 0 streams the A and B tiles of
+// every 64-k step into a ring of stages (cp.async.bulk, completion counted in
+// bytes on the stage's mbarrier); one thread of warp 1 issues the
+// S (S + 1) / 2 slice products of each 32-k half and releases the stage with
+// tcgen05.commit; warps 4-7 wait for the last products and write C. Waits are
+// bounded as in k_gemm_tc.
+// ===========================================================================
+__global__ void __launch_bounds__(256) k_oz_exp(const OzOperand* __restrict__ ops,
+                                                const int* __restrict__ tile_off, int nops) {
+  const int oi = find_desc(tile_off, nops, blockIdx.x);
+  const OzOperand o = ops[oi];
+  const int local = blockIdx.x - tile_off[oi];
+  const int kt_n = (o.kdim + kOzK - 1) / kOzK;
+  const int rt = local / kt_n, kt = local % kt_n;
+  const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
+  const int gi = rt * 128 + row;
+  if (gi >= o.rows) return;
+  const int k0 = kt * kOzK + 32 * half;
+  double m = 0.0;
+#pragma unroll 8
+  for (int e = 0; e < 32; ++e) {
+    const int gk = k0 + e;
+    if (gk < o.kdim) {
+      const double x = o.trans ? o.X[gk + (long long)gi * o.ld] : o.X[gi + (long long)gk * o.ld];
+      m = fmax(m, fabs(x));
+    }
+  }
+  if (m > 0.0) {
+    int ex;
+    frexp(m, &ex);  // m < 2^ex
+    atomicMax(&o.rexp[gi], ex);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_oz_slice(const OzOperand* __restrict__ ops,
+                                                  const int* __restrict__ tile_off, int nops,
+                                                  int S) {
+  const int oi = find_desc(tile_off, nops, blockIdx.x);
+  const OzOperand o = ops[oi];
+  const int local = blockIdx.x - tile_off[oi];
+  const int kt_n = (o.kdim + kOzK - 1) / kOzK;
+  const int rt = local / kt_n, kt = local % kt_n;
+  const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
+  const int gi = rt * 128 + row;
+  // rows without a nonzero keep the cleared exponent; their slices are zero
+  const int ex = gi < o.rows ? max(o.rexp[gi], -4096) : 0;
+  signed char* dst = o.out + (size_t)local * S * kOzPart;
+#pragma unroll 1
+  for (int c = 0; c < 2; ++c) {
+    const int kc = 2 * half + c;  // 16-byte chunk of the row's 64 bytes
+    unsigned w[kOzMaxS][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+      for (int s = 0; s < kOzMaxS; ++s) w[s][q] = 0u;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int gk = kt * kOzK + 16 * kc + 4 * q + b;
+        const double x = (gi < o.rows && gk < o.kdim)
+                             ? (o.trans ? o.X[gk + (long long)gi * o.ld]
+                                        : o.X[gi + (long long)gk * o.ld])
+                             : 0.0;
+        double v = ldexp(x, -ex);  // |v| < 1
+#pragma unroll
+        for (int s = 0; s < kOzMaxS; ++s) {
+          if (s < S) {
+            v *= 128.0;
+            const double t = trunc(v);
+            v -= t;
+            w[s][q] |= ((unsigned)(int)t & 0xFFu) << (8 * b);
+          }
+        }
+      }
+    }
+    const int off = ((row >> 3) * 4 + kc) * 128 + (row & 7) * 16;
+#pragma unroll
+    for (int s = 0; s < kOzMaxS; ++s)
+      if (s < S)
+        *reinterpret_cast<uint4*>(dst + (size_t)s * kOzPart + off) =
+            make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+  }
+}
+
+void launch_oz_convert(const OzOperand* d_ops, const int* d_tile_off, int nops, int total_tiles,
+                       int slices, int* d_rexp, long long n_rexp, cudaStream_t s) {
+  if (total_tiles <= 0) return;
+  // 0x80808080: below every exponent a double can have
+  cudaMemsetAsync(d_rexp, 0x80, (size_t)n_rexp * sizeof(int), s);
+  k_oz_exp<<<total_tiles, 256, 0, s>>>(d_ops, d_tile_off, nops);
+  k_oz_slice<<<total_tiles, 256, 0, s>>>(d_ops, d_tile_off, nops, slices);
+}
+
+// Shared-memory matrix descriptor: K-major, no swizzle, LBO 128 B, SBO 512 B.
+__device__ __forceinline__ unsigned long long oz_desc(unsigned addr) {
+  unsigned long long d = (unsigned long long)((addr >> 4) & 0x3FFF);
+  d |= (unsigned long long)(128 >> 4) << 16;
+  d |= (unsigned long long)(512 >> 4) << 32;
+  d |= 1ull << 46;
+  return d;
+}
+
+template <int S, int BN>
+struct OzCfg {
+  static constexpr int kA = S * kOzPart;   // A bytes of one stage
+  static constexpr int kB = S * BN * kOzK;  // B bytes of one stage
+  static constexpr int kStage = kA + kB;
+  static constexpr int kStages = (200 * 1024) / kStage > 4 ? 4 : (200 * 1024) / kStage;
+  static constexpr int kSmem = kStages * kStage + 256;
+  static constexpr int kCols = S * BN <= 256 ? 256 : 512;  // tensor-memory columns
+  // Instruction descriptor, kind::i8: D S32 (bits 4-5 = 2), A and B signed
+  // 8-bit (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at 24.
+  static constexpr unsigned kIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
+                                     ((unsigned)(BN >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
+  static_assert(S * BN <= 512, "diagonal accumulators exceed tensor memory");
+  static_assert(kStages >= 2, "stage ring");
+};
+
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, int bytes, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+template <int S, int BN>
+__global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ descs,
+                                                    const int* __restrict__ tile_off, int nd,
+                                                    int* __restrict__ status) {
+  using Cfg = OzCfg<S, BN>;
+  constexpr int NS = Cfg::kStages;
+  extern __shared__ __align__(1024) unsigned char oz_smem[];
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(oz_smem + NS * Cfg::kStage);
+  unsigned long long* full = bars;        // [NS]
+  unsigned long long* empty = bars + NS;  // [NS]
+  unsigned long long* done = bars + 2 * NS;
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(done + 1);
+  volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int di = find_desc(tile_off, nd, blockIdx.x);
+  const OzGemm g = descs[di];
+  const int local = blockIdx.x - tile_off[di];
+  const int tiles_m = (g.m + 127) / 128;
+  const int mt = local % tiles_m, nt = local / tiles_m;
+  const int m0 = mt * 128, n0 = nt * BN;
+  if (g.lower && n0 >= m0 + 128) return;  // whole CTA, before any barrier or allocation
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(Cfg::kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int q = 0; q < NS; ++q) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[q])) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(done)) : "memory");
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const unsigned tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // producer: the S slices of the A tile, then those of the B tile
+    const int bt = n0 / 128, bhalf = (n0 / 64) & 1;
+    for (int i = 0; i < g.kt_cnt; ++i) {
+      const int kt = g.kt0 + i, s = i % NS;
+      if (i >= NS && !mbar_wait(smem_u32(&empty[s]), (unsigned)((i / NS - 1) & 1), abort)) break;
+      const unsigned fb = smem_u32(&full[s]);
+      const unsigned dst = smem_u32(oz_smem + s * Cfg::kStage);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                   "r"(Cfg::kStage)
+                   : "memory");
+      bulk_g2s(dst, g.A + ((size_t)mt * g.kt_total + kt) * S * kOzPart, Cfg::kA, fb);
+      const signed char* b = g.B + ((size_t)bt * g.kt_total + kt) * S * kOzPart;
+      if (BN == 128) {
+        bulk_g2s(dst + Cfg::kA, b, Cfg::kB, fb);
+      } else {
+#pragma unroll
+        for (int q = 0; q < S; ++q)
+          bulk_g2s(dst + Cfg::kA + q * BN * kOzK, b + (size_t)q * kOzPart + bhalf * BN * kOzK,
+                   BN * kOzK, fb);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // tensor-core issue: slice pair (p, q) adds into the accumulator of diagonal p + q
+    for (int i = 0; i < g.kt_cnt; ++i) {
+      const int s = i % NS;
+      if (!mbar_wait(smem_u32(&full[s]), (unsigned)((i / NS) & 1), abort)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned base = smem_u32(oz_smem + s * Cfg::kStage);
+#pragma unroll
+      for (int j = 0; j < kOzK / 32; ++j) {
+#pragma unroll
+        for (int p = 0; p < S; ++p) {
+          const unsigned long long da = oz_desc(base + p * kOzPart + 256 * j);
+#pragma unroll
+          for (int q = 0; p + q < S; ++q) {
+            const unsigned long long db = oz_desc(base + Cfg::kA + q * BN * kOzK + 256 * j);
+            const unsigned acc = (i > 0 || j > 0 || p > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred r;\n\t"
+                "setp.ne.b32 r, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, r;\n\t}\n" ::"r"(
+                    tmem + (unsigned)((p + q) * BN)),
+                "l"(da), "l"(db), "r"(Cfg::kIdesc), "r"(acc)
+                : "memory");
+          }
+        }
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(&empty[s]))
+          : "memory");
+    }
+    if (g.kt_cnt > 0)
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(done))
+          : "memory");
+  } else if (warp >= 4) {
+    // epilogue: C = alpha 2^{e_i + f_j - 14} sum_d 2^{-7d} P_d + beta C
+    const int q4 = warp - 4;
+    const int gm = m0 + 32 * q4 + lane;
+    const unsigned lanes = (unsigned)(32 * q4) << 16;
+    // k = 0: no products, nothing to wait for (C = beta C)
+    const bool ok = g.kt_cnt == 0 || (mbar_wait(smem_u32(done), 0u, abort) && !*abort);
+    if (ok) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int ea = gm < g.m ? max(g.ea[gm], -4096) : 0;
+#pragma unroll 1
+      for (int cc = 0; cc < BN / 16; ++cc) {
+        double h[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) h[e] = 0.0;
+        if (g.kt_cnt > 0) {
+#pragma unroll 1
+          for (int d = S - 1; d >= 0; --d) {
+            unsigned v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+                "%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + lanes + (unsigned)(d * BN + 16 * cc))
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 16; ++e) h[e] = fma(h[e], 0.0078125, (double)(int)v[e]);
+          }
+        }
+        if (gm < g.m) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int gn = n0 + 16 * cc + e;
+            if (gn < g.n) {
+              double* cp = g.C + gm + (long long)gn * g.ldc;
+              const double val = g.alpha * ldexp(h[e], ea + max(g.eb[gn], -4096) - 14);
+              *cp = (g.beta == 0.0) ? val : fma(g.beta, *cp, val);
+            }
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (tid == 0 && *abort) atomicOr(status, kStatusTimeout);
+  if (warp == 2) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(Cfg::kCols)
+                 : "memory");
+  }
+}
+
+int oz_tile_n(int slices) { return slices <= 4 ? 128 : 64; }
+
+template <int S, int BN>
+static void launch_gemm_oz_t(const OzGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                             int* d_status, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_gemm_oz<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         OzCfg<S, BN>::kSmem);
+    attr = true;
+  }
+  k_gemm_oz<S, BN><<<total_tiles, 256, OzCfg<S, BN>::kSmem, s>>>(d_desc, d_tile_off, nd, d_status);
+}
+
+void launch_gemm_oz(const OzGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                    int slices, int* d_status, cudaStream_t s) {
+  if (total_tiles <= 0) return;
+  switch (slices) {
+    case 2: launch_gemm_oz_t<2, 128>(d_desc, d_tile_off, nd, total_tiles, d_status, s); break;
+    case 3: launch_gemm_oz_t<3, 128>(d_desc, d_tile_off, nd, total_tiles, d_status, s); break;
+    case 4: launch_gemm_oz_t<4, 128>(d_desc, d_tile_off, nd, total_tiles, d_status, s); break;
+    case 5: launch_gemm_oz_t<5, 64>(d_desc, d_tile_off, nd, total_tiles, d_status, s); break;
+    case 6: launch_gemm_oz_t<6, 64>(d_desc, d_tile_off, nd, total_tiles, d_status, s); break;
+    case 7: launch_gemm_oz_t<7, 64>(d_desc, d_tile_off, nd, total_tiles, d_status, s); break;
+    case 8: launch_gemm_oz_t<8, 64>(d_desc, d_tile_off, nd, total_tiles, d_status, s); break;
+    default: break;
+  }
+}
+
+// ===========================================================================
 // Gauss-Jordan sweep. For B = [A22 A21; A12 A11] (red first), eliminating
 // pivots 0..r-1 in place gives [A22^{-1} X; * A11 - A12 X] with
 // X = A22^{-1} A21: the three outputs of the reference's Schur().

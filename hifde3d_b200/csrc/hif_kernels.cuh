@@ -236,11 +236,6 @@ struct SplitKDesc {
 };
 void launch_splitk_reduce(const SplitKDesc* d_desc, int nd, cudaStream_t s);
 
-// Mixed-precision variant of launch_dgemm for Schur-complement updates: the
-// FP64 operands are rounded to FP32 and split into two TF32 parts each
-// (x = hi + lo); hi*hi + hi*lo + lo*hi run on the tensor cores (mma.sync
-// m16n8k8, FP32 accumulation), then C (FP64) = beta C + alpha acc.
-// 128 x 128 x 16 tiles; tile offsets from dgemm_tiles(m, n, 128).
 // Split-TF32 tensor-core GEMM (tcgen05, FP32 accumulation in tensor memory).
 // Operands are first converted to TF32 (hi, lo) pairs in 128 x 32 tiles of
 // kTcTileBytes each: element (i, kk) of an operand is op(X)[i, kk] for A and
@@ -271,6 +266,48 @@ struct TcGemm {
 };
 void launch_gemm_tc(const TcGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
                     int* d_status, cudaStream_t s);
+
+// FP64 products on the int8 tensor cores (Ozaki scheme). Every operand row
+// (a row of op(A), a column of op(B)) gets a power-of-two exponent e (its
+// largest magnitude is below 2^e) and S signed 7-bit slices q_s with
+// x = 2^e sum_s q_s 2^{-7(s+1)} + r, |r| < 2^{e - 7S}. Converted operands are
+// tiles of 128 rows x 64 values of k: tile (rt, kt) holds S slices of
+// kOzPart bytes at out + ((rt * ceil(kdim / 64) + kt) * S + s) * kOzPart.
+constexpr int kOzK = 64, kOzPart = 128 * kOzK, kOzMaxS = 8;
+// Largest k of one product: every diagonal sum of slice products stays exact in
+// int32 ((d + 1) k 127^2 < 2^31 for d < kOzMaxS).
+constexpr int kOzMaxK = 16384;
+struct OzOperand {
+  const double* X;
+  long long ld;
+  int trans;  // 0: element (i, kk) at X[i + kk ld]; 1: at X[kk + i ld]
+  int rows, kdim;
+  signed char* out;
+  int* rexp;  // per-row exponent, ceil(rows / 128) * 128 entries
+};
+// d_tile_off: prefix over operands of ceil(rows / 128) * ceil(kdim / 64).
+// Every rexp lies in [d_rexp, d_rexp + n_rexp): it is cleared, then the
+// exponents are taken (one pass over the operands), then the slices (a second).
+void launch_oz_convert(const OzOperand* d_ops, const int* d_tile_off, int nops, int total_tiles,
+                       int slices, int* d_rexp, long long n_rexp, cudaStream_t s);
+struct OzGemm {
+  const signed char* A;  // converted op(A): rows m
+  const signed char* B;  // converted op(B)^T: rows n
+  const int* ea;
+  const int* eb;
+  double* C;
+  long long ldc;
+  int m, n;
+  int kt_total;     // k tiles of the converted operands
+  int kt0, kt_cnt;  // k tiles of this product (kt_cnt * kOzK <= kOzMaxK)
+  double alpha, beta;
+  int lower;  // skip the tiles entirely above the diagonal
+};
+// C = alpha op(A) op(B) + beta C from converted operands with `slices` slices
+// (2..kOzMaxS); d_tile_off counts tiles of 128 x oz_tile_n(slices) columns.
+int oz_tile_n(int slices);
+void launch_gemm_oz(const OzGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
+                    int slices, int* d_status, cudaStream_t s);
 
 // In-shared-memory Gauss-Jordan sweep of the first r pivots (n <= kSmallSweepN).
 constexpr int kSmallSweepN = 160;

@@ -151,10 +151,14 @@ enum hif_option {
   HIF_OPT_PROFILE = 4,       /* time every launch with CUDA events (resets the counters) */
   HIF_OPT_ID_GROUP_MIN_N = 5, /* faces with at least this many columns get a CTA group (default 512) */
   HIF_OPT_PRECISION = 6,      /* HIF_PRECISION_FP64 (default) or HIF_PRECISION_MIXED */
-  HIF_OPT_AUTOTUNE = 7        /* 1: tune the tile shape of the batched FP64 products online
+  HIF_OPT_AUTOTUNE = 7,       /* 1: tune the tile shape of the batched FP64 products online
                                  (each batch signature tries both tiles on the first
                                  factorizations, then keeps the faster); results may then
                                  differ in the last bits between those factorizations */
+  HIF_OPT_SCHUR_SLICES = 8,   /* MIXED: int8 slices (2..8) of the Schur-complement products
+                                 S = A11 - A12 X (default 5); 0: split TF32 */
+  HIF_OPT_X_SLICES = 9        /* MIXED: int8 slices (2..8) of X = A22^{-1} A21 (default 7);
+                                 0: FP64 */
 };
 /* Arithmetic of the factorization. MIXED: the Schur complements S = A11 - A12 X of the
  * eliminations run on the tcgen05 tensor cores as split-TF32 products with FP64
@@ -199,7 +203,9 @@ enum hif_kernel_class {
   HIF_KCLASS_VECTOR = 7,      /* reductions / vector updates of the apply */
   HIF_KCLASS_QR = 8,          /* blocked Householder row compression of face blocks */
   HIF_KCLASS_GEMM_MIXED = 9,  /* split-TF32 tensor-core Schur-complement updates */
-  HIF_KCLASS_COUNT = 10
+  HIF_KCLASS_GEMM_INT8 = 10,  /* FP64 products from int8 slices on the tensor cores (flops:
+                                 the int8 operations of the slice products) */
+  HIF_KCLASS_COUNT = 11
 };
 /* Accumulated launches, milliseconds (CUDA events on the handle's stream), algorithmic
  * flops and bytes of one kernel class since HIF_OPT_PROFILE was last set. */
@@ -230,6 +236,19 @@ int hif_trim_device_pool(void);
 int hif_gemm_mixed_device(int transA, int transB, int m, int n, int k, double alpha,
                           const double* dA, long long lda, const double* dB, long long ldb,
                           double beta, double* dC, long long ldc);
+
+/* FP64 GEMM on device pointers from exact int8 products on the tcgen05 tensor cores
+ * (Ozaki scheme): every row of op(A) and column of op(B) is scaled by a power of two
+ * and cut into `slices` (2..8) signed 7-bit pieces; the slice products with
+ * s + t < slices are accumulated exactly in int32 and summed in FP64. The error is
+ * of order k 2^(-7 slices) max|row of op(A)| max|column of op(B)|; the result does
+ * not depend on the order of the products. C = alpha op(A) op(B) + beta C,
+ * column-major. No reference counterpart (the reference's products are
+ * hmat_tools::Multiply dgemm calls, include/Schur.hpp:97-99). Runs on the calling
+ * thread's default per-thread stream and returns after completion. */
+int hif_gemm_int8_device(int transA, int transB, int m, int n, int k, double alpha,
+                         const double* dA, long long lda, const double* dB, long long ldb,
+                         double beta, double* dC, long long ldc, int slices);
 
 /* ---- Serving: many operators resident on one GPU ------------------------------
  * No reference counterpart (the reference factors one operator per process,
