@@ -43,6 +43,35 @@ def dofs(n: int) -> int:
 
 
 # ---------------------------------------------------------------------------
+# replicas (N > 1): every rank factors and solves its own operator
+# ---------------------------------------------------------------------------
+def replica_seeds(rank: int):
+    """(coefficient-field seed, right-hand-side seed) of a rank's operator: the
+    replicas factor different operators of the same size."""
+    return 2 + rank, rank
+
+
+def replica_times(ms_step: float, e2e_s: float, world: int, device=None):
+    """Max over ranks of the device time per step and of the end-to-end step
+    time: the job's step ends when its slowest replica's does. Every rank calls
+    this once, with the same collective on every path."""
+    if world <= 1:
+        return ms_step, e2e_s
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms_step, e2e_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0]), float(t[1])
+
+
+def job_value(world: int, ms_step: float) -> float:
+    """Whole-job steps per second: `world` replicas each finish one step per
+    (max over ranks) `ms_step` milliseconds."""
+    return world * 1e3 / ms_step
+
+
+# ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
@@ -337,9 +366,10 @@ def run_ours(args, rank: int, world: int):
     eps = args.eps
 
     # synthetic operator (per-rank seed for replicas) and right-hand side
-    ax, ay, az = synth.face_coefficients_grf(N, 2 + rank, 1.0 / 16, 1.0)
+    seed_op, seed_rhs = replica_seeds(rank)
+    ax, ay, az = synth.face_coefficients_grf(N, seed_op, 1.0 / 16, 1.0)
     V = np.zeros((NC + 1,) * 3)
-    b = synth.dof_vector(N, rank)
+    b = synth.dof_vector(N, seed_rhs)
     host = [np.ascontiguousarray(x.ravel(order="F")) for x in (ax, ay, az, V)]
     dcoef = [torch.from_numpy(x).to(dev) for x in host]
     db = torch.from_numpy(b).to(dev)
@@ -444,10 +474,7 @@ def run_ours(args, rank: int, world: int):
 
     # max over ranks
     ms_step = ms_total / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step, e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step, e2e_s = float(t[0]), float(t[1])
+    ms_step, e2e_s = replica_times(ms_step, e2e_s, world, dev)
     if rank != 0:
         f.close()
         return
@@ -512,7 +539,7 @@ def run_ours(args, rank: int, world: int):
                           f"({dofs(32)} DOFs) on 1 core took {s:.2f} s; scaled to n={n} "
                           "linearly in DOFs (a lower bound on the reference's time)")}
 
-    value = world * 1e3 / ms_step
+    value = job_value(world, ms_step)
     line = {
         "metric": METRIC,
         "value": value,
