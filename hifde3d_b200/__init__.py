@@ -27,7 +27,7 @@ _LIB_PATH = os.path.join(_HERE, "libhif_b200.so")
 _lib = None
 
 HIF_OK, HIF_ERR_ARG, HIF_ERR_CUDA, HIF_ERR_NOMEM, HIF_ERR_SINGULAR = 0, 1, 2, 3, 4
-HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET = 5, 6, 7
+HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET, HIF_ERR_IO = 5, 6, 7, 8
 PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
 OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE, OPT_ID_GROUP_MIN_N = 1, 2, 3, 4, 5
 OPT_PRECISION, OPT_AUTOTUNE, OPT_SCHUR_SLICES, OPT_X_SLICES = 6, 7, 8, 9
@@ -58,12 +58,16 @@ _SIGNATURES = {
     "hif_setup_stencil_faces_device": [_p, _i, _d, _p, _p, _p, _p],
     "hif_initialize": [_p],
     "hif_factor": [_p],
+    "hif_save_factor": [_p, ctypes.c_char_p],
+    "hif_load_factor": [_p, ctypes.c_char_p],
     "hif_apply": [_p, _dp, _i, _ll, _i],
     "hif_apply_device": [_p, _p, _i, _ll, _i],
     "hif_spmv": [_p, _dp, _dp, _i, _ll, _i],
     "hif_spmv_device": [_p, _p, _p, _i, _ll, _i],
     "hif_solve_pcg": [_p, _dp, _dp, _i, _ll, _d, _i, _ip, _dp],
     "hif_solve_pcg_device": [_p, _p, _p, _i, _ll, _d, _i, _ip, _dp],
+    "hif_solve_gmres": [_p, _dp, _dp, _i, _ll, _d, _i, _i, _ip, _dp],
+    "hif_solve_gmres_device": [_p, _p, _p, _i, _ll, _d, _i, _i, _ip, _dp],
     "hif_num_levels": [_p, _ip],
     "hif_num_blocks": [_p, _i, _i, _ip],
     "hif_block_info": [_p, _i, _i, _i, _ip, _ip, _ip, _ip],
@@ -189,6 +193,16 @@ class HIFFactor:
     def Factor(self):
         _check(lib().hif_factor(self._h))
 
+    def save(self, path: str):
+        """Write the factorization (and the operator, when set) to `path`
+        (hif_save_factor)."""
+        _check(lib().hif_save_factor(self._h, os.fsencode(path)))
+
+    def load(self, path: str):
+        """Replace this handle's factorization by the one saved in `path`; the
+        handle must have the saved N, P, epsilon and partition (hif_load_factor)."""
+        _check(lib().hif_load_factor(self._h, os.fsencode(path)))
+
     def set_option(self, option: int, value: int):
         _check(lib().hif_set_option(self._h, int(option), int(value)))
 
@@ -248,6 +262,32 @@ class HIFFactor:
         _check(lib().hif_solve_pcg(self._h, _dptr(b), _dptr(x), nrhs, n, tol, maxit,
                                    _iptr(it), _dptr(rr)))
         return x, it, rr
+
+    def solve_gmres(self, b: np.ndarray, tol: float = 1e-10, maxit: int = 200,
+                    restart: int = 30):
+        """Restarted GMRES on A x = b, right-preconditioned by the inverse apply (the
+        solver for the non-symmetric node operator). Returns (x, iters, relres); for
+        b of shape (NC^3, nrhs) iters and relres are per right-hand side."""
+        b = np.asarray(b, dtype=np.float64)
+        single = b.ndim == 1
+        b2 = np.asfortranarray(b.reshape(-1, 1) if single else b)
+        n, nrhs = b2.shape
+        x = np.zeros((n, nrhs), order="F")
+        it = np.zeros(nrhs, np.int32)
+        rr = np.zeros(nrhs)
+        _check(lib().hif_solve_gmres(self._h, _dptr(b2), _dptr(x), nrhs, n, tol, maxit,
+                                     int(restart), _iptr(it), _dptr(rr)))
+        if single:
+            return x[:, 0].copy(), int(it[0]), float(rr[0])
+        return x, it, rr
+
+    def solve_gmres_device(self, db: int, dx: int, nrhs: int, ld: int, tol: float, maxit: int,
+                           restart: int = 30):
+        it = np.zeros(nrhs, np.int32)
+        rr = np.zeros(nrhs)
+        _check(lib().hif_solve_gmres_device(self._h, _p(db), _p(dx), nrhs, ld, tol, maxit,
+                                            int(restart), _iptr(it), _dptr(rr)))
+        return it, rr
 
     def solve_pcg_device(self, db: int, dx: int, nrhs: int, ld: int, tol: float, maxit: int):
         it = np.zeros(nrhs, np.int32)

@@ -13,7 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhif_b200.so")
 SOURCES = ["hif_kernels.cu", "hif_engine.cpp", "hif_noalloc.cu"]
-HEADERS = ["hif_kernels.cuh", "hif_partition.hpp", os.path.join("..", "..", "include", "hif_b200.h")]
+HEADERS = ["hif_kernels.cuh", "hif_partition.hpp", "hif_server.inl", "hif_factor_io.inl",
+           "hif_gmres.inl",
+           os.path.join("..", "..", "include", "hif_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

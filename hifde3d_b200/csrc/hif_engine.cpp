@@ -25,6 +25,7 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <cstdint>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -992,6 +993,7 @@ class Engine {
   bool keep_schur = false, verbose = false;
   int verbose_mode = 0;
   int precision = HIF_PRECISION_FP64;
+  int factor_precision = HIF_PRECISION_FP64;  // the precision the held factor was made in
   long long budget_mb = 0;
   std::map<int, std::vector<std::vector<int>>> replay;
   double t_total = 0, t_gather = 0, t_elim = 0, t_id = 0, t_host = 0, t_plan = 0;
@@ -2529,6 +2531,7 @@ class Engine {
     int st = 0;
     HIF_CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
     factored = true;
+    factor_precision = precision;
     if (st & kStatusTinyPivot) throw Error{HIF_ERR_SINGULAR, "zero or non-finite pivot"};
     if (st & kStatusTimeout)
       throw Error{HIF_ERR_CUDA, "a bounded device wait timed out (grouped ID barrier or tensor-core "
@@ -2877,6 +2880,9 @@ class Engine {
   }
 };
 
+#include "hif_factor_io.inl"
+#include "hif_gmres.inl"
+
 }  // namespace hif
 
 // ===========================================================================
@@ -3021,6 +3027,16 @@ int hif_factor(hif_handle h) {
   return guarded([&] { h->e->factor(); });
 }
 
+int hif_save_factor(hif_handle h, const char* path) {
+  if (!h || !path || !*path) return HIF_ERR_ARG;
+  return guarded([&] { hif::save_factor(*h->e, path); });
+}
+
+int hif_load_factor(hif_handle h, const char* path) {
+  if (!h || !path || !*path) return HIF_ERR_ARG;
+  return guarded([&] { hif::load_factor(*h->e, path); });
+}
+
 int hif_apply_device(hif_handle h, double* du, int nrhs, long long ldu, int apply_inverse) {
   if (!h || !du) return HIF_ERR_ARG;
   return guarded([&] { h->e->apply_device(du, nrhs, ldu, apply_inverse != 0); });
@@ -3095,6 +3111,39 @@ int hif_solve_pcg(hif_handle h, const double* b, double* x, int nrhs, long long 
       HIF_CK(cudaMemcpyAsync(x + c * ld, dx + c * e.n3, e.n3 * 8, cudaMemcpyDeviceToHost, e.stream));
     hif::dfree(db, e.stream);
     hif::dfree(dx, e.stream);
+    e.sync();
+  });
+}
+
+int hif_solve_gmres_device(hif_handle h, const double* db, double* dx, int nrhs, long long ld,
+                           double tol, int maxit, int restart, int* iters, double* relres) {
+  if (!h || !db || !dx || !iters || !relres || nrhs <= 0 || maxit < 0) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::solve_gmres_device(*h->e, db, dx, nrhs, ld, tol, maxit, restart, iters, relres);
+  });
+}
+
+int hif_solve_gmres(hif_handle h, const double* b, double* x, int nrhs, long long ld, double tol,
+                    int maxit, int restart, int* iters, double* relres) {
+  if (!h || !b || !x || !iters || !relres || nrhs <= 0 || maxit < 0) return HIF_ERR_ARG;
+  return guarded([&] {
+    hif::Engine& e = *h->e;
+    if (ld < e.n3) throw hif::Error{HIF_ERR_ARG, "ld < (N+1)^3"};
+    double* db = hif::dalloc<double>(e.n3 * nrhs, e.stream);
+    double* dx = hif::dalloc<double>(e.n3 * nrhs, e.stream);
+    struct Free {
+      double *a, *b;
+      cudaStream_t s;
+      ~Free() {
+        hif::dfree(a, s);
+        hif::dfree(b, s);
+      }
+    } guard{db, dx, e.stream};
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(db + c * e.n3, b + c * ld, e.n3 * 8, cudaMemcpyHostToDevice, e.stream));
+    hif::solve_gmres_device(e, db, dx, nrhs, e.n3, tol, maxit, restart, iters, relres);
+    for (int c = 0; c < nrhs; ++c)
+      HIF_CK(cudaMemcpyAsync(x + c * ld, dx + c * e.n3, e.n3 * 8, cudaMemcpyDeviceToHost, e.stream));
     e.sync();
   });
 }

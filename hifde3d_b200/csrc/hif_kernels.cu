@@ -3011,4 +3011,84 @@ void launch_pcg_update_p(double* p, const double* z, const double* rz_new,
   k_pcg_p<<<(int)((total + 255) / 256), 256, 0, s>>>(p, z, rz_new, rz_old, n, nrhs, ld);
 }
 
+// ---------------------------------------------------------------------------
+// GMRES vector kernels. A Krylov basis of nb vectors per right-hand side is
+// stored as V[(i * nrhs + c) * n + t] (vector i of column c); coefficient
+// arrays as coef[i * nrhs + c]. Reductions run in a fixed order (per block,
+// then over the kDotBlocks partials), so results are bit-reproducible.
+// ---------------------------------------------------------------------------
+
+// partial dots of w against basis vectors i0 .. i0 + nb - 1 (nb <= kGmresGroup):
+// part[(q * nrhs + c) * gridDim.x + block]
+__global__ void __launch_bounds__(256) k_gmres_dots(const double* __restrict__ V, int i0, int nb,
+                                                    const double* __restrict__ w, long long n,
+                                                    int nrhs, double* __restrict__ part) {
+  const int c = blockIdx.y;
+  const double* wc = w + (long long)c * n;
+  double acc[kGmresGroup];
+#pragma unroll
+  for (int q = 0; q < kGmresGroup; ++q) acc[q] = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const double wv = wc[t];
+#pragma unroll
+    for (int q = 0; q < kGmresGroup; ++q)
+      if (q < nb) acc[q] = fma(V[((long long)(i0 + q) * nrhs + c) * n + t], wv, acc[q]);
+  }
+  __shared__ double sc[40];
+#pragma unroll
+  for (int q = 0; q < kGmresGroup; ++q) {
+    if (q < nb) {  // nb is the same for the whole block: the barriers inside match
+      const double tot = block_sum(acc[q], sc);
+      if (threadIdx.x == 0) part[((long long)q * nrhs + c) * gridDim.x + blockIdx.x] = tot;
+    }
+  }
+}
+
+void launch_gmres_dots(const double* V, int nb, const double* w, long long n, int nrhs,
+                       double* d_partial, double* d_out, cudaStream_t s) {
+  for (int i0 = 0; i0 < nb; i0 += kGmresGroup) {
+    const int g = nb - i0 < kGmresGroup ? nb - i0 : kGmresGroup;
+    k_gmres_dots<<<dim3(kDotBlocks, nrhs), 256, 0, s>>>(V, i0, g, w, n, nrhs, d_partial);
+    k_dot_final<<<g * nrhs, 256, 0, s>>>(d_partial, kDotBlocks, d_out + (long long)i0 * nrhs);
+  }
+}
+
+// w[:, c] += sign * sum_{i < nb} coef[i * nrhs + c] V_i[:, c]
+__global__ void __launch_bounds__(256) k_gmres_axpy(double* __restrict__ w,
+                                                    const double* __restrict__ V, int nb,
+                                                    const double* __restrict__ coef, double sign,
+                                                    long long n, int nrhs) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (t >= n) return;
+  double acc = 0.0;
+  for (int i = 0; i < nb; ++i)
+    acc = fma(coef[(long long)i * nrhs + c], V[((long long)i * nrhs + c) * n + t], acc);
+  w[(long long)c * n + t] = fma(sign, acc, w[(long long)c * n + t]);
+}
+
+void launch_gmres_axpy(double* w, const double* V, int nb, const double* coef, double sign,
+                       long long n, int nrhs, cudaStream_t s) {
+  if (nb <= 0) return;
+  k_gmres_axpy<<<dim3((unsigned)((n + 255) / 256), nrhs), 256, 0, s>>>(w, V, nb, coef, sign, n,
+                                                                       nrhs);
+}
+
+// dst[:, c] = scale[c] * src[:, c]
+__global__ void __launch_bounds__(256) k_gmres_scale(double* __restrict__ dst,
+                                                     const double* __restrict__ src,
+                                                     const double* __restrict__ scale,
+                                                     long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (t >= n) return;
+  dst[(long long)c * n + t] = scale[c] * src[(long long)c * n + t];
+}
+
+void launch_gmres_scale(double* dst, const double* src, const double* scale, long long n, int nrhs,
+                        cudaStream_t s) {
+  k_gmres_scale<<<dim3((unsigned)((n + 255) / 256), nrhs), 256, 0, s>>>(dst, src, scale, n);
+}
+
 }  // namespace hif

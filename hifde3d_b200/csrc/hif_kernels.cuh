@@ -437,4 +437,18 @@ void launch_pcg_update_p(double* p, const double* z, const double* rz_new,
                          const double* rz_old, long long n, int nrhs, long long ld,
                          cudaStream_t s);
 
+// GMRES (basis vector i of rhs c at V + (i * nrhs + c) * n, coefficients at
+// coef[i * nrhs + c]; all deterministic):
+//   out[i * nrhs + c] = <V_i[:, c], w[:, c]> for i < nb (partial: kGmresGroup *
+//   nrhs * kDotBlocks doubles)
+constexpr int kGmresGroup = 16;
+void launch_gmres_dots(const double* V, int nb, const double* w, long long n, int nrhs,
+                       double* d_partial, double* d_out, cudaStream_t s);
+//   w[:, c] += sign * sum_{i < nb} coef[i * nrhs + c] V_i[:, c]
+void launch_gmres_axpy(double* w, const double* V, int nb, const double* coef, double sign,
+                       long long n, int nrhs, cudaStream_t s);
+//   dst[:, c] = scale[c] src[:, c]
+void launch_gmres_scale(double* dst, const double* src, const double* scale, long long n, int nrhs,
+                        cudaStream_t s);
+
 }  // namespace hif

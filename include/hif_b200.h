@@ -33,7 +33,8 @@ enum hif_status {
   HIF_ERR_SINGULAR = 4,   /* zero / non-finite pivot in an elimination */
   HIF_ERR_STATE = 5,      /* call out of order (e.g. Apply before Factor) */
   HIF_ERR_NODEVICE = 6,   /* no CUDA device / kernels not loadable */
-  HIF_ERR_BUDGET = 7      /* would exceed the handle's memory budget */
+  HIF_ERR_BUDGET = 7,     /* would exceed the handle's memory budget */
+  HIF_ERR_IO = 8          /* factor file unreadable, unwritable, truncated or corrupt */
 };
 
 enum hif_partition {
@@ -67,6 +68,23 @@ int hif_initialize(hif_handle h);
 /* HIFFactor::Factor -- src/Factor.cpp:41-63. */
 int hif_factor(hif_handle h);
 
+/* Factor save / load. No counterpart in the reference, whose factor data
+ * (FactorData / IndexData per block, include/data.hpp:11-62,84-110) lives only in
+ * the HIFFactor object. hif_save_factor writes the factorization held by h (after
+ * hif_factor or hif_load_factor) to `path`: every level's index data, the matrices
+ * the apply reads (A22, A22^{-1}, X, W) and, when h has one, the operator, so
+ * that hif_solve_pcg works after a load. The file is written as path + ".tmp"
+ * and renamed when complete. hif_load_factor reads such a file into a handle
+ * created with the same N, P, epsilon and partition (HIF_ERR_ARG otherwise),
+ * replacing any factorization it held; afterwards hif_apply / hif_solve_pcg give
+ * the results of the saved factorization bit for bit. Schur complements kept
+ * with HIF_OPT_KEEP_SCHUR are not saved. A file that is missing, truncated,
+ * corrupt (sizes, offsets or DOF ids out of range, checksum) or written on a
+ * machine of the other byte order returns HIF_ERR_IO and leaves h without a
+ * factorization. Both synchronise the handle's stream. */
+int hif_save_factor(hif_handle h, const char* path);
+int hif_load_factor(hif_handle h, const char* path);
+
 /* HIFFactor::Apply(u, apply_inverse) -- src/Factor.cpp:992-1081, in place. */
 int hif_apply(hif_handle h, double* u, int nrhs, long long ldu, int apply_inverse);
 int hif_apply_device(hif_handle h, double* du, int nrhs, long long ldu, int apply_inverse);
@@ -86,6 +104,19 @@ int hif_solve_pcg(hif_handle h, const double* b, double* x, int nrhs, long long 
                   double tol, int maxit, int* iters, double* relres);
 int hif_solve_pcg_device(hif_handle h, const double* db, double* dx, int nrhs, long long ld,
                          double tol, int maxit, int* iters, double* relres);
+
+/* Restarted GMRES(restart) on A x = b with the factor's inverse apply as right
+ * preconditioner, so the residual it minimises and reports is the true FP64
+ * residual |b - A x| / |b| on the operator. No counterpart in the reference (it has
+ * no iterative solver); this is the solver for its node-coefficient operator
+ * (SetupStencil, include/setup_stencil.hpp:6-76), which is not symmetric for
+ * variable coefficients. x is an output (x0 = 0); restart in 1..64; maxit bounds
+ * the Arnoldi steps (one preconditioner and one operator apply each) per
+ * right-hand side; iters / relres per right-hand side. Bit-reproducible. */
+int hif_solve_gmres(hif_handle h, const double* b, double* x, int nrhs, long long ld,
+                    double tol, int maxit, int restart, int* iters, double* relres);
+int hif_solve_gmres_device(hif_handle h, const double* db, double* dx, int nrhs, long long ld,
+                           double tol, int maxit, int restart, int* iters, double* relres);
 
 /* ---- the reference's free functions on the hot path -----------------------------
  * Schur(matrix, data) -- include/Schur.hpp:72-100: eliminate the redundant DOFs of a

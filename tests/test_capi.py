@@ -68,3 +68,5 @@ def test_bad_arguments_are_rejected():
     assert L.hif_create(7, 4, 1e-6, 9, ctypes.byref(h)) == hb.HIF_ERR_ARG
     assert L.hif_factor(None) == hb.HIF_ERR_ARG
     assert L.hif_apply(None, None, 1, 1, 0) == hb.HIF_ERR_ARG
+    assert L.hif_save_factor(None, b"/tmp/f.hif") == hb.HIF_ERR_ARG
+    assert L.hif_load_factor(None, b"/tmp/f.hif") == hb.HIF_ERR_ARG
