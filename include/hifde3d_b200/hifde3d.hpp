@@ -211,6 +211,42 @@ class HIFFactor<double> {
                  "HIFFactor::Apply");
   }
 
+  // ---- extensions (no counterpart in the reference) ----------------------
+  // Iterative solves with the factor as preconditioner and an FP64 residual on the
+  // operator, x0 = 0: PCG for the symmetric face-coefficient operator, GMRES for
+  // SetupStencil's node operator (not symmetric for variable coefficients).
+  // Return the iteration count; `relres` receives |b - A x| / |b|.
+  int SolvePCG(const Vector<double>& b, Vector<double>& x, double tol = 1e-10,
+               int maxit = 200, double* relres = nullptr) {
+    x.Resize(b.Size());
+    int it = 0;
+    double rr = 0;
+    ThrowOnError(hif_solve_pcg(h_, b.LockedBuffer(), x.Buffer(), 1, b.Size(), tol, maxit, &it,
+                               &rr),
+                 "HIFFactor::SolvePCG");
+    if (relres) *relres = rr;
+    return it;
+  }
+  int SolveGMRES(const Vector<double>& b, Vector<double>& x, double tol = 1e-10,
+                 int maxit = 200, int restart = 30, double* relres = nullptr) {
+    x.Resize(b.Size());
+    int it = 0;
+    double rr = 0;
+    ThrowOnError(hif_solve_gmres(h_, b.LockedBuffer(), x.Buffer(), 1, b.Size(), tol, maxit,
+                                 restart, &it, &rr),
+                 "HIFFactor::SolveGMRES");
+    if (relres) *relres = rr;
+    return it;
+  }
+  // The factorization (and the operator) to / from a file; Load needs a
+  // HIFFactor of the saved N, P and epsilon and replaces what it held.
+  void Save(const std::string& path) {
+    ThrowOnError(hif_save_factor(h_, path.c_str()), "HIFFactor::Save");
+  }
+  void Load(const std::string& path) {
+    ThrowOnError(hif_load_factor(h_, path.c_str()), "HIFFactor::Load");
+  }
+
   void set_N(int) { throw std::logic_error("set_N: recreate the HIFFactor"); }
   int N() { return N_; }
   void set_P(int) { throw std::logic_error("set_P: recreate the HIFFactor"); }
