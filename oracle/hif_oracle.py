@@ -36,6 +36,8 @@ is the only oracle):
   integer division leaves part of the domain uncovered (src/Factor.cpp:51-53).
 * ``setup_stencil_faces``: the symmetric flux form -div(a grad u) + b u with a
   given at cell faces.
+* ``pcg`` and ``gmres``: the iterative solves that use the factor as
+  preconditioner (the reference has none; its driver only reports e_a / e_s).
 
 Parity of this module with the reference itself is pinned by the golden files
 under tests/golden (written by tests/golden/make_golden.py from the reference
@@ -642,3 +644,64 @@ def pcg(op: sp.spmatrix, b: np.ndarray, precond, tol: float = 1e-10, maxit: int 
         p = z + (rz2 / rz) * p
         rz = rz2
     return x, maxit, hist
+
+
+def gmres(op: sp.spmatrix, b: np.ndarray, precond, tol: float = 1e-10, restart: int = 30,
+          maxit: int = 200):
+    """Restarted GMRES(restart) on A x = b with ``precond`` as right preconditioner
+    (the reference has no iterative solver). Same steps as the library's solver:
+    Krylov space of A M^-1 from r0 = b - A x0 (x0 = 0), classical Gram-Schmidt
+    applied twice, Givens rotations on the Hessenberg matrix, a cycle ends when
+    the rotated residual estimate reaches tol (or maxit Arnoldi steps in all),
+    x += M^-1 V y, and convergence is decided on the true residual.
+    Returns (x, Arnoldi steps, true relative residual)."""
+    x = np.zeros_like(b)
+    bn = np.linalg.norm(b)
+    if bn == 0:
+        return x, 0, 0.0
+    r = b.copy()
+    total = 0
+    rel = 1.0
+    while total < maxit:
+        beta = np.linalg.norm(r)
+        if beta == 0:
+            break
+        V = [r / beta]
+        R = np.zeros((restart + 1, restart))
+        cs, sn = np.zeros(restart), np.zeros(restart)
+        g = np.zeros(restart + 1)
+        g[0] = beta
+        k = 0
+        for j in range(restart):
+            w = op @ precond(V[j])
+            h = np.zeros(j + 2)
+            for _ in range(2):
+                c = np.array([v @ w for v in V])
+                w = w - np.asarray(V).T @ c
+                h[:j + 1] += c
+            hn = np.linalg.norm(w)
+            h[j + 1] = hn
+            for i in range(j):
+                t = cs[i] * h[i] + sn[i] * h[i + 1]
+                h[i + 1] = -sn[i] * h[i] + cs[i] * h[i + 1]
+                h[i] = t
+            den = np.hypot(h[j], h[j + 1])
+            cs[j], sn[j] = (h[j] / den, h[j + 1] / den) if den > 0 else (1.0, 0.0)
+            h[j], h[j + 1] = den, 0.0
+            g[j + 1] = -sn[j] * g[j]
+            g[j] = cs[j] * g[j]
+            R[:j + 1, j] = h[:j + 1]
+            total += 1
+            k = j + 1
+            if abs(g[j + 1]) / bn <= tol or total >= maxit or not hn > 0 or den == 0:
+                break
+            V.append(w / hn)
+        y = np.zeros(k)
+        for i in range(k - 1, -1, -1):
+            y[i] = (g[i] - R[i, i + 1:k] @ y[i + 1:k]) / R[i, i] if R[i, i] != 0 else 0.0
+        x = x + precond(np.asarray(V[:k]).T @ y)
+        r = b - op @ x
+        rel = np.linalg.norm(r) / bn
+        if rel <= tol:
+            break
+    return x, total, rel
