@@ -1,4 +1,4 @@
-"""Many right-hand sides at once (BASELINE config 3 style: one batched apply).
+"""Many right-hand sides at once (one batched apply for all of them).
 
 From 16 right-hand sides on, the apply runs every sweep stage as gather / GEMM /
 emit instead of GEMVs over groups of 4 right-hand sides. Each column must match the
