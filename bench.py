@@ -65,6 +65,13 @@ def replica_times(ms_step: float, e2e_s: float, world: int, device=None):
     return float(t[0]), float(t[1])
 
 
+def workload_config(n: int, eps: float, world: int) -> dict:
+    """The `config` object of both arms' JSON lines: the workload they measure."""
+    return {"workload": f"hif factor + pcg(1e-10), n={n} (N={n - 1}, {dofs(n)} DOFs), "
+                        f"face a=exp(GRF ell=1/16 sigma=1), eps={eps}, P=4",
+            "parallelism": f"replicas x{world}"}
+
+
 def job_value(world: int, ms_step: float) -> float:
     """Whole-job steps per second: `world` replicas each finish one step per
     (max over ranks) `ms_step` milliseconds."""
@@ -177,7 +184,10 @@ def run_reference_arm(args, rank: int, world: int):
         "unit": f"factor+solve steps/s at n={args.n}", "n_gpus": world, "steps": steps,
         "warmup": warm, "ms_per_step": 1e3 / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"hif factor+pcg n={args.n} (sampled at n={n_sample})"},
+        "config": {**workload_config(args.n, args.eps, world),
+                   "arithmetic": "FP64 (the reference's CPU build; its node operator with the "
+                                 "same field sampled at nodes, timed on a sample at "
+                                 f"n={n_sample})"},
         "cpu_baseline": {"value": value, "unit": f"factor+solve steps/s at n={args.n}",
                          "cores": threads, "kind": "reference", "sample": sample,
                          "measured_sample_s": t},
@@ -553,13 +563,12 @@ def run_ours(args, rank: int, world: int):
         "vs_baseline": None,
         "dtype": "f64" if head_prec == hb.PRECISION_FP64 else "f64+int8-slices",
         "data": "synthetic",
-        "config": {"workload": f"hif factor + pcg(1e-10), n={n} (N={N}, {dofs(n)} DOFs), "
-                               f"face a=exp(GRF ell=1/16 sigma=1), eps={eps}, P=4, "
-                               + ("FP64" if head_prec == hb.PRECISION_FP64 else
+        "config": {**workload_config(n, eps, world),
+                   "arithmetic": ("FP64" if head_prec == hb.PRECISION_FP64 else
                                   "mixed: Schur complements from 5 and X from 7 int8 slices "
                                   "per value on the tcgen05 tensor cores (exact int32 sums), "
                                   "FP64 A22^-1 / pivots / storage / residual"),
-                   "parallelism": f"replicas x{world}", "l2_flush": "256 MB write per step",
+                   "l2_flush": "256 MB write per step",
                    "inputs": "coefficients and rhs resident in HBM"},
         "factor_s": float(np.mean(fac)),
         "solve_ms": float(np.median(solve_ms)),

@@ -1,0 +1,56 @@
+"""bench.py pieces that run on host cores (CPU).
+
+The reference arm (`bench.py --impl reference`) times the reference's own CPU
+build and must print one JSON line with the same metric, unit, config and
+direction as the GPU arm, a cpu_baseline describing the run and an e2e entry
+without host-device traffic. The serving arrivals are a seeded Poisson process
+whose mix the workload description states.
+"""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import bench
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.skipif(not os.path.exists(bench.REF_PROBE),
+                    reason="reference CPU build absent (make -C oracle)")
+def test_reference_arm_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "0"],
+                         capture_output=True, text=True, timeout=600, check=True).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["metric"] == bench.METRIC
+    assert line["unit"] == "factor+solve steps/s at n=128" and line["higher_is_better"] is True
+    cfg = line["config"]
+    for k, v in bench.workload_config(128, 1e-6, 1).items():
+        assert cfg[k] == v
+    assert line["value"] > 0 and line["ms_per_step"] == pytest.approx(1e3 / line["value"])
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"],
+                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_units_scale_linearly_in_dofs():
+    assert bench.reference_units(10.0, 32, 32) == pytest.approx(0.1)
+    ratio = bench.dofs(128) / bench.dofs(32)
+    assert bench.reference_units(10.0, 32, 128) == pytest.approx(1.0 / (10.0 * ratio))
+
+
+def test_serving_schedule_is_seeded_poisson_with_the_stated_mix():
+    a = bench.serving_schedule(400, 8.0)
+    b = bench.serving_schedule(400, 8.0)
+    assert a == b
+    arr = np.array([x[0] for x in a])
+    assert np.all(np.diff(arr) >= 0)
+    assert 400 / arr[-1] == pytest.approx(8.0, rel=0.15)  # mean rate
+    n_factor = sum(1 for x in a if x[1] == "factor")
+    assert 0.22 < n_factor / 400 < 0.38  # 30% factorizations
