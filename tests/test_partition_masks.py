@@ -3,9 +3,10 @@
 The golden cases pin the partition to the reference for N <= 31 with the masks
 the reference's own eliminations leave. The serving and bench sizes go further:
 n = 48 and 96 use the clipped partition (cells of P * 2^l DOFs per side, the last
-one per direction cut at N), and n = 64 the reference partition beyond the
-goldens. Cell and face index data depend only on the remaining-DOF mask, so for
-random masks at every level both implementations must produce identical lists:
+one per direction cut at N), and n = 64 and 128 (the bench's size) the reference
+partition beyond the goldens. Cell and face index data depend only on the
+remaining-DOF mask, so for random masks at every level both implementations must
+produce identical lists:
 global / redundant / skeleton positions of every cell (InteriorCellIndexData,
 src/Factor.cpp:359-392) and rows / columns of every face
 (SkelInteractionIndexData, src/Factor.cpp:645-755). Large levels are sampled,
@@ -36,7 +37,7 @@ def cells(cpd, limit, rng):
 
 
 @pytest.mark.parametrize("n,partition,limit", [(48, "clipped", 2000), (96, "clipped", 250),
-                                               (64, "reference", 400)])
+                                               (64, "reference", 400), (128, "reference", 120)])
 def test_partition_on_random_masks(n, partition, limit):
     N, P = n - 1, 4
     NC = N + 1
