@@ -3,8 +3,9 @@
 One step = assemble the face-coefficient operator from HBM-resident coefficient
 arrays, hif_factor (every level: assembly, eliminations, IDs) and one PCG solve
 to relative residual 1e-10 with the factor's inverse apply as preconditioner,
-at n = 128 (N = 127, 2,048,383 DOFs), a = exp(GRF) at faces (correlation 1/16,
-sigma 1, seed 2), eps = 1e-6, FP64. The metric's unit is whole-job
+at n = 128 (N = 127, 2,048,383 DOFs), a = exp(GRF) at faces (generator
+correlation parameter 1/16, i.e. correlation length 1/32 of the unit cube; sigma
+1, seed 2), eps = 1e-6, FP64 and mixed precision. The metric's unit is whole-job
 (factor + solve) steps per second; factor seconds, solves per second and PCG
 iterations are reported alongside.
 
@@ -68,7 +69,8 @@ def replica_times(ms_step: float, e2e_s: float, world: int, device=None):
 def workload_config(n: int, eps: float, world: int) -> dict:
     """The `config` object of both arms' JSON lines: the workload they measure."""
     return {"workload": f"hif factor + pcg(1e-10), n={n} (N={n - 1}, {dofs(n)} DOFs), "
-                        f"face a=exp(GRF ell=1/16 sigma=1), eps={eps}, P=4",
+                        f"face a=exp(GRF sigma=1, correlation length 1/32 of the unit cube), "
+                        f"eps={eps}, P=4",
             "parallelism": f"replicas x{world}"}
 
 

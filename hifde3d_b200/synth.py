@@ -77,9 +77,10 @@ def node_lognormal(N: int, seed: int, sigma: float = 0.5, vscale: float = 0.0):
 
 
 def gaussian_random_field(n: int, seed: int, ell: float, sigma: float) -> np.ndarray:
-    """Periodic GRF on an m^3 grid (m = 2n) over the unit-cell [0, 2)^3 with
-    Gaussian covariance exp(-r^2 / (2 ell^2)), standard deviation sigma.
-    Spectral synthesis: white noise filtered by sqrt of the covariance's FFT."""
+    """Periodic GRF on an m^3 grid (m = 2n, spacing 1/n) over the box [0, 2)^3 with
+    Gaussian covariance exp(-r^2 / (2 ell^2)), standard deviation sigma; ell is in
+    the box's units. Spectral synthesis: white noise filtered by sqrt of the
+    covariance's FFT."""
     m = 2 * n
     h = 1.0 / n
     x = np.fft.fftfreq(m, d=1.0 / m) * h  # signed periodic distance
@@ -95,9 +96,13 @@ def gaussian_random_field(n: int, seed: int, ell: float, sigma: float) -> np.nda
 def face_coefficients_grf(N: int, seed: int, ell: float = 1.0 / 16, sigma: float = 1.0):
     """Face coefficients (ax, ay, az) of a = exp(g), g a GRF sampled at face
     midpoints of the (N+1)-cell grid. Each array has shape (NC+1)^3 and
-    ax[i, j, k] couples nodes (i, j, k) and (i+1, j, k)."""
+    ax[i, j, k] couples nodes (i, j, k) and (i+1, j, k).
+
+    The unit cube is mapped onto the generator's whole box [0, 2)^3 (node i at
+    grid point 2i, spacing 1/NC per grid step), so distances on the cube are half
+    the box's: the field's correlation length on the unit cube is ell / 2."""
     NC = N + 1
-    g = gaussian_random_field(NC, seed, ell, sigma)  # grid spacing 1/(2 NC)
+    g = gaussian_random_field(NC, seed, ell, sigma)
     # node (i, j, k) sits at g[2i, 2j, 2k]; the x-face midpoint at g[2i+1, 2j, 2k].
     m = g.shape[0]
     idx = np.arange(NC + 1)
