@@ -14,7 +14,7 @@
 //     on the GPU (different streams, or host threads sharing a device) race on
 //     it and must be serialised by the caller;
 //   * the first call on a device looks the array's address up once, with that
-//     device current.
+//     device current; that first call should come before any stream capture.
 #include <cuda_runtime.h>
 
 #include <cmath>

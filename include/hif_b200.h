@@ -138,7 +138,8 @@ int hif_schur_device(const double* dB, int n, int r, double* dA22inv, double* dX
  * and the call waits for it to read the pivot status. Every call on a device shares the
  * scratch array: calls whose kernels may overlap on the GPU race and must be
  * serialised by the caller. The first call on a device looks up the array's device
- * address with that device current. */
+ * address with that device current; make that first call before any stream
+ * capture begins. */
 int hif_schur_device_noalloc(const double* dB, int n, int r, double* dA22inv, double* dX,
                              double* dS, void* stream);
 /* InterpDecomp(M, W, skel, red, eps) -- src/InterpDecomp.cpp:86-138: column-pivoted
