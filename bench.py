@@ -3,9 +3,8 @@
 One step = assemble the face-coefficient operator from HBM-resident coefficient
 arrays, hif_factor (every level: assembly, eliminations, IDs) and one PCG solve
 to relative residual 1e-10 with the factor's inverse apply as preconditioner,
-at n = 128 (N = 127, 2,048,383 DOFs), a = exp(GRF) at faces (generator
-correlation parameter 1/16, i.e. correlation length 1/32 of the unit cube; sigma
-1, seed 2), eps = 1e-6, FP64 and mixed precision. The metric's unit is whole-job
+at n = 128 (N = 127, 2,048,383 DOFs), a = exp(GRF) at faces (correlation length
+1/16 of the unit cube, sigma 1, seed 2), eps = 1e-6, FP64 and mixed precision. The metric's unit is whole-job
 (factor + solve) steps per second; factor seconds, solves per second and PCG
 iterations are reported alongside.
 
@@ -43,6 +42,12 @@ def dofs(n: int) -> int:
     return (n - 1) ** 3
 
 
+# Correlation length of the coefficient field on the unit cube, and the value the
+# generator takes for it: synth maps the cube onto its periodic box of length 2.
+GRF_CORRELATION = 1.0 / 16
+GRF_ELL_PARAM = 2 * GRF_CORRELATION
+
+
 # ---------------------------------------------------------------------------
 # replicas (N > 1): every rank factors and solves its own operator
 # ---------------------------------------------------------------------------
@@ -69,7 +74,7 @@ def replica_times(ms_step: float, e2e_s: float, world: int, device=None):
 def workload_config(n: int, eps: float, world: int) -> dict:
     """The `config` object of both arms' JSON lines: the workload they measure."""
     return {"workload": f"hif factor + pcg(1e-10), n={n} (N={n - 1}, {dofs(n)} DOFs), "
-                        f"face a=exp(GRF sigma=1, correlation length 1/32 of the unit cube), "
+                        f"face a=exp(GRF sigma=1, correlation length 1/16 of the unit cube), "
                         f"eps={eps}, P=4",
             "parallelism": f"replicas x{world}"}
 
@@ -136,7 +141,7 @@ def reference_sample(n_sample: int, threads: int, workdir: str):
     from hifde3d_b200 import synth
     N = n_sample - 1
     NC = N + 1
-    g = synth.gaussian_random_field(NC, 2, 1.0 / 16, 1.0)
+    g = synth.gaussian_random_field(NC, 2, GRF_ELL_PARAM, 1.0)
     idx = (2 * np.arange(NC + 1)) % g.shape[0]
     A = np.exp(g[np.ix_(idx, idx, idx)])
     V = np.zeros_like(A)
@@ -379,7 +384,7 @@ def run_ours(args, rank: int, world: int):
 
     # synthetic operator (per-rank seed for replicas) and right-hand side
     seed_op, seed_rhs = replica_seeds(rank)
-    ax, ay, az = synth.face_coefficients_grf(N, seed_op, 1.0 / 16, 1.0)
+    ax, ay, az = synth.face_coefficients_grf(N, seed_op, GRF_ELL_PARAM, 1.0)
     V = np.zeros((NC + 1,) * 3)
     b = synth.dof_vector(N, seed_rhs)
     host = [np.ascontiguousarray(x.ravel(order="F")) for x in (ax, ay, az, V)]

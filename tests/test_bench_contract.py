@@ -54,3 +54,23 @@ def test_serving_schedule_is_seeded_poisson_with_the_stated_mix():
     assert 400 / arr[-1] == pytest.approx(8.0, rel=0.15)  # mean rate
     n_factor = sum(1 for x in a if x[1] == "factor")
     assert 0.22 < n_factor / 400 < 0.38  # 30% factorizations
+
+
+def test_bench_field_has_the_stated_correlation_length():
+    """The bench's coefficient field a = exp(g): g has standard deviation 1 and
+    correlation exp(-d^2 / (2 l^2)) with l = 1/16 of the unit cube."""
+    from hifde3d_b200 import synth
+
+    N = 63
+    NC = N + 1
+    assert bench.GRF_CORRELATION == 1.0 / 16
+    vals = {1: [], 2: [], 4: []}
+    for seed in range(3):
+        ax, _, _ = synth.face_coefficients_grf(N, seed, bench.GRF_ELL_PARAM, 1.0)
+        g = np.log(ax)
+        for q in vals:
+            vals[q].append(np.mean(g * np.roll(g, -q, axis=0)) / np.mean(g * g))
+    ell = bench.GRF_CORRELATION
+    for q, v in vals.items():
+        d = q / NC
+        assert np.mean(v) == pytest.approx(np.exp(-d * d / (2 * ell * ell)), abs=0.04)
