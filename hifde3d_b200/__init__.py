@@ -31,7 +31,9 @@ HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET, HIF_ERR_IO = 5, 6, 7, 8
 PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
 OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE, OPT_ID_GROUP_MIN_N = 1, 2, 3, 4, 5
 OPT_PRECISION, OPT_AUTOTUNE, OPT_SCHUR_SLICES, OPT_X_SLICES = 6, 7, 8, 9
+OPT_ELIMINATION, OPT_Y_SLICES = 10, 11
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+ELIM_AUTO, ELIM_GAUSS_JORDAN, ELIM_CHOLESKY = 0, 1, 2
 KCLASS_NAMES = ["gather", "gemm", "sweep_small", "sweep_panel", "id", "gemv", "copy", "vector",
                 "qr", "gemm_mixed", "gemm_int8"]
 TOP, BOTTOM, RIGHT, LEFT, FRONT, BACK = range(6)
@@ -74,6 +76,7 @@ _SIGNATURES = {
     "hif_block_indices": [_p, _i, _i, _i, _ip, _ip, _ip],
     "hif_block_matrix": [_p, _i, _i, _i, _i, _dp],
     "hif_block_pivots": [_p, _i, _i, _ip, _dp],
+    "hif_dof_levels": [_p, _ip],
     "hif_set_option": [_p, _i, _ll],
     "hif_set_replay_pivots": [_p, _i, _i, _ip, _ip],
     "hif_factor_stats": [_p, _dp, _dp, _dp, _dp, _dp, _llp],
@@ -95,6 +98,7 @@ _SIGNATURES = {
     "hif_server_submit_factor": [_p, _i, _i, _i, _d, _i, _i, _d, _dp, _dp, _dp, _dp, _llp],
     "hif_server_submit_solve": [_p, _i, _dp, _i, _d, _i, _dp, _llp],
     "hif_server_wait": [_p, _ll, _ip, _ip, _dp, _dp],
+    "hif_server_wait_detail": [_p, _ll, _ip, _ip, _dp, _dp, _dp],
     "hif_server_release": [_p, _i],
     "hif_server_stats": [_p, _llp, _llp, _llp, _llp, _llp],
     "hif_partition_cell": [_i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_ubyte),
@@ -346,6 +350,13 @@ class HIFFactor:
         _check(lib().hif_block_pivots(self._h, level, b, _iptr(jp), _dptr(rd)))
         return jp[:n].astype(np.int64), rd[:n]
 
+    def dof_levels(self) -> np.ndarray:
+        """Per DOF id: the phase that eliminated it (2 * level + kind), -1 on the
+        index-0 planes."""
+        out = np.zeros(self.NC ** 3, np.int32)
+        _check(lib().hif_dof_levels(self._h, _iptr(out)))
+        return out
+
     def kernel_stats(self) -> dict:
         """Per kernel class: launches, ms, algorithmic flops and bytes (needs OPT_PROFILE)."""
         out = {}
@@ -464,14 +475,18 @@ class Server:
         return rid.value
 
     def wait(self, request_id: int) -> dict:
+        """Blocks until the request ends. latency_ms = submit to completion,
+        queue_ms = submit to admission, service_ms = the rest."""
         st, it = _i(), _i()
-        rr, lat = _d(), _d()
-        code = lib().hif_server_wait(self._h, int(request_id), ctypes.byref(st), ctypes.byref(it),
-                                     ctypes.byref(rr), ctypes.byref(lat))
+        rr, lat, qu = _d(), _d(), _d()
+        code = lib().hif_server_wait_detail(self._h, int(request_id), ctypes.byref(st),
+                                            ctypes.byref(it), ctypes.byref(rr),
+                                            ctypes.byref(lat), ctypes.byref(qu))
         _check(code)
         x, meta = self._out.pop(int(request_id), (None, None))
         res = {"status": st.value, "iters": it.value, "relres": rr.value,
-               "latency_ms": lat.value}
+               "latency_ms": lat.value, "queue_ms": qu.value,
+               "service_ms": lat.value - qu.value}
         if st.value != HIF_OK:
             res["error"] = lib().hif_last_error().decode()
         if x is not None:

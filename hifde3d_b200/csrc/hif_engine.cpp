@@ -278,6 +278,9 @@ struct BlockInfo {
 struct StepData {
   int level = 0;
   bool skel = false;
+  // elimination by Cholesky: the A22 / A22^{-1} / X slots hold L, L^{-1} and
+  // Y = L^{-1} A21 instead (see chol_blocks)
+  bool chol = false;
   int cpd = 0;
   std::vector<BlockInfo> blocks;
   double* arena = nullptr;  // A22 | A22inv | X | W per block
@@ -297,7 +300,7 @@ struct ApplyLaunch {
   GemvDesc* d_desc = nullptr;
   int* d_toff = nullptr;
   int nd = 0, tiles = 0;
-  int in_vec = 0, out_vec = 0;  // 0 = ua, 1 = ub
+  int in_vec = 0, out_vec = 0;  // 0 = ua, 1 = ub, 2 = uc (Cholesky phases' L^{-1} u_r)
   int* d_dof = nullptr;
   int* d_off = nullptr;
   int* d_slot = nullptr;
@@ -634,6 +637,248 @@ struct ElimArith {
   int schur = -1;
   int x = 0;
 };
+
+// Cholesky elimination of a batch of symmetric positive definite interiors
+// (lower triangles only): writes L (descs[b].L), L^{-1} (a22inv) and
+// Y = L^{-1} A21 (X); B's trailing block ends as A11 - Y^T Y, mirrored.
+//   small blocks: k_chol_small, whole in shared memory;
+//   large blocks: right-looking over 128-pivot blocks of A22 only:
+//     L_KK = chol(B[K, K]) and L_KK^{-1} (k_chol_diag),
+//     panel  B[K1:r, K] = B[K1:r, K] L_KK^{-T},
+//     update B[K1:r, K1:r] -= panel panel^T (lower tiles),
+//     row block K of L^{-1}: -L_KK^{-1} (L[K, 0:K0] L^{-1}[0:K0, 0:K0]), and L_KK^{-1};
+//   then Y = L^{-1} A21 and S = A11 - Y^T Y as long-K products (FP64, or from
+//   int8 slices in mixed precision: ar.x slices for Y, ar.schur for S).
+// 2r^3/3 + 2r^2 s + r s^2 flops against the Gauss-Jordan path's
+// r^3 + 2r^2 s + r s^2 (symmetric), with Y's product entries bounded by
+// about sqrt(cond(A22)) times A21's rather than cond(A22) times.
+template <class Timed>
+void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t stream,
+                 int* d_status, Timed&& timed, ElimArith ar, Arena* scratch) {
+  auto big = [&](size_t count) -> double* {
+    return scratch ? scratch->alloc<double>(count) : tmp.add(dalloc<double>(count, stream));
+  };
+  std::vector<SweepDesc> small, large;
+  int max_small = 0;
+  for (const SweepDesc& d : descs) {
+    if (d.r <= 0) continue;
+    if (d.n <= kSmallSweepN) {
+      small.push_back(d);
+      max_small = std::max(max_small, d.n);
+    } else {
+      large.push_back(d);
+    }
+  }
+  if (!small.empty()) {
+    SweepDesc* dd = tmp.add(upload(small, stream));
+    double fl = 0, by = 0;
+    for (const SweepDesc& d : small) {
+      const double r = d.r, sk = d.n - d.r;
+      fl += 2.0 / 3.0 * r * r * r + 2 * r * r * sk + 2 * r * sk * sk;
+      by += 8.0 * d.n * d.n + 8.0 * (2 * r * r + r * sk + sk * sk);
+    }
+    timed(HIF_KCLASS_SWEEP_SMALL, fl, by, [&] {
+      launch_chol_small(dd, (int)small.size(), max_small, d_status, stream);
+    });
+    HIF_CK(cudaGetLastError());
+  }
+  if (large.empty()) return;
+  const int nl = (int)large.size();
+  SweepDesc* dd = tmp.add(upload(large, stream));
+  double* dinv = big((size_t)nl * kSweepNB * kSweepNB);
+  int maxr = 0;
+  std::vector<long long> oq(nl);
+  long long qsz = 0;
+  for (int b = 0; b < nl; ++b) {
+    maxr = std::max(maxr, large[b].r);
+    oq[b] = qsz;
+    qsz += (long long)large[b].r * kSweepNB;
+  }
+  double* Qb = big(qsz);  // per block: old panel (r x 128, ld r)
+  double* Tb = big(qsz);  // per block: L[K, 0:K0] L^{-1}[0:K0, 0:K0] (128 x r, ld 128)
+  // L and L^{-1} read as zero above their diagonals
+  {
+    std::vector<GemmDesc> z;
+    for (const SweepDesc& d : large)
+      for (double* C : {d.L, d.a22inv}) {
+        GemmDesc g{};
+        g.C = C;
+        g.A = g.B = C;
+        g.ldc = g.lda = g.ldb = d.r;
+        g.m = g.n = d.r;
+        g.k = 0;
+        z.push_back(g);
+      }
+    gemm_batch(z, tmp, stream, HIF_KCLASS_COPY, timed);
+  }
+  for (int k0 = 0; k0 < maxr; k0 += kSweepNB) {
+    std::vector<int> active;
+    std::vector<CopyDesc> cq, cdg;
+    std::vector<int> ocq(1, 0), ocd(1, 0);
+    std::vector<GemmDesc> gp, gu, gt, gl;
+    for (int b = 0; b < nl; ++b) {
+      const SweepDesc& d = large[b];
+      if (d.r <= k0) continue;
+      active.push_back(b);
+      const int r = d.r, k1 = std::min(r, k0 + kSweepNB), nbk = k1 - k0;
+      const double* Dv = dinv + (long long)b * kSweepNB * kSweepNB;  // nbk x nbk, ld nbk
+      double* Q = Qb + oq[b];
+      double* T = Tb + oq[b];
+      double* P = d.B + k1 + (long long)k0 * d.n;  // panel rows k1..r of column block K
+      if (r > k1) {
+        cq.push_back(CopyDesc{P, Q, d.n, r, r - k1, nbk});
+        ocq.push_back(ocq.back() + copy_tiles(r - k1, nbk));
+        GemmDesc g{};
+        g.C = P;
+        g.ldc = d.n;
+        g.A = Q;
+        g.lda = r;
+        g.B = Dv;
+        g.ldb = nbk;
+        g.transB = 1;
+        g.m = r - k1;
+        g.n = nbk;
+        g.k = nbk;
+        g.alpha = 1.0;
+        gp.push_back(g);
+        GemmDesc u{};
+        u.C = d.B + k1 + (long long)k1 * d.n;
+        u.ldc = d.n;
+        u.A = P;
+        u.lda = d.n;
+        u.B = P;
+        u.ldb = d.n;
+        u.transB = 1;
+        u.m = u.n = r - k1;
+        u.k = nbk;
+        u.alpha = -1.0;
+        u.beta = 1.0;
+        u.lower = 1;
+        gu.push_back(u);
+      }
+      if (k0 > 0) {
+        GemmDesc t{};
+        t.C = T;
+        t.ldc = kSweepNB;
+        t.A = d.B + k0;  // L[K, 0:k0]
+        t.lda = d.n;
+        t.B = d.a22inv;  // L^{-1}[0:k0, 0:k0]
+        t.ldb = r;
+        t.m = nbk;
+        t.n = k0;
+        t.k = k0;
+        t.alpha = 1.0;
+        gt.push_back(t);
+        GemmDesc l{};
+        l.C = d.a22inv + k0;
+        l.ldc = r;
+        l.A = Dv;
+        l.lda = nbk;
+        l.B = T;
+        l.ldb = kSweepNB;
+        l.m = nbk;
+        l.n = k0;
+        l.k = nbk;
+        l.alpha = -1.0;
+        gl.push_back(l);
+      }
+      cdg.push_back(CopyDesc{Dv, d.a22inv + k0 + (long long)k0 * r, nbk, r, nbk, nbk});
+      ocd.push_back(ocd.back() + copy_tiles(nbk, nbk));
+    }
+    BufList step;
+    int* dact = step.add(upload(active, stream));
+    timed(HIF_KCLASS_SWEEP_PANEL, 0, 0, [&] {
+      launch_chol_diag(dd, dact, (int)active.size(), k0, dinv, d_status, stream);
+    });
+    if (!cq.empty()) {
+      CopyDesc* dq = step.add(upload(cq, stream));
+      int* doq = step.add(upload(ocq, stream));
+      timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dq, doq, (int)cq.size(), ocq.back(), stream); });
+    }
+    gemm_batch(gp, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+    gemm_batch(gu, step, stream, HIF_KCLASS_GEMM, timed, 128);
+    gemm_batch(gt, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+    gemm_batch(gl, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+    {
+      CopyDesc* dc = step.add(upload(cdg, stream));
+      int* doc = step.add(upload(ocd, stream));
+      timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dc, doc, (int)cdg.size(), ocd.back(), stream); });
+    }
+    HIF_CK(cudaGetLastError());
+    step.release(stream);
+  }
+  // L: the block-lower column strips of B[0:r, 0:r] (its diagonal tiles already
+  // hold zeros above the diagonal; the tiles above them still hold A22)
+  {
+    std::vector<CopyDesc> cl;
+    std::vector<int> ocl(1, 0);
+    for (const SweepDesc& d : large)
+      for (int j0 = 0; j0 < d.r; j0 += kSweepNB) {
+        const int nbj = std::min(kSweepNB, d.r - j0);
+        cl.push_back(CopyDesc{d.B + j0 + (long long)j0 * d.n, d.L + j0 + (long long)j0 * d.r,
+                              d.n, d.r, d.r - j0, nbj});
+        ocl.push_back(ocl.back() + copy_tiles(d.r - j0, nbj));
+      }
+    CopyDesc* dc = tmp.add(upload(cl, stream));
+    int* doc = tmp.add(upload(ocl, stream));
+    timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dc, doc, (int)cl.size(), ocl.back(), stream); });
+    HIF_CK(cudaGetLastError());
+  }
+  // Y = L^{-1} A21 and S = A11 - Y^T Y
+  std::vector<GemmDesc> gy, gs;
+  for (const SweepDesc& d : large) {
+    const int r = d.r, sk = d.n - d.r;
+    if (sk == 0) continue;
+    GemmDesc y{};
+    y.C = d.X;
+    y.ldc = r;
+    y.A = d.a22inv;
+    y.lda = r;
+    y.B = d.B + (long long)r * d.n;
+    y.ldb = d.n;
+    y.m = r;
+    y.n = sk;
+    y.k = r;
+    y.alpha = 1.0;
+    gy.push_back(y);
+    GemmDesc g{};
+    g.C = d.B + r + (long long)r * d.n;
+    g.ldc = d.n;
+    g.A = d.X;
+    g.lda = r;
+    g.transA = 1;
+    g.B = d.X;
+    g.ldb = r;
+    g.m = g.n = sk;
+    g.k = r;
+    g.alpha = -1.0;
+    g.beta = 1.0;
+    g.lower = 1;
+    gs.push_back(g);
+  }
+  if (ar.x > 0) gemm_batch_int8(gy, tmp, stream, timed, ar.x, d_status);
+  else gemm_batch(gy, tmp, stream, HIF_KCLASS_GEMM, timed);
+  if (ar.schur > 0) gemm_batch_int8(gs, tmp, stream, timed, ar.schur, d_status);
+  else if (ar.schur == 0) gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM_MIXED, timed, 128, d_status);
+  else gemm_batch(gs, tmp, stream, HIF_KCLASS_GEMM, timed, 128);
+  std::vector<TCopyDesc> tm;
+  std::vector<int> otm(1, 0);
+  for (const SweepDesc& d : large) {
+    const int sk = d.n - d.r;
+    double* S = d.B + d.r + (long long)d.r * d.n;
+    for (int j0 = 128; j0 < sk; j0 += 128) {
+      const int j1 = std::min(sk, j0 + 128);
+      tm.push_back(TCopyDesc{S + j0, S + (long long)j0 * d.n, d.n, d.n, j0, j1 - j0, 1.0});
+      otm.push_back(otm.back() + copy_tiles(j0, j1 - j0));
+    }
+  }
+  if (!tm.empty()) {
+    TCopyDesc* dm = tmp.add(upload(tm, stream));
+    int* dom = tmp.add(upload(otm, stream));
+    timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_tcopy(dm, dom, (int)tm.size(), otm.back(), stream); });
+    HIF_CK(cudaGetLastError());
+  }
+}
 
 template <class Timed>
 void sweep_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t stream,
@@ -1069,6 +1314,7 @@ class Engine {
   // apply / solve workspace
   double* d_ua = nullptr;
   double* d_ub = nullptr;
+  double* d_uc = nullptr;
   double* d_contrib = nullptr;
   int ws_nrhs = 0;
   ApplyPlan plan_inv, plan_fwd;
@@ -1168,8 +1414,9 @@ class Engine {
     drop_graphs();
     dfree(d_ua, stream);
     dfree(d_ub, stream);
+    dfree(d_uc, stream);
     dfree(d_pcg, stream);
-    d_ua = d_ub = d_pcg = nullptr;
+    d_ua = d_ub = d_uc = d_pcg = nullptr;
     ws_nrhs = pcg_nrhs = 0;
   }
 
@@ -1282,7 +1529,7 @@ class Engine {
   }
 
   void run_gemm_plan(ApplyPlan& plan, GemmPlan& gp, int nrhs) {
-    double* vec[2] = {d_ua, d_ub};
+    double* vec[3] = {d_ua, d_ub, d_uc};
     for (GemmStage& st : gp.stages) {
       ApplyLaunch& l = plan.launches[st.launch];
       if (l.type == 0) {
@@ -1374,11 +1621,11 @@ class Engine {
     ElimArith ar;
     if (precision == HIF_PRECISION_MIXED) {
       ar.schur = schur_slices;
-      ar.x = x_slices;
+      ar.x = use_chol ? y_slices : x_slices;
     }
-    sweep_blocks(descs, tmp, stream, d_status,
-                 [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); },
-                 ar, symmetric, cur_work);
+    auto tm = [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); };
+    if (use_chol) chol_blocks(descs, tmp, stream, d_status, tm, ar, cur_work);
+    else sweep_blocks(descs, tmp, stream, d_status, tm, ar, symmetric, cur_work);
   }
 
   void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
@@ -1426,6 +1673,7 @@ class Engine {
     StepData st;
     st.level = level;
     st.skel = false;
+    st.chol = use_chol;
     st.cpd = cpd;
     Partitioner part{N, P, NC, rem.data()};
     const int ncell = cpd * cpd * cpd;
@@ -1554,6 +1802,7 @@ class Engine {
       d.B = dB + o_B[b];
       d.a22inv = st.arena + st.o_inv[b];
       d.X = st.arena + st.o_x[b];
+      d.L = st.arena + st.o_a22[b];
       d.n = bi.global.size();
       d.r = bi.r();
       sd.push_back(d);
@@ -1685,6 +1934,7 @@ class Engine {
     StepData st;
     st.level = level;
     st.skel = true;
+    st.chol = use_chol;
     st.cpd = cpd;
     std::vector<std::vector<int>> rows_l;
     std::vector<BlockInfo>& blocks = st.blocks;
@@ -1784,8 +2034,11 @@ class Engine {
       idm[f] = rows_l[f].size();
     }
     // mixed precision: tall faces go to the pivoted Cholesky ID instead (no
-    // compression; replayed pivot orders keep the QR path)
-    const bool chol = precision == HIF_PRECISION_MIXED && d_ord == nullptr;
+    // compression; replayed pivot orders keep the QR path). The Gram matrix
+    // M^T M resolves a column's remaining norm only down to about sqrt(u) ||M||
+    // = 1.5e-8 ||M||, so the rank test R_ii <= eps R_00 needs eps well above
+    // that: below kGramMinEps the faces take the FP64 pivoted QR as in FP64 mode.
+    const bool chol = precision == HIF_PRECISION_MIXED && d_ord == nullptr && eps >= kGramMinEps;
     if (!chol) compress_faces(blocks, rows_l, dM, o_M, idM, idm, tmp);
     mark("skel row compression", level);
     std::vector<IdDesc> idd(nf);
@@ -2039,6 +2292,7 @@ class Engine {
   // choices equal column-pivoted QR's in exact arithmetic (InterpDecomp.cpp:
   // 86-138); the skeleton test is the reference's |R_ii| > eps |R_00|.
   static constexpr int kPcholNB = 32;
+  static constexpr double kGramMinEps = 1e-7;
   void id_cholesky(const std::vector<IdDesc>& v, BufList& tmp) {
     Arena& work = *cur_work;
     const int nd = (int)v.size();
@@ -2458,6 +2712,7 @@ class Engine {
       d.B = dB + o_B[f];
       d.a22inv = st.arena + st.o_inv[f];
       d.X = st.arena + st.o_x[f];
+      d.L = st.arena + st.o_a22[f];
       d.n = b.global.size();
       d.r = b.r();
       sd.push_back(d);
@@ -2473,7 +2728,10 @@ class Engine {
   bool autotune = false;
   // HIF_PRECISION_MIXED: int8 slices of the Schur products (0: split TF32) and
   // of the X products (0: FP64)
-  int schur_slices = 5, x_slices = 7;
+  int schur_slices = 5, x_slices = 7, y_slices = 6;
+  // HIF_OPT_ELIMINATION, and the choice made for the factorization in progress
+  int elimination = HIF_ELIM_AUTO;
+  bool use_chol = false;
   struct StageScope {
     PinnedStage* prev;
     Arena* prev_scratch;
@@ -2502,6 +2760,14 @@ class Engine {
     if (partition == HIF_PARTITION_CLIPPED && NC % P != 0)
       throw Error{HIF_ERR_ARG, "clipped partition needs (N+1) divisible by P"};
     initialize();
+    // Cholesky elimination for symmetric operators: by default in mixed
+    // precision; the FP64 default keeps the reference's explicit inverse
+    // (getrf + getri, include/Schur.hpp:86)
+    if (elimination == HIF_ELIM_CHOLESKY && !symmetric)
+      throw Error{HIF_ERR_ARG, "Cholesky elimination needs a symmetric operator "
+                               "(hif_setup_stencil_faces)"};
+    use_chol = symmetric && (elimination == HIF_ELIM_CHOLESKY ||
+                             (elimination == HIF_ELIM_AUTO && precision == HIF_PRECISION_MIXED));
     t_total = t_gather = t_elim = t_id = t_host = 0;
     cur_bytes = peak_bytes = 0;
     HIF_CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), stream));
@@ -2549,7 +2815,7 @@ class Engine {
   // W (k x r, ld k), A22 / A22^{-1} (r x r, ld r).
   long long plan_key = 0;  // stage key for the next launches added to a plan
   void add_gemv(ApplyPlan& plan, const StepData& st, int which, int trans, bool in_red,
-                bool out_red, double alpha, int mode, int in_vec, int out_vec) {
+                bool out_red, double alpha, int mode, int in_vec, int out_vec, int tri = 0) {
     const long long my_key = plan_key++;  // taken even when the launch is empty
     std::vector<GemvDesc> dd;
     std::vector<int> toff(1, 0);
@@ -2578,6 +2844,7 @@ class Engine {
       g.in_idx = in_red ? st.d_red + st.o_red[b] : st.d_skel + st.o_skel[b];
       g.out_idx = out_red ? st.d_red + st.o_red[b] : st.d_skel + st.o_skel[b];
       g.trans = trans;
+      g.tri = tri;
       g.alpha = alpha;
       g.mode = mode;
       g.contrib = (mode == 1) ? d_contrib + st.o_skel[b] : nullptr;
@@ -2598,6 +2865,40 @@ class Engine {
     l.hdesc = dd;
     l.key = my_key;
     plan.launches.push_back(l);
+  }
+
+  // A22 = L L^T, A22^{-1} = L^{-T} L^{-1} or X = L^{-T} Y (which 0 / 1 / 2) of
+  // block b of a Cholesky phase, formed on the device, copied to `out`.
+  void chol_readback(const StepData& st, int b, int which, double* out) {
+    const BlockInfo& bi = st.blocks[b];
+    const int r = bi.r(), k = bi.s();
+    const int ncol = which == 2 ? k : r;
+    BufList tmp;
+    double* C = tmp.add(dalloc<double>((size_t)r * ncol, stream));
+    GemmDesc g{};
+    g.C = C;
+    g.ldc = r;
+    g.m = r;
+    g.n = ncol;
+    g.k = r;
+    g.alpha = 1.0;
+    g.lda = g.ldb = r;
+    if (which == 0) {
+      g.A = g.B = st.arena + st.o_a22[b];
+      g.transB = 1;
+    } else {
+      g.A = st.arena + st.o_inv[b];
+      g.transA = 1;
+      g.B = which == 1 ? st.arena + st.o_inv[b] : st.arena + st.o_x[b];
+    }
+    std::vector<GemmDesc> v(1, g);
+    gemm_batch(v, tmp, stream, HIF_KCLASS_GEMM,
+               [&](int, double, double, auto&& f, int = 1) { f(); }, 128);
+    HIF_CK(cudaGetLastError());
+    sync();
+    HIF_CK(cudaMemcpy(out, C, (size_t)r * ncol * 8, cudaMemcpyDeviceToHost));
+    tmp.release(stream);
+    sync();
   }
 
   void add_reduce(ApplyPlan& plan, const StepData& st, double alpha, int vec) {
@@ -2665,59 +2966,127 @@ class Engine {
     auto key = [](int seg, int lev, int sub) {
       return ((long long)seg << 32) | ((long long)lev << 8) | sub;
     };
+    // Vectors: 0 = ua (input, forward sweeps), 1 = ub (output, backward
+    // sweeps), 2 = uc. A Gauss-Jordan phase (A22^{-1}, X) follows
+    // src/Factor.cpp:992-1081: forward u_s -= X^T u_r, diagonal u_r = A22^{-1} u_r
+    // (ua -> ub), backward u_r -= X u_s. A Cholesky phase (L, L^{-1}, Y) splits
+    // A22^{-1} = L^{-T} L^{-1} around the sweeps: forward v_r = L^{-1} u_r
+    // (ua -> uc), u_s -= Y^T v_r; backward v_r -= Y u_s (uc), u_r = L^{-T} v_r
+    // (uc -> ub); no diagonal step (the top phase, which has no skeleton, does
+    // both triangles there). Each phase's redundant entries of uc are its own.
     // inverse
     {
       ApplyPlan& p = plan_inv;
       for (int l = 0; l < L - 1; ++l) {
         if (sch[l]) {
           plan_key = key(0, l, 0);
-          add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 0, 0);
+          if (sch[l]->chol) {
+            add_gemv(p, *sch[l], 3, 0, true, true, 1.0, 2, 0, 2, 1);
+            add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 2, 0);
+          } else {
+            add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 0, 0);
+          }
           add_reduce(p, *sch[l], -1.0, 0);
         }
         if (skl[l]) {
           plan_key = key(0, l, 4);
           add_gemv(p, *skl[l], 1, 1, false, true, -1.0, 0, 0, 0);
-          add_gemv(p, *skl[l], 0, 1, true, false, -1.0, 0, 0, 0);
+          if (skl[l]->chol) {
+            add_gemv(p, *skl[l], 3, 0, true, true, 1.0, 2, 0, 2, 1);
+            add_gemv(p, *skl[l], 0, 1, true, false, -1.0, 0, 2, 0);
+          } else {
+            add_gemv(p, *skl[l], 0, 1, true, false, -1.0, 0, 0, 0);
+          }
         }
       }
       for (int l = 0; l < L; ++l) {
-        plan_key = key(1, l, 0);
-        if (sch[l]) add_gemv(p, *sch[l], 3, 0, true, true, 1.0, 2, 0, 1);
-        plan_key = key(1, l, 4);
-        if (skl[l]) add_gemv(p, *skl[l], 3, 0, true, true, 1.0, 2, 0, 1);
+        for (const StepData* st : {sch[l], skl[l]}) {
+          if (!st) continue;
+          plan_key = key(1, l, st->skel ? 4 : 0);
+          if (!st->chol) {
+            add_gemv(p, *st, 3, 0, true, true, 1.0, 2, 0, 1);
+          } else if (l == L - 1) {
+            add_gemv(p, *st, 3, 0, true, true, 1.0, 2, 0, 2, 1);
+            add_gemv(p, *st, 3, 1, true, true, 1.0, 2, 2, 1, 1);
+          }
+        }
       }
       for (int l = L - 2; l >= 0; --l) {
         if (skl[l]) {
           plan_key = key(2, 255 - l, 0);
-          add_gemv(p, *skl[l], 0, 0, false, true, -1.0, 0, 1, 1);
+          if (skl[l]->chol) {
+            add_gemv(p, *skl[l], 0, 0, false, true, -1.0, 0, 1, 2);
+            add_gemv(p, *skl[l], 3, 1, true, true, 1.0, 2, 2, 1, 1);
+          } else {
+            add_gemv(p, *skl[l], 0, 0, false, true, -1.0, 0, 1, 1);
+          }
           add_gemv(p, *skl[l], 1, 0, true, false, -1.0, 0, 1, 1);
         }
         plan_key = key(2, 255 - l, 4);
-        if (sch[l]) add_gemv(p, *sch[l], 0, 0, false, true, -1.0, 0, 1, 1);
+        if (sch[l]) {
+          if (sch[l]->chol) {
+            add_gemv(p, *sch[l], 0, 0, false, true, -1.0, 0, 1, 2);
+            add_gemv(p, *sch[l], 3, 1, true, true, 1.0, 2, 2, 1, 1);
+          } else {
+            add_gemv(p, *sch[l], 0, 0, false, true, -1.0, 0, 1, 1);
+          }
+        }
       }
     }
-    // forward (F u)
+    // forward (F u). Gauss-Jordan phase: u_r += X u_s, u_r = A22 u_r, u_s += X^T u_r.
+    // Cholesky phase, F = [L 0; Y^T I] [I 0; 0 S] [L^T Y; 0 I]: w_r = L^T u_r + Y u_s
+    // (ua -> uc), then u_s += Y^T w_r and u_r = L w_r (uc -> ub).
     {
       ApplyPlan& p = plan_fwd;
       for (int l = 0; l < L - 1; ++l) {
-        if (sch[l]) add_gemv(p, *sch[l], 0, 0, false, true, 1.0, 0, 0, 0);
+        if (sch[l]) {
+          if (sch[l]->chol) {
+            add_gemv(p, *sch[l], 2, 1, true, true, 1.0, 2, 0, 2, 1);
+            add_gemv(p, *sch[l], 0, 0, false, true, 1.0, 0, 0, 2);
+          } else {
+            add_gemv(p, *sch[l], 0, 0, false, true, 1.0, 0, 0, 0);
+          }
+        }
         if (skl[l]) {
           add_gemv(p, *skl[l], 1, 0, true, false, 1.0, 0, 0, 0);
-          add_gemv(p, *skl[l], 0, 0, false, true, 1.0, 0, 0, 0);
+          if (skl[l]->chol) {
+            add_gemv(p, *skl[l], 2, 1, true, true, 1.0, 2, 0, 2, 1);
+            add_gemv(p, *skl[l], 0, 0, false, true, 1.0, 0, 0, 2);
+          } else {
+            add_gemv(p, *skl[l], 0, 0, false, true, 1.0, 0, 0, 0);
+          }
         }
       }
       for (int l = 0; l < L; ++l) {
-        if (sch[l]) add_gemv(p, *sch[l], 2, 0, true, true, 1.0, 2, 0, 1);
-        if (skl[l]) add_gemv(p, *skl[l], 2, 0, true, true, 1.0, 2, 0, 1);
+        for (const StepData* st : {sch[l], skl[l]}) {
+          if (!st) continue;
+          if (!st->chol) {
+            add_gemv(p, *st, 2, 0, true, true, 1.0, 2, 0, 1);
+          } else if (l == L - 1) {
+            add_gemv(p, *st, 2, 1, true, true, 1.0, 2, 0, 2, 1);
+            add_gemv(p, *st, 2, 0, true, true, 1.0, 2, 2, 1, 1);
+          }
+        }
       }
       for (int l = L - 2; l >= 0; --l) {
         if (skl[l]) {
-          add_gemv(p, *skl[l], 0, 1, true, false, 1.0, 0, 1, 1);
+          if (skl[l]->chol) {
+            add_gemv(p, *skl[l], 0, 1, true, false, 1.0, 0, 2, 1);
+            add_gemv(p, *skl[l], 2, 0, true, true, 1.0, 2, 2, 1, 1);
+          } else {
+            add_gemv(p, *skl[l], 0, 1, true, false, 1.0, 0, 1, 1);
+          }
           add_gemv(p, *skl[l], 1, 1, false, true, 1.0, 0, 1, 1);
         }
         if (sch[l]) {
-          add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 1, 1);
-          add_reduce(p, *sch[l], 1.0, 1);
+          if (sch[l]->chol) {
+            add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 2, 1);
+            add_reduce(p, *sch[l], 1.0, 1);
+            add_gemv(p, *sch[l], 2, 0, true, true, 1.0, 2, 2, 1, 1);
+          } else {
+            add_gemv(p, *sch[l], 0, 1, true, false, 1.0, 1, 1, 1);
+            add_reduce(p, *sch[l], 1.0, 1);
+          }
         }
       }
     }
@@ -2730,13 +3099,15 @@ class Engine {
     drop_graphs();
     dfree(d_ua, stream);
     dfree(d_ub, stream);
+    dfree(d_uc, stream);
     d_ua = dalloc<double>(n3 * nrhs, stream);
     d_ub = dalloc<double>(n3 * nrhs, stream);
+    d_uc = dalloc<double>(n3 * nrhs, stream);
     ws_nrhs = nrhs;
   }
 
   void run_plan(ApplyPlan& plan, int nrhs) {
-    double* vec[2] = {d_ua, d_ub};
+    double* vec[3] = {d_ua, d_ub, d_uc};
     for (ApplyLaunch& l : plan.launches) {
       if (l.type == 0) {
         const double by = l.bytes * ((nrhs + 3) / 4);
@@ -3193,6 +3564,16 @@ int hif_block_matrix(hif_handle h, int level, int kind, int b, int which, double
     const hif::BlockInfo& bi = s->blocks[b];
     const long long r = bi.r(), k = bi.s();
     long long off = 0, cnt = 0;
+    if (s->chol && which >= 0 && which <= 2) {
+      // the reference's A22, A22^{-1}, X from the stored L, L^{-1}, Y
+      if (r == 0 || (which == 2 && k == 0)) return;
+      h->e->chol_readback(*s, b, which, out);
+      return;
+    }
+    if (which >= 5 && which <= 7) {
+      if (!s->chol) throw hif::Error{HIF_ERR_ARG, "which 5-7: Cholesky phases only"};
+      which -= 5;
+    }
     switch (which) {
       case 0: off = s->o_a22[b]; cnt = r * r; break;
       case 1: off = s->o_inv[b]; cnt = r * r; break;
@@ -3217,6 +3598,19 @@ int hif_block_matrix(hif_handle h, int level, int kind, int b, int which, double
     h->e->sync();
     HIF_CK(cudaMemcpy(out, s->arena + off, cnt * 8, cudaMemcpyDeviceToHost));
   });
+}
+
+int hif_dof_levels(hif_handle h, int* phase_of_dof) {
+  if (!h || !phase_of_dof) return HIF_ERR_ARG;
+  if (!h->e->factored) {
+    hif::g_last_error = "no factorization";
+    return HIF_ERR_STATE;
+  }
+  std::fill(phase_of_dof, phase_of_dof + h->e->n3, -1);
+  for (const hif::StepData& st : h->e->steps)
+    for (const hif::BlockInfo& bi : st.blocks)
+      for (int p : bi.red_pos) phase_of_dof[bi.global[p]] = 2 * st.level + (st.skel ? 1 : 0);
+  return HIF_OK;
 }
 
 int hif_block_pivots(hif_handle h, int level, int b, int* jpvt, double* rdiag) {
@@ -3252,6 +3646,15 @@ int hif_set_option(hif_handle h, int option, long long value) {
     case HIF_OPT_X_SLICES:
       if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
       h->e->x_slices = (int)value;
+      return HIF_OK;
+    case HIF_OPT_ELIMINATION:
+      if (value != HIF_ELIM_AUTO && value != HIF_ELIM_GAUSS_JORDAN && value != HIF_ELIM_CHOLESKY)
+        return HIF_ERR_ARG;
+      h->e->elimination = (int)value;
+      return HIF_OK;
+    case HIF_OPT_Y_SLICES:
+      if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
+      h->e->y_slices = (int)value;
       return HIF_OK;
     case HIF_OPT_ID_GROUP_MIN_N:
       if (value < 2) return HIF_ERR_ARG;

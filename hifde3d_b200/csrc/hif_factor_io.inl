@@ -11,7 +11,9 @@
 //            symmetric, precision the factor was made in (informational),
 //            has_operator, nsteps, f64 eps, i64 NC^3
 //   per step (Schur or skeletonization phase of one level)
-//            i32 level, skel, cells_per_dir, nblocks; i64 arena doubles, n_red,
+//            i32 level, kind (bit 0: skeletonization; bit 1: eliminated by
+//            Cholesky, so the arena holds L | L^-1 | Y | W), cells_per_dir,
+//            nblocks; i64 arena doubles, n_red,
 //            n_skel; per block i32 face, cell, nbr and the int vectors
 //            global, red_pos, skel_pos, jpvt and the double vector rdiag
 //            (each an i64 count then the values); the i64 offset vectors
@@ -223,7 +225,8 @@ void save_factor(Engine& e, const char* path) {
   w.pod<double>(e.eps);
   w.pod<long long>(e.n3);
   for (const StepData& st : e.steps) {
-    const int32_t sh[4] = {st.level, st.skel ? 1 : 0, st.cpd, (int32_t)st.blocks.size()};
+    const int32_t sh[4] = {st.level, (st.skel ? 1 : 0) | (st.chol ? 2 : 0), st.cpd,
+                           (int32_t)st.blocks.size()};
     w.raw(sh, sizeof(sh));
     const long long asz = step_arena_doubles(st);
     w.pod<long long>(asz);
@@ -289,10 +292,12 @@ void load_factor(Engine& e, const char* path) {
       int32_t sh[4];
       rd.raw(sh, sizeof(sh));
       st.level = sh[0];
-      st.skel = sh[1] != 0;
+      st.skel = (sh[1] & 1) != 0;
+      st.chol = (sh[1] & 2) != 0;
       st.cpd = sh[2];
       const int nb = sh[3];
-      if (st.level < 0 || st.level >= e.L || (sh[1] != 0 && sh[1] != 1) || nb < 0 || nb > n3)
+      if (st.level < 0 || st.level >= e.L || sh[1] < 0 || sh[1] > 3 || nb < 0 || nb > n3 ||
+          (st.chol && !symmetric))
         io_fail("corrupt factor file: phase header");
       for (const StepData& o : e.steps)
         if (o.level == st.level && o.skel == st.skel) io_fail("corrupt factor file: repeated phase");

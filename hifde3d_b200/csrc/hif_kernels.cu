@@ -22,10 +22,33 @@
 #include <climits>
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
 
 namespace hif {
 
 namespace {
+
+// Kernel attributes are per device (cudaFuncSetAttribute acts on the current
+// device) and launchers run on several host threads at once (the serving
+// loop's factor workers): every one-time setting goes through this table,
+// keyed by (device, kernel), under one mutex.
+std::mutex g_attr_mu;
+std::map<std::pair<int, const void*>, size_t> g_attr_smem;
+
+// Raises `fn`'s dynamic shared-memory limit on the current device to at least
+// `bytes` (never lowers it).
+void ensure_smem(const void* fn, size_t bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  size_t& cur = g_attr_smem[{dev, fn}];
+  if (bytes > cur) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cur = bytes;
+  }
+}
 
 __device__ __forceinline__ int find_desc(const int* __restrict__ off, int nd, int t) {
   int lo = 0, hi = nd - 1;
@@ -89,68 +112,84 @@ __device__ __forceinline__ void resolve_cover(const GatherTarget& g, int p,
   }
 }
 
+// Persistent over the tile list: CTA b assembles the contiguous tiles
+// [b chunk, (b + 1) chunk), so the target of its first tile is found once by
+// binary search and the rest by stepping through tile_off (a per-tile search
+// costs ~log2(targets) dependent loads, more than a small tile's own work).
 __global__ void __launch_bounds__(256) k_gather(const GatherTarget* __restrict__ tg,
                                                 const int* __restrict__ tile_off, int ntg,
+                                                int total_tiles,
                                                 const SourceDesc* __restrict__ src,
                                                 const int* __restrict__ src_owner,
                                                 const int* __restrict__ dof_src,
                                                 const double* __restrict__ band,
                                                 long long ncell3, int NC) {
-  const int d = find_desc(tile_off, ntg, blockIdx.x);
-  const GatherTarget g = tg[d];
-  const int local = blockIdx.x - tile_off[d];
-  const int tiles_m = (g.m + kGT - 1) / kGT;
-  const int i0 = (local % tiles_m) * kGT, j0 = (local / tiles_m) * kGT;
-
+  const int chunk = (total_tiles + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * chunk, t1 = min(total_tiles, t0 + chunk);
+  if (t0 >= t1) return;
+  int d = find_desc(tile_off, ntg, t0);
+  int dbeg = tile_off[d], dend = tile_off[d + 1];
   __shared__ int s_row[kGT], s_col[kGT];
   __shared__ CoverEntry s_rc[kGT][kCover], s_cc[kGT][kCover];
-  for (int x = threadIdx.x; x < 2 * kGT; x += blockDim.x) {
-    if (x < kGT) {
-      const int i = i0 + x;
-      const int p = (i < g.m) ? g.rows[i] : -1;
-      s_row[x] = p;
-      resolve_cover(g, p, dof_src, src_owner, ncell3, s_rc[x]);
-    } else {
-      const int y = x - kGT, j = j0 + y;
-      const int q = (j < g.n) ? g.cols[j] : -1;
-      s_col[y] = q;
-      resolve_cover(g, q, dof_src, src_owner, ncell3, s_cc[y]);
+  for (int t = t0; t < t1; ++t) {
+    while (t >= dend) {
+      ++d;
+      dbeg = dend;
+      dend = tile_off[d + 1];
     }
-  }
-  __syncthreads();
-  const long long NC2 = (long long)NC * NC;
-  for (int e = threadIdx.x; e < kGT * kGT; e += blockDim.x) {
-    const int x = e % kGT, y = e / kGT;
-    const int i = i0 + x, j = j0 + y;
-    if (i >= g.m || j >= g.n) continue;
-    const long long p = s_row[x], q = s_col[y];
-    double v = 0.0;
-    if (!(i >= g.a0_skip && j >= g.a0_skip)) {
-      const long long dd = q - p;
-      int b = -1;
-      if (dd == 0) b = 0;
-      else if (dd == -1) b = 1;
-      else if (dd == 1) b = 2;
-      else if (dd == -NC) b = 3;
-      else if (dd == NC) b = 4;
-      else if (dd == -NC2) b = 5;
-      else if (dd == NC2) b = 6;
-      if (b >= 0) v = band[b * ncell3 + p];
-    }
-#pragma unroll
-    for (int a = 0; a < kCover; ++a) {
-      const int sa = s_rc[x][a].src;
-      if (sa < 0) continue;
-#pragma unroll
-      for (int c = 0; c < kCover; ++c) {
-        if (s_cc[y][c].src == sa) {
-          const SourceDesc sd = src[sa];
-          v += sd.ptr[(long long)s_rc[x][a].pos + (long long)s_cc[y][c].pos * sd.ld];
-        }
+    const GatherTarget g = tg[d];
+    const int local = t - dbeg;
+    const int tiles_m = (g.m + kGT - 1) / kGT;
+    const int i0 = (local % tiles_m) * kGT, j0 = (local / tiles_m) * kGT;
+    __syncthreads();  // the previous tile's readers of s_row / s_col / covers are done
+    for (int x = threadIdx.x; x < 2 * kGT; x += blockDim.x) {
+      if (x < kGT) {
+        const int i = i0 + x;
+        const int p = (i < g.m) ? g.rows[i] : -1;
+        s_row[x] = p;
+        resolve_cover(g, p, dof_src, src_owner, ncell3, s_rc[x]);
+      } else {
+        const int y = x - kGT, j = j0 + y;
+        const int q = (j < g.n) ? g.cols[j] : -1;
+        s_col[y] = q;
+        resolve_cover(g, q, dof_src, src_owner, ncell3, s_cc[y]);
       }
     }
-    g.out[i + (long long)j * g.ld] = v;
-    if (g.a22_out != nullptr && i < g.r && j < g.r) g.a22_out[i + (long long)j * g.r] = v;
+    __syncthreads();
+    const long long NC2 = (long long)NC * NC;
+    for (int e = threadIdx.x; e < kGT * kGT; e += blockDim.x) {
+      const int x = e % kGT, y = e / kGT;
+      const int i = i0 + x, j = j0 + y;
+      if (i >= g.m || j >= g.n) continue;
+      const long long p = s_row[x], q = s_col[y];
+      double v = 0.0;
+      if (!(i >= g.a0_skip && j >= g.a0_skip)) {
+        const long long dd = q - p;
+        int b = -1;
+        if (dd == 0) b = 0;
+        else if (dd == -1) b = 1;
+        else if (dd == 1) b = 2;
+        else if (dd == -NC) b = 3;
+        else if (dd == NC) b = 4;
+        else if (dd == -NC2) b = 5;
+        else if (dd == NC2) b = 6;
+        if (b >= 0) v = band[b * ncell3 + p];
+      }
+#pragma unroll
+      for (int a = 0; a < kCover; ++a) {
+        const int sa = s_rc[x][a].src;
+        if (sa < 0) continue;
+#pragma unroll
+        for (int c = 0; c < kCover; ++c) {
+          if (s_cc[y][c].src == sa) {
+            const SourceDesc sd = src[sa];
+            v += sd.ptr[(long long)s_rc[x][a].pos + (long long)s_cc[y][c].pos * sd.ld];
+          }
+        }
+      }
+      g.out[i + (long long)j * g.ld] = v;
+      if (g.a22_out != nullptr && i < g.r && j < g.r) g.a22_out[i + (long long)j * g.r] = v;
+    }
   }
 }
 
@@ -158,8 +197,11 @@ void launch_gather(const GatherTarget* d_tg, const int* d_tile_off, int ntg, int
                    const SourceDesc* d_src, const int* d_src_owner, const int* d_dof_src,
                    const double* d_band, long long ncell3, int NC, cudaStream_t s) {
   if (total_tiles <= 0) return;
-  k_gather<<<total_tiles, 256, 0, s>>>(d_tg, d_tile_off, ntg, d_src, d_src_owner, d_dof_src,
-                                       d_band, ncell3, NC);
+  // 8 resident CTAs of 256 threads per SM, 148 SMs, several waves' worth of
+  // chunks so that uneven tiles even out
+  const int grid = std::min(total_tiles, 148 * 8 * 4);
+  k_gather<<<grid, 256, 0, s>>>(d_tg, d_tile_off, ntg, total_tiles, d_src, d_src_owner,
+                                d_dof_src, d_band, ncell3, NC);
 }
 
 // ===========================================================================
@@ -421,11 +463,7 @@ void launch_dgemm(const GemmDesc* d_desc, const int* d_tile_off, int nd, int tot
                   cudaStream_t s, int tile) {
   if (total_tiles <= 0) return;
   if (tile == 128) {
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_dgemm128, cudaFuncAttributeMaxDynamicSharedMemorySize, kLSmemC);
-      attr = true;
-    }
+    ensure_smem((const void*)k_dgemm128, kLSmemC);
     k_dgemm128<<<total_tiles, 512, kLSmemC, s>>>(d_desc, d_tile_off, nd);
   } else {
     k_dgemm<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd);
@@ -799,11 +837,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const TcGemm* __restrict__ d
 void launch_gemm_tc(const TcGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
                     int* d_status, cudaStream_t s) {
   if (total_tiles <= 0) return;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
-    attr = true;
-  }
+  ensure_smem((const void*)k_gemm_tc, kTcSmem);
   k_gemm_tc<<<total_tiles, 256, kTcSmem, s>>>(d_desc, d_tile_off, nd, d_status);
 }
 
@@ -1119,12 +1153,7 @@ int oz_tile_n(int slices) { return slices <= 4 ? 128 : 64; }
 template <int S, int BN>
 static void launch_gemm_oz_t(const OzGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
                              int* d_status, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_gemm_oz<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         OzCfg<S, BN>::kSmem);
-    attr = true;
-  }
+  ensure_smem((const void*)k_gemm_oz<S, BN>, OzCfg<S, BN>::kSmem);
   k_gemm_oz<S, BN><<<total_tiles, 256, OzCfg<S, BN>::kSmem, s>>>(d_desc, d_tile_off, nd, d_status);
 }
 
@@ -1206,12 +1235,7 @@ void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_statu
                         cudaStream_t s) {
   if (nd <= 0) return;
   const size_t smem = (size_t)max_n * max_n * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_sweep_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kSmallSweepN * kSmallSweepN * (int)sizeof(double));
-    attr_set = true;
-  }
+  ensure_smem((const void*)k_sweep_small, kSmallSweepN * kSmallSweepN * sizeof(double));
   k_sweep_small<<<nd, 256, smem, s>>>(d_desc, d_status);
 }
 
@@ -1326,11 +1350,7 @@ void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, i
                        double* d_dinv, int* d_status, cudaStream_t s, int sym) {
   if (nact <= 0) return;
   const int smem = kSweepNB * kSweepNB * (int)sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
+  ensure_smem((const void*)k_sweep_diag, smem);
   k_sweep_diag<<<nact, 512, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status, sym);
 }
 
@@ -1351,6 +1371,255 @@ void launch_sweep_setdiag(const SweepDesc* d_desc, const int* d_active, int nact
                           const double* d_dinv, cudaStream_t s) {
   if (nact <= 0) return;
   k_sweep_setdiag<<<nact, 256, 0, s>>>(d_desc, d_active, k0, d_dinv);
+}
+
+// ===========================================================================
+// Cholesky elimination (symmetric positive definite interiors; the lower
+// triangle of every block is the one read and written).
+//   [A22 A12^T; A12 A11] = [L 0; Y^T I] [I 0; 0 S] [L^T Y; 0 I],
+//   A22 = L L^T, Y = L^{-1} A12^T, S = A11 - Y^T Y.
+// The factor keeps L (for F u), L^{-1} and Y (for F^{-1} u): in exact
+// arithmetic X = L^{-T} Y and A22^{-1} = L^{-T} L^{-1}, the reference's
+// Schur() outputs (include/Schur.hpp:72-100).
+// ===========================================================================
+
+// Small blocks whole in shared memory. Right-looking: for k < r, d = sqrt(S_kk),
+// column k below the diagonal / d, then S_ij -= S_ik S_jk for k < j <= i; after
+// r steps S[0:r, 0:r] = L, S[r:n, 0:r] = Y^T and S[r:n, r:n] = A11 - Y^T Y
+// (lower). L^{-1} then replaces L in place by Gauss-Jordan on the lower
+// triangle (entries above the diagonal stay zero under those steps).
+__global__ void __launch_bounds__(256) k_chol_small(const SweepDesc* __restrict__ descs,
+                                                    int* __restrict__ status) {
+  const SweepDesc d = descs[blockIdx.x];
+  const int n = d.n, r = d.r, s = n - r;
+  extern __shared__ double S[];  // n x n, ld n; lower triangle used
+  const int nn = n * n;
+  for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+    const int i = e % n, j = e / n;
+    S[e] = (i >= j) ? d.B[e] : 0.0;
+  }
+  __syncthreads();
+  __shared__ double s_d;
+  int bad = 0;
+  for (int k = 0; k < r; ++k) {
+    if (threadIdx.x == 0) {
+      const double p = S[k + k * n];
+      if (!(p > 1e-300) || !isfinite(p)) bad = 1;
+      s_d = sqrt(fabs(p) > 1e-300 ? fabs(p) : 1.0);
+    }
+    __syncthreads();
+    const double dk = s_d, idk = 1.0 / dk;
+    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) S[i + k * n] *= idk;
+    if (threadIdx.x == 0) S[k + k * n] = dk;
+    __syncthreads();
+    const int m = n - k - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int ii = e % m, jj = e / m;
+      if (ii < jj) continue;
+      const int i = k + 1 + ii, j = k + 1 + jj;
+      S[i + j * n] = fma(-S[i + k * n], S[j + k * n], S[i + j * n]);
+    }
+    __syncthreads();
+  }
+  // outputs: L (zeros above), Y = (S[r:n, 0:r])^T, Schur complement (mirrored)
+  for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
+    const int i = e % r, j = e / r;
+    d.L[e] = (i >= j) ? S[i + j * n] : 0.0;
+  }
+  for (int e = threadIdx.x; e < r * s; e += blockDim.x) {
+    const int i = e % r, j = e / r;
+    d.X[e] = S[(r + j) + i * n];
+  }
+  for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
+    const int i = e % s, j = e / s;
+    const int a = max(i, j), b = min(i, j);
+    d.B[(r + i) + (long long)(r + j) * n] = S[(r + a) + (r + b) * n];
+  }
+  __syncthreads();
+  // L^{-1} in place (lower triangle of S[0:r, 0:r])
+  for (int k = 0; k < r; ++k) {
+    const double ip = 1.0 / S[k + k * n];
+    for (int j = threadIdx.x; j < k; j += blockDim.x) S[k + j * n] *= ip;
+    __syncthreads();
+    const int m = r - k - 1;
+    for (int e = threadIdx.x; e < m * k; e += blockDim.x) {
+      const int i = k + 1 + e % m, j = e / m;
+      S[i + j * n] = fma(-S[i + k * n], S[k + j * n], S[i + j * n]);
+    }
+    __syncthreads();
+    for (int i = k + 1 + threadIdx.x; i < r; i += blockDim.x) S[i + k * n] *= -ip;
+    if (threadIdx.x == 0) S[k + k * n] = ip;
+    __syncthreads();
+  }
+  if (bad) atomicOr(status, kStatusTinyPivot);
+  for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
+    const int i = e % r, j = e / r;
+    d.a22inv[e] = (i >= j) ? S[i + j * n] : 0.0;
+  }
+}
+
+void launch_chol_small(const SweepDesc* d_desc, int nd, int max_n, int* d_status,
+                       cudaStream_t s) {
+  if (nd <= 0) return;
+  const size_t smem = (size_t)max_n * max_n * sizeof(double);
+  ensure_smem((const void*)k_chol_small, kSmallSweepN * kSmallSweepN * sizeof(double));
+  k_chol_small<<<nd, 256, smem, s>>>(d_desc, d_status);
+}
+
+// Pivot block of the blocked Cholesky, with the block in registers as in
+// k_sweep_diag (thread (tx, ty) of a 16 x 32 grid holds rows 4 ty.., columns
+// 8 tx..). The trailing part is kept symmetric (both triangles updated), so
+// column k is also row k: its owners publish it to shared memory (two
+// alternating buffers, one barrier per step). Step k: d = sqrt(a_kk),
+// l_i = a_ik / d; a_ij -= l_i l_j for i, j > k; column k = l (d on the
+// diagonal), row k right of the diagonal = 0. L goes back over B[K, K]; then
+// the same registers run the Gauss-Jordan inverse of L (lower triangular, so
+// its zeros stay zero) into dinv.
+__global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__ descs,
+                                                   const int* __restrict__ active, int k0,
+                                                   double* __restrict__ dinv,
+                                                   int* __restrict__ status) {
+  const int di = active[blockIdx.x];
+  const SweepDesc d = descs[di];
+  const int nb = min(kSweepNB, d.r - k0);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  __shared__ double colk[2][kSweepNB];
+  extern __shared__ double dg_sm[];  // kSweepNB x kSweepNB staging
+  for (int e = threadIdx.x; e < kSweepNB * kSweepNB; e += blockDim.x) {
+    const int i = e & (kSweepNB - 1), j = e / kSweepNB;
+    const int ii = i < j ? j : i, jj = i < j ? i : j;
+    dg_sm[e] = (i < nb && j < nb) ? d.B[(k0 + ii) + (long long)(k0 + jj) * d.n] : 0.0;
+  }
+  __syncthreads();
+  double a[4][8];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[r][c] = dg_sm[(4 * ty + r) + (8 * tx + c) * kSweepNB];
+  int bad = 0;
+  for (int k = 0; k < nb; ++k) {
+    const int buf = k & 1;
+    if (tx == (k >> 3)) {
+      const int kc = k & 7;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double v = a[r][0];
+#pragma unroll
+        for (int c = 1; c < 8; ++c)
+          if (c == kc) v = a[r][c];
+        colk[buf][4 * ty + r] = v;
+      }
+    }
+    __syncthreads();
+    const double p = colk[buf][k];
+    if (threadIdx.x == 0 && (!(p > 1e-300) || !isfinite(p))) bad = 1;
+    const double dk = sqrt(fabs(p) > 1e-300 ? fabs(p) : 1.0);
+    const double idk = 1.0 / dk;
+    double lj[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) lj[c] = colk[buf][8 * tx + c] * idk;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = 4 * ty + r;
+      const double li = colk[buf][i] * idk;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int j = 8 * tx + c;
+        if (i > k && j > k) a[r][c] = fma(-li, lj[c], a[r][c]);
+        else if (j == k && i >= k) a[r][c] = (i == k) ? dk : li;
+        else if (i == k && j > k) a[r][c] = 0.0;
+      }
+    }
+  }
+  if (bad) atomicOr(status, kStatusTinyPivot);
+  // L over B[K, K]
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) dg_sm[(4 * ty + r) + (8 * tx + c) * kSweepNB] = a[r][c];
+  __syncthreads();
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int i = e % nb, j = e / nb;
+    d.B[(k0 + i) + (long long)(k0 + j) * d.n] = dg_sm[i + j * kSweepNB];
+  }
+  // L^{-1} by the Gauss-Jordan steps of k_sweep_diag (pivots are the positive
+  // diagonal of L; padding beyond nb is never pivoted)
+  __shared__ double rowk[2][kSweepNB];
+  for (int k = 0; k < nb; ++k) {
+    const int buf = k & 1;
+    if (ty == (k >> 2)) {
+      const int kr = k & 3;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        double v = a[0][c];
+#pragma unroll
+        for (int r = 1; r < 4; ++r)
+          if (r == kr) v = a[r][c];
+        rowk[buf][8 * tx + c] = v;
+      }
+    }
+    if (tx == (k >> 3)) {
+      const int kc = k & 7;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double v = a[r][0];
+#pragma unroll
+        for (int c = 1; c < 8; ++c)
+          if (c == kc) v = a[r][c];
+        colk[buf][4 * ty + r] = v;
+      }
+    }
+    __syncthreads();
+    const double ip = 1.0 / rowk[buf][k];
+    double rj[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) rj[c] = rowk[buf][8 * tx + c] * ip;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const double cir = colk[buf][4 * ty + r];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) a[r][c] = fma(-cir, rj[c], a[r][c]);
+    }
+    if (ty == (k >> 2)) {
+      const int kr = k & 3;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (r == kr) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c) a[r][c] = rj[c];
+        }
+    }
+    if (tx == (k >> 3)) {
+      const int kc = k & 7;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c == kc) {
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            a[r][c] = (4 * ty + r == k) ? ip : colk[buf][4 * ty + r] * -ip;
+        }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) dg_sm[(4 * ty + r) + (8 * tx + c) * kSweepNB] = a[r][c];
+  __syncthreads();
+  double* out = dinv + (long long)di * kSweepNB * kSweepNB;
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int i = e % nb, j = e / nb;
+    out[e] = (i >= j) ? dg_sm[i + j * kSweepNB] : 0.0;
+  }
+}
+
+void launch_chol_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
+                      double* d_dinv, int* d_status, cudaStream_t s) {
+  if (nact <= 0) return;
+  const int smem = kSweepNB * kSweepNB * (int)sizeof(double);
+  ensure_smem((const void*)k_chol_diag, smem);
+  k_chol_diag<<<nact, 512, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
 }
 
 // ===========================================================================
@@ -1817,11 +2086,7 @@ cudaError_t launch_id_group(const IdGroupDesc* d_desc, int nd, int group, double
                             int* d_status, cudaStream_t s, int max_m, int max_n) {
   if (nd <= 0) return cudaSuccess;
   size_t smem = (size_t)std::max(max_m, 2 * max_n) * sizeof(double) + 64;
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    cudaFuncSetAttribute(k_id_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = smem;
-  }
+  if (smem > 48 * 1024) ensure_smem((const void*)k_id_group, smem);
   int grid = nd * group;
   if (group > 1) {
     // co-residency of the whole grid is required by the group barriers; the
@@ -1839,11 +2104,7 @@ void launch_id(const IdDesc* d_desc, int nd, int max_n, double eps, int* d_statu
   if (nd <= 0) return;
   const size_t smem = (size_t)max_n * 2 * sizeof(double) + 64 * sizeof(double) +
                       (size_t)max_n * 3 * sizeof(int) + 32 * sizeof(int);
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    cudaFuncSetAttribute(k_id, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = smem;
-  }
+  if (smem > 48 * 1024) ensure_smem((const void*)k_id, smem);
   k_id<<<nd, 512, smem, s>>>(d_desc, eps, d_status);
 }
 
@@ -2207,10 +2468,15 @@ void launch_qr_panel(const QrDesc* d_desc, const int* d_active, int nact, int k1
 }
 
 int qr_cluster_max_rows() {
-  static int cap = -1;
+  // per device: the attributes and the cluster occupancy belong to the device
+  static std::mutex mu;
+  static std::map<int, int> caps;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  int& cap = caps.emplace(dev, -1).first->second;
   if (cap < 0) {
-    cudaFuncSetAttribute(k_qr_panel_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (kQrcRows + 1) * kQrNB * 8);
+    ensure_smem((const void*)k_qr_panel_cluster, (kQrcRows + 1) * kQrNB * 8);
     cudaFuncSetAttribute(k_qr_panel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     // the largest cluster the device can place with this kernel's footprint
     int best = 1;
@@ -2280,12 +2546,7 @@ __global__ void __launch_bounds__(256) k_qr_tfactor(const TFactorDesc* __restric
 
 void launch_qr_tfactor(const TFactorDesc* d_desc, int nd, cudaStream_t s) {
   if (nd <= 0) return;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_qr_tfactor, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kQrNB2 * kQrNB2 * 8);
-    attr = true;
-  }
+  ensure_smem((const void*)k_qr_tfactor, kQrNB2 * kQrNB2 * 8);
   k_qr_tfactor<<<nd, 256, kQrNB2 * kQrNB2 * 8, s>>>(d_desc);
 }
 
@@ -2432,11 +2693,7 @@ void launch_pchol_panel(const PcholDesc* d_desc, const int* d_active, int nact, 
                         double eps, int max_n, int* d_status, cudaStream_t s) {
   if (nact <= 0) return;
   const size_t smem = (size_t)max_n * (sizeof(double) + sizeof(int));
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    cudaFuncSetAttribute(k_pchol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = smem;
-  }
+  if (smem > 48 * 1024) ensure_smem((const void*)k_pchol_panel, smem);
   k_pchol_panel<<<nact, 512, smem, s>>>(d_desc, d_active, i0, nb, eps, d_status);
 }
 
@@ -2478,11 +2735,7 @@ __global__ void __launch_bounds__(512) k_pchol_finish(const PcholDesc* __restric
 void launch_pchol_finish(const PcholDesc* d_desc, int nd, int max_n, cudaStream_t s) {
   if (nd <= 0) return;
   const size_t smem = (size_t)max_n * sizeof(int);
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    cudaFuncSetAttribute(k_pchol_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = smem;
-  }
+  if (smem > 48 * 1024) ensure_smem((const void*)k_pchol_finish, smem);
   k_pchol_finish<<<nd, 512, smem, s>>>(d_desc);
 }
 
@@ -2520,11 +2773,7 @@ void launch_trsm_block(const TrsmBlockDesc* d_desc, int nd, int max_cols, cudaSt
   if (nd <= 0 || max_cols <= 0) return;
   const int chunks = (max_cols + 127) / 128;
   const int smem = (kTrsmNB * kTrsmNB + kTrsmNB * 128) * (int)sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_trsm_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
+  ensure_smem((const void*)k_trsm_block, smem);
   k_trsm_block<<<nd * chunks, 128, smem, s>>>(d_desc, chunks);
 }
 
@@ -2613,8 +2862,10 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
     for (int c0 = 0; c0 < nrhs; c0 += kRhsGroup) {
       const int nc = min(kRhsGroup, nrhs - c0);
       double acc[kRhsGroup] = {0.0, 0.0, 0.0, 0.0};
-      for (int j0 = 0; j0 < g.n; j0 += kXChunk) {
-        const int nj = min(kXChunk, g.n - j0);
+      // lower triangular: this strip's rows need no column right of its last row
+      const int jend = g.tri ? min(g.n, (local + 1) * 256) : g.n;
+      for (int j0 = 0; j0 < jend; j0 += kXChunk) {
+        const int nj = min(kXChunk, jend - j0);
         __syncthreads();
         for (int e = tid; e < nj * kRhsGroup; e += 256) {
           const int jj = e / kRhsGroup, cc = e % kRhsGroup;
@@ -2642,7 +2893,9 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
       for (int q = 0; q < 4; ++q)
 #pragma unroll
         for (int cc = 0; cc < kRhsGroup; ++cc) acc[q][cc] = 0.0;
-      for (int i0 = 0; i0 < g.m; i0 += kXChunk) {
+      // lower triangular: these columns have no entry above their first column
+      const int ibeg = g.tri ? ((local * 32) / kXChunk) * kXChunk : 0;
+      for (int i0 = ibeg; i0 < g.m; i0 += kXChunk) {
         const int ni = min(kXChunk, g.m - i0);
         __syncthreads();
         for (int e = tid; e < ni * kRhsGroup; e += 256) {

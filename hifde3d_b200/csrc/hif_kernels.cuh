@@ -68,11 +68,16 @@ struct GemmDesc {
 };
 
 // Dense elimination block: B (n x n, ld n) in assembly order [red | skel].
+// Gauss-Jordan: a22inv = A22^{-1}, X = A22^{-1} A21. Cholesky (symmetric
+// positive definite A22): L = chol(A22) (lower, zeros above), a22inv = L^{-1}
+// (lower), X = Y = L^{-1} A21; in both the skeleton block ends as
+// A11 - A12 A22^{-1} A21 in B.
 struct SweepDesc {
   double* B;
   double* a22inv;  // r x r, ld r  (compact copy written at the end)
   double* X;       // r x s, ld r
   int n, r;
+  double* L;       // Cholesky only: r x r, ld r
 };
 
 // Interpolative decomposition of M (m x n, ld m) for one face.
@@ -159,6 +164,7 @@ struct GemvDesc {
   double* contrib;      // mode 1: contribution slots (length = rows of op(M))
   int m, n;             // M is m x n
   int trans;            // 0: y = M x (len m), 1: y = M^T x (len n)
+  int tri;              // 1: M is lower triangular (square); entries above the diagonal are not read
   double alpha;
   int mode;             // 0: u_out[out] += alpha y; 1: contrib = y; 2: u_out[out] = alpha y
   // Optional per-descriptor vectors (batched solves of several operators in one
@@ -318,6 +324,16 @@ void launch_sweep_small(const SweepDesc* d_desc, int nd, int max_n, int* d_statu
 constexpr int kSweepNB = 128;
 void launch_sweep_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
                        double* d_dinv, int* d_status, cudaStream_t s, int sym = 0);
+// Cholesky elimination of symmetric positive definite interiors (lower
+// triangles only). Small blocks whole in shared memory: L, L^{-1}, Y and the
+// Schur complement in one launch.
+void launch_chol_small(const SweepDesc* d_desc, int nd, int max_n, int* d_status,
+                       cudaStream_t s);
+// Pivot block K = [k0, k0 + 128) of the blocked factorization: L_KK = chol(B[K, K])
+// written over B[K, K] (zeros above its diagonal) and L_KK^{-1} (lower, zeros
+// above) into dinv (128 x 128 per active block, ld = its width).
+void launch_chol_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
+                      double* d_dinv, int* d_status, cudaStream_t s);
 void launch_sweep_setdiag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
                           const double* d_dinv, cudaStream_t s);
 

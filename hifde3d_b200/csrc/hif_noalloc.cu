@@ -15,6 +15,13 @@
 //     it and must be serialised by the caller;
 //   * the first call on a device looks the array's address up once, with that
 //     device current; that first call should come before any stream capture.
+//     The address is kept for the life of the process, so the library must not
+//     be used on a device after cudaDeviceReset has torn its context down;
+//   * every call ends by copying the pivot status word to the host and
+//     synchronising its stream: it returns after its kernels have finished;
+//   * the kernels favour simplicity over speed (the panel kernels keep a 64-entry
+//     row or column per thread and read the pivot-block inverse from global
+//     memory); the results are those of hif_schur_device within rounding.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -173,12 +180,17 @@ int fail(int code, const char* msg) {
 
 extern "C" int hif_schur_device_noalloc(const double* dB, int n, int r, double* dA22inv,
                                         double* dX, double* dS, void* stream) {
-  if (!dB || n < 1 || r < 0 || r > n) return fail(HIF_ERR_ARG, "hif_schur_device_noalloc: bad block");
+  // the same argument and device checks as hif_schur_device, in the same order
+  if (!dB || n < 0 || r < 0 || r > n) return fail(HIF_ERR_ARG, "hif_schur_device_noalloc: bad block");
   if (n > kNoAllocMaxN)
     return fail(HIF_ERR_ARG, "hif_schur_device_noalloc: block larger than 512 DOFs "
                              "(the fixed scratch size); use hif_schur_device");
   if ((r > 0 && !dA22inv) || (r > 0 && r < n && !dX) || (r < n && !dS))
     return fail(HIF_ERR_ARG, "hif_schur_device_noalloc: missing output");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(HIF_ERR_NODEVICE, "no CUDA device");
+  if (n == 0) return HIF_OK;  // an empty block: nothing to eliminate or write
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(HIF_ERR_NODEVICE, "hif_schur_device_noalloc: no current CUDA device");

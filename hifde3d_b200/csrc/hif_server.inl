@@ -51,7 +51,8 @@ class Server {
     int status = -1;
     int iters = 0;
     double relres = 0;
-    double t_submit = 0, t_done = 0;
+    double t_submit = 0, t_start = 0, t_done = 0;  // t_start: admitted (factor
+                                                    // worker / active solve set)
     bool done = false;
     std::string err;
   };
@@ -105,7 +106,8 @@ class Server {
   }
 
   // Blocks until the request completes; the request record is dropped.
-  void wait(long long id, int* status, int* iters, double* relres, double* latency_ms) {
+  void wait(long long id, int* status, int* iters, double* relres, double* latency_ms,
+            double* queue_ms = nullptr) {
     std::unique_lock<std::mutex> lk(mu_);
     auto it = reqs_.find(id);
     if (it == reqs_.end()) throw Error{HIF_ERR_ARG, "unknown request"};
@@ -115,6 +117,7 @@ class Server {
     if (iters) *iters = r->iters;
     if (relres) *relres = r->relres;
     if (latency_ms) *latency_ms = 1e3 * (r->t_done - r->t_submit);
+    if (queue_ms) *queue_ms = 1e3 * ((r->t_start > 0 ? r->t_start : r->t_done) - r->t_submit);
     const std::string err = r->err;
     reqs_.erase(it);
     if (!err.empty()) g_last_error = err;
@@ -161,6 +164,12 @@ class Server {
     return (long long)(dofs * 12.0 * 1024.0) + (256LL << 20);
   }
 
+  // Device bytes of one active solve: x r z p q ua ub uc and the contribution
+  // slots (the scalars are negligible).
+  static long long solve_bytes(const Engine& e, int nrhs) {
+    return 8LL * (8 * e.n3 * nrhs + e.contrib_ld * nrhs);
+  }
+
   void finish(Req* r, int status, const std::string& err) {
     r->status = status;
     r->err = err;
@@ -178,15 +187,33 @@ class Server {
       long long need = 0;
       {
         std::unique_lock<std::mutex> lk(mu_);
+        // the head request waits until its estimate fits beside what is
+        // resident and running; one whose estimate exceeds the whole budget
+        // can never fit and is refused
         cv_.wait(lk, [&] {
           if (stop_) return true;
           if (fq_.empty()) return false;
           need = estimate_bytes(fq_.front()->N);
-          return used_ + need <= budget_ || (used_ == 0);
+          return need > budget_ || used_ + need <= budget_;
         });
         if (stop_) return;
         r = fq_.front();
         fq_.pop_front();
+        r->t_start = wall();
+        if (need > budget_) {
+          Op& o = ops_[r->op];
+          o.state = 2;
+          o.err = "factorization needs an estimated " + std::to_string(need >> 20) +
+                  " MiB, more than the server's budget of " + std::to_string(budget_ >> 20) +
+                  " MiB";
+          r->ax.clear();
+          r->ay.clear();
+          r->az.clear();
+          r->V.clear();
+          finish(r, HIF_ERR_BUDGET, o.err);
+          cv_.notify_all();
+          continue;
+        }
         used_ += need;
       }
       std::unique_ptr<Engine> e;
@@ -255,8 +282,8 @@ class Server {
     Engine* e;
     int nrhs;
     long long n3;
-    double* mem = nullptr;  // x r z p q ua ub | contrib | scalars
-    double *x, *rv, *z, *p, *q, *ua, *ub, *contrib, *sc;
+    double* mem = nullptr;  // x r z p q ua ub uc | contrib | scalars
+    double *x, *rv, *z, *p, *q, *ua, *ub, *uc, *contrib, *sc;
     int it = 0;
     bool fresh = true;
     std::vector<double> bb, relres;
@@ -280,7 +307,7 @@ class Server {
     a.nrhs = a.r->nrhs;
     const long long nv = a.n3 * a.nrhs;
     const long long cl = e.contrib_ld;
-    const long long tot = 7 * nv + cl * a.nrhs + 8LL * a.nrhs + (long long)kDotBlocks * a.nrhs;
+    const long long tot = 8 * nv + cl * a.nrhs + 8LL * a.nrhs + (long long)kDotBlocks * a.nrhs;
     a.mem = a.bufs.add(dalloc<double>(tot, sstream_));
     a.x = a.mem;
     a.rv = a.x + nv;
@@ -289,12 +316,13 @@ class Server {
     a.q = a.p + nv;
     a.ua = a.q + nv;
     a.ub = a.ua + nv;
-    a.contrib = a.ub + nv;
+    a.uc = a.ub + nv;
+    a.contrib = a.uc + nv;
     a.sc = a.contrib + cl * a.nrhs;
     HIF_CK(cudaMemcpyAsync(a.rv, a.r->b.data(), nv * 8, cudaMemcpyHostToDevice, sstream_));
     a.r->b.clear();
     // bind the operator's inverse-apply plan to this request's vectors
-    double* vec[2] = {a.ua, a.ub};
+    double* vec[3] = {a.ua, a.ub, a.uc};
     for (const ApplyLaunch& l : e.plan_inv.launches) {
       Active::L x{};
       x.key = l.key;
@@ -407,10 +435,11 @@ class Server {
             it = sq_.erase(it);
             continue;
           }
-          const long long need = 8LL * (7 * o.e->n3 * r->nrhs + o.e->contrib_ld * r->nrhs);
+          const long long need = solve_bytes(*o.e, r->nrhs);
           if (used_ + need > budget_ && !act.empty()) break;
           used_ += need;
           o.active += 1;
+          r->t_start = wall();
           auto a = std::unique_ptr<Active>(new Active());
           a->r = r;
           try {
@@ -434,7 +463,7 @@ class Server {
         std::lock_guard<std::mutex> lk(mu_);
         for (auto& a : act) {
           ops_[a->r->op].active -= 1;
-          used_ -= 8LL * (7 * a->n3 * a->nrhs + a->e->contrib_ld * a->nrhs);
+          used_ -= solve_bytes(*a->e, a->nrhs);
           a->bufs.release(sstream_);
           finish(a->r, x.code, x.msg);
         }
@@ -528,7 +557,7 @@ class Server {
       for (Active* a : retire) {
         Op& o = ops_[a->r->op];
         o.active -= 1;
-        used_ -= 8LL * (7 * a->n3 * a->nrhs + a->e->contrib_ld * a->nrhs);
+        used_ -= solve_bytes(*a->e, a->nrhs);
         a->bufs.release(sstream_);
         finish(a->r, HIF_OK, "");
       }
@@ -634,6 +663,12 @@ int hif_server_wait(hif_server s, long long request_id, int* status, int* iters,
                     double* latency_ms) {
   if (!s) return HIF_ERR_ARG;
   return guarded([&] { s->s->wait(request_id, status, iters, relres, latency_ms); });
+}
+
+int hif_server_wait_detail(hif_server s, long long request_id, int* status, int* iters,
+                           double* relres, double* latency_ms, double* queue_ms) {
+  if (!s) return HIF_ERR_ARG;
+  return guarded([&] { s->s->wait(request_id, status, iters, relres, latency_ms, queue_ms); });
 }
 
 int hif_server_release(hif_server s, int op_id) {

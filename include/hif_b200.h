@@ -134,12 +134,14 @@ int hif_schur_device(const double* dB, int n, int r, double* dA22inv, double* dX
  * its own kernels. All scratch lives in one fixed device array inside the library
  * (about 2 MiB per GPU, held from library load until process exit), so blocks are limited
  * to n <= 512 (larger ones return HIF_ERR_ARG). Inputs and outputs are the caller's
- * device buffers; work is queued on `stream` (a cudaStream_t, NULL = legacy default)
- * and the call waits for it to read the pivot status. Every call on a device shares the
+ * device buffers; work is queued on `stream` (a cudaStream_t, NULL = legacy default).
+ * Every call ends by copying the pivot status to the host and synchronising `stream`,
+ * so it returns only after its kernels have finished. Every call on a device shares the
  * scratch array: calls whose kernels may overlap on the GPU race and must be
  * serialised by the caller. The first call on a device looks up the array's device
  * address with that device current; make that first call before any stream
- * capture begins. */
+ * capture begins. The address is kept for the process's life: do not use the library
+ * on a device after cudaDeviceReset. n = 0 is a no-op returning HIF_OK. */
 int hif_schur_device_noalloc(const double* dB, int n, int r, double* dA22inv, double* dX,
                              double* dS, void* stream);
 /* InterpDecomp(M, W, skel, red, eps) -- src/InterpDecomp.cpp:86-138: column-pivoted
@@ -169,11 +171,18 @@ int hif_block_info(hif_handle h, int level, int kind, int b, int* ng, int* nr, i
 int hif_block_indices(hif_handle h, int level, int kind, int b, int* global_inds,
                       int* redundant_inds, int* skeleton_inds);
 /* which: 0 A_22, 1 A_22^{-1}, 2 X = A_22^{-1} A_21, 3 W (skeletonization only),
- * 4 Schur complement S (only with HIF_OPT_KEEP_SCHUR). Column-major, rows / columns
+ * 4 Schur complement S (only with HIF_OPT_KEEP_SCHUR); for phases eliminated by
+ * Cholesky (HIF_OPT_ELIMINATION) 0-2 are formed from the stored factors and
+ * 5 L, 6 L^{-1}, 7 Y = L^{-1} A_21 are the stored ones. Column-major, rows / columns
  * ordered as redundant_inds / skeleton_inds. */
 int hif_block_matrix(hif_handle h, int level, int kind, int b, int which, double* out);
 /* Pivot order (0-based, n entries) and R diagonal of a skeletonized face's ID. */
 int hif_block_pivots(hif_handle h, int level, int b, int* jpvt, double* rdiag);
+/* For every DOF id p in [0, NC^3): the phase that eliminated it, 2 * level + kind
+ * (kind 0 = Schur, 1 = skeletonization), or -1 for the index-0 planes. The union of
+ * the redundant_inds of every block (UpdateRemainingDOFs, src/Factor.cpp:91-111);
+ * used to state errors per level. */
+int hif_dof_levels(hif_handle h, int* phase_of_dof);
 
 enum hif_option {
   HIF_OPT_KEEP_SCHUR = 1,    /* keep every Schur complement for hif_block_matrix(which=4) */
@@ -189,15 +198,28 @@ enum hif_option {
                                  differ in the last bits between those factorizations */
   HIF_OPT_SCHUR_SLICES = 8,   /* MIXED: int8 slices (2..8) of the Schur-complement products
                                  S = A11 - A12 X (default 5); 0: split TF32 */
-  HIF_OPT_X_SLICES = 9        /* MIXED: int8 slices (2..8) of X = A22^{-1} A21 (default 7);
-                                 0: FP64 */
+  HIF_OPT_X_SLICES = 9,       /* MIXED, Gauss-Jordan elimination: int8 slices (2..8) of
+                                 X = A22^{-1} A21 (default 7); 0: FP64 */
+  HIF_OPT_ELIMINATION = 10,   /* enum hif_elimination (default HIF_ELIM_AUTO) */
+  HIF_OPT_Y_SLICES = 11       /* MIXED, Cholesky elimination: int8 slices (2..8) of
+                                 Y = L^{-1} A21 (default 6); 0: FP64 */
 };
-/* Arithmetic of the factorization. MIXED: the Schur complements S = A11 - A12 X of the
- * eliminations run on the tcgen05 tensor cores as split-TF32 products with FP64
- * accumulation every 256 terms; the interpolative decompositions of the large faces
- * use the pivoted Cholesky of M^T M (FP64) instead of the column-pivoted QR; A22^{-1},
- * X, the factor storage, the apply and the PCG residual stay FP64. */
+/* Arithmetic of the factorization. MIXED: the long-K products of the eliminations
+ * (S = A11 - A12 X, and X or Y) are FP64 products formed from exact int8 slice
+ * products on the tcgen05 tensor cores (HIF_OPT_SCHUR_SLICES 0 selects split TF32 for
+ * S); the interpolative decompositions of the large faces use the pivoted Cholesky of
+ * M^T M (FP64) instead of the column-pivoted QR when epsilon >= 1e-7; the diagonal-block
+ * factorization, the factor storage, the apply and the PCG residual stay FP64. */
 enum hif_precision { HIF_PRECISION_FP64 = 0, HIF_PRECISION_MIXED = 1 };
+/* Elimination of the redundant DOFs of each block.
+ * GAUSS_JORDAN: explicit A22^{-1}, X = A22^{-1} A21, S = A11 - A12 X (the reference's
+ *   Schur(): getrf + getri, include/Schur.hpp:72-100).
+ * CHOLESKY (symmetric operators, hif_setup_stencil_faces): A22 = L L^T,
+ *   Y = L^{-1} A21, S = A11 - Y^T Y; the factor keeps L, L^{-1} and Y. Same operator
+ *   to rounding (X = L^{-T} Y, A22^{-1} = L^{-T} L^{-1}); hif_block_matrix still
+ *   returns A22, A22^{-1} and X, formed from them.
+ * AUTO: CHOLESKY for symmetric operators in MIXED precision, else GAUSS_JORDAN. */
+enum hif_elimination { HIF_ELIM_AUTO = 0, HIF_ELIM_GAUSS_JORDAN = 1, HIF_ELIM_CHOLESKY = 2 };
 int hif_set_option(hif_handle h, int option, long long value);
 
 /* Test hook: prescribe the ID column order of every face of one level (replay of
@@ -288,7 +310,9 @@ int hif_gemm_int8_device(int transA, int transB, int m, int n, int k, double alp
  * runs requests from any host thread:
  *   - factor requests (face-coefficient operator, as hif_setup_stencil_faces) run on
  *     worker threads, each on its operator's own stream; one is admitted when its
- *     expected device footprint fits in budget_bytes beside the resident factors;
+ *     expected device footprint fits in budget_bytes beside the resident factors and
+ *     the factorizations running; one whose expected footprint exceeds budget_bytes
+ *     itself is refused with HIF_ERR_BUDGET (and so are the solves submitted for it);
  *   - solve requests (PCG preconditioned by the inverse apply, as hif_solve_pcg)
  *     are batched across operators at every iteration: up to max_active_solves run
  *     together, one launch per apply stage for all of them; requests join and
@@ -312,6 +336,12 @@ int hif_server_submit_solve(hif_server s, int op_id, const double* b, int nrhs, 
  * right-hand sides; latency_ms: submit to completion. */
 int hif_server_wait(hif_server s, long long request_id, int* status, int* iters,
                     double* relres, double* latency_ms);
+/* hif_server_wait plus queue_ms: submit until the request was admitted (a factor
+ * request by the memory budget and a free worker; a solve into the active set, which
+ * needs its operator factored, a free slot and memory); latency_ms - queue_ms is the
+ * time in service. */
+int hif_server_wait_detail(hif_server s, long long request_id, int* status, int* iters,
+                           double* relres, double* latency_ms, double* queue_ms);
 /* Waits for the operator's solves in flight, then frees its factor. */
 int hif_server_release(hif_server s, int op_id);
 int hif_server_stats(hif_server s, long long* device_bytes, long long* resident_ops,

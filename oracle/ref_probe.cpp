@@ -11,10 +11,24 @@
 //       clears it, src/Factor.cpp:293) and W; then Apply(u,false), Apply(u,true)
 //       (src/Factor.cpp:992-1081) and the driver's e_a / e_s check
 //       (tests/HIFDE3D/main.cpp:88-134) on the v = 1 vector.
+//   dumpf <N> <P> <eps> <ax.bin> <ay.bin> <az.bin> <V.bin> <u.bin> <out.bin>
+//       dump on the face-coefficient operator (see timef).
 //   time <N> <P> <eps> <max_levels> [A.bin V.bin]
 //       Wall-clocks SetupStencil, each level's Schur / skeletonization / update
 //       phase and one inverse Apply; prints one JSON object. max_levels < 0
-//       runs the whole factorization.
+//       runs the whole factorization. Each level's times are also written to
+//       stderr as a "LEVEL {...}" line (flushed) the moment the level ends, so
+//       that a run stopped by a wall-clock cap still records the levels it
+//       reached.
+//   timef <N> <P> <eps> <max_levels> <ax.bin> <ay.bin> <az.bin> <V.bin>
+//       The same timings on the symmetric face-coefficient operator
+//       -div(a grad u) + V u: the reference factors whatever its sparse matrix
+//       holds, so the probe fills sp_matrix() through the reference's own
+//       Sparse::Add (include/hifde3d/core/sparse.hpp:34), one row per DOF as
+//       SetupStencil does (include/setup_stencil.hpp:17-70), with diagonal
+//       V + sum of the six face coefficients / h^2 and -a_face / h^2 for each
+//       interior neighbour. ax(i,j,k) couples nodes (i,j,k) and (i+1,j,k), ay
+//       and az likewise; all four arrays are (NC+1)^3, i fastest.
 //
 // Input tensors are (NC+1)^3 float64 arrays in the reference's NumTns order
 // (i fastest, include/numtns.hpp:99); u is NC^3 float64 in the DOF order
@@ -115,15 +129,55 @@ void setup(HIFFactor<double>& f, int NC, NumTns<double>& A, NumTns<double>& V,
     SetupStencil(f, NC - 1, 1.0 / NC, A, V);
 }
 
-int mode_dump(int argc, char** argv) {
-    if (argc != 9) return 2;
+// Face-coefficient operator into the reference's sparse matrix (see timef).
+void setup_faces(HIFFactor<double>& f, int NC, const char* fax, const char* fay,
+                 const char* faz, const char* fv) {
+    const size_t nt = (size_t)(NC + 1) * (NC + 1) * (NC + 1);
+    std::vector<double> ax = read_doubles(fax, nt), ay = read_doubles(fay, nt),
+                        az = read_doubles(faz, nt), vv = read_doubles(fv, nt);
+    const int N = NC - 1, T = NC + 1;
+    const double h = 1.0 / NC, hh = h * h;
+    auto at = [T](const std::vector<double>& a, int i, int j, int k) {
+        return a[i + (size_t)T * (j + (size_t)T * k)];
+    };
+    Sparse<double>& matrix = f.sp_matrix();
+    for (int i = 1; i <= N; ++i)
+        for (int j = 1; j <= N; ++j)
+            for (int k = 1; k <= N; ++k) {
+                const double w[6] = {at(ax, i - 1, j, k), at(ax, i, j, k), at(ay, i, j - 1, k),
+                                     at(ay, i, j, k),     at(az, i, j, k - 1), at(az, i, j, k)};
+                const int nb[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k},
+                                      {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
+                Vector<int> jidx;
+                Vector<double> vals;
+                double d = at(vv, i, j, k);
+                for (int q = 0; q < 6; ++q) d += w[q] / hh;
+                jidx.PushBack(f.Tensor2LinearInd(Index3(i, j, k)));
+                vals.PushBack(d);
+                for (int q = 0; q < 6; ++q) {
+                    const int a = nb[q][0], b = nb[q][1], c = nb[q][2];
+                    if (a < 1 || a > N || b < 1 || b > N || c < 1 || c > N) continue;
+                    jidx.PushBack(f.Tensor2LinearInd(Index3(a, b, c)));
+                    vals.PushBack(-w[q] / hh);
+                }
+                matrix.Add(f.Tensor2LinearInd(Index3(i, j, k)), jidx, vals);
+            }
+}
+
+int mode_dump(int argc, char** argv, bool faces) {
+    if (argc != (faces ? 11 : 9)) return 2;
     int N = std::atoi(argv[2]), P = std::atoi(argv[3]);
     double eps = std::atof(argv[4]);
     HIFFactor<double> f(N, P, eps);
     int NC = N + 1;
     NumTns<double> A(NC + 1, NC + 1, NC + 1), V(NC + 1, NC + 1, NC + 1);
-    setup(f, NC, A, V, argv[5], argv[6]);
-    std::vector<double> u0 = read_doubles(argv[7], (size_t)NC * NC * NC);
+    if (faces)
+        setup_faces(f, NC, argv[5], argv[6], argv[7], argv[8]);
+    else
+        setup(f, NC, A, V, argv[5], argv[6]);
+    const char* u_path = argv[faces ? 9 : 7];
+    const char* out_path = argv[faces ? 10 : 8];
+    std::vector<double> u0 = read_doubles(u_path, (size_t)NC * NC * NC);
 
     // Driver check vector (tests/HIFDE3D/main.cpp:88-103): v = 1 on DOFs.
     Vector<double> v(NC * NC * NC), w(NC * NC * NC);
@@ -136,7 +190,7 @@ int mode_dump(int argc, char** argv) {
     for (int t = 0; t < NC * NC * NC; ++t) uvec.Set(t, u0[t]);
     SpMV(f.sp_matrix(), uvec, Au);
 
-    Out o{std::fopen(argv[8], "wb")};
+    Out o{std::fopen(out_path, "wb")};
     if (!o.f) return 2;
     std::fwrite("HIFG", 1, 4, o.f);
     o.i32(1);
@@ -175,8 +229,8 @@ int mode_dump(int argc, char** argv) {
     return 0;
 }
 
-int mode_time(int argc, char** argv) {
-    if (argc != 6 && argc != 8) return 2;
+int mode_time(int argc, char** argv, bool faces) {
+    if (faces ? argc != 10 : (argc != 6 && argc != 8)) return 2;
     int N = std::atoi(argv[2]), P = std::atoi(argv[3]);
     double eps = std::atof(argv[4]);
     int max_levels = std::atoi(argv[5]);
@@ -184,7 +238,10 @@ int mode_time(int argc, char** argv) {
     int NC = N + 1;
     NumTns<double> A(NC + 1, NC + 1, NC + 1), V(NC + 1, NC + 1, NC + 1);
     double t0 = now();
-    setup(f, NC, A, V, argc == 8 ? argv[6] : nullptr, argc == 8 ? argv[7] : nullptr);
+    if (faces)
+        setup_faces(f, NC, argv[6], argv[7], argv[8], argv[9]);
+    else
+        setup(f, NC, A, V, argc == 8 ? argv[6] : nullptr, argc == 8 ? argv[7] : nullptr);
     double t_setup = now() - t0;
     f.Initialize();
     int L = (int)f.schur_level_data_.size();
@@ -209,8 +266,12 @@ int mode_time(int argc, char** argv) {
             ku = now() - e;
         }
         t_schur += b - a; t_upd += (c - b) + ku; t_skel += ks;
-        lv << (level ? "," : "") << "{\"level\":" << level << ",\"schur_s\":" << (b - a)
-           << ",\"skel_s\":" << ks << ",\"update_s\":" << (c - b) + ku << "}";
+        std::ostringstream one;
+        one << "{\"level\":" << level << ",\"schur_s\":" << (b - a) << ",\"skel_s\":" << ks
+            << ",\"update_s\":" << (c - b) + ku << ",\"elapsed_s\":" << now() - tf << "}";
+        lv << (level ? "," : "") << one.str();
+        std::fprintf(stderr, "LEVEL %s\n", one.str().c_str());
+        std::fflush(stderr);
     }
     double t_factor = now() - tf;
     double t_apply = -1;
@@ -237,7 +298,9 @@ int main(int argc, char** argv) {
     std::cout.rdbuf(std::cerr.rdbuf());
     if (argc < 2) return 2;
     std::string m = argv[1];
-    if (m == "dump") return mode_dump(argc, argv);
-    if (m == "time") return mode_time(argc, argv);
+    if (m == "dump") return mode_dump(argc, argv, false);
+    if (m == "dumpf") return mode_dump(argc, argv, true);
+    if (m == "time") return mode_time(argc, argv, false);
+    if (m == "timef") return mode_time(argc, argv, true);
     return 2;
 }

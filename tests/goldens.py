@@ -34,11 +34,36 @@ def blocks(g: dict, level: int, kind: str):
                g[pre + "s"][so[b]:so[b + 1]].astype(np.int64))
 
 
+def is_compact(g: dict) -> bool:
+    return str(g["full"]) == "compact"
+
+
+def compact_matrices(g: dict, level: int, kind: str, name: str):
+    """Per block of a compact fixture: (shape, ||M||_F, zr^T M zc)."""
+    pre = f"L{level}_{kind}_"
+    return [(tuple(int(x) for x in sh), float(fr), float(bl))
+            for sh, fr, bl in zip(g[pre + name + "_shape"], g[pre + name + "_fro"],
+                                  g[pre + name + "_bil"])]
+
+
+def bilinear_error(M: np.ndarray, fro: float, bil: float) -> float:
+    """Distance of M from a compact fixture's (||M||_F, zr^T M zc), relative to
+    ||M||_F (the bilinear form scaled by the probe vectors' norms)."""
+    r, c = M.shape
+    zr, zc = probe_vector(r, 1.1), probe_vector(c, 0.3)
+    scale = max(fro, 1e-300)
+    e_fro = abs(float(np.linalg.norm(M)) - fro) / scale
+    e_bil = abs(float(zr @ (M @ zc)) - bil) / (scale * np.linalg.norm(zr) * np.linalg.norm(zc))
+    return max(e_fro, e_bil)
+
+
 def matrices(g: dict, level: int, kind: str, name: str):
     """Per block: the full matrix (full fixtures) or (M@zc, M.T@zr, ||M||_F)."""
     pre = f"L{level}_{kind}_"
     shapes = g[pre + name + "_shape"]
     out = []
+    if is_compact(g):
+        raise ValueError("compact fixture: use compact_matrices")
     if bool(g["full"]):
         flat = g[pre + name]
         o = 0
@@ -58,6 +83,14 @@ def matrices(g: dict, level: int, kind: str, name: str):
 def sketch(M: np.ndarray):
     r, c = M.shape
     return M @ probe_vector(c, 0.3), M.T @ probe_vector(r, 1.1), float(np.linalg.norm(M))
+
+
+def face_case_inputs(g: dict):
+    """(ax, ay, az, V, u) of a face-operator fixture."""
+    from make_golden import face_inputs
+    N = int(g["N"])
+    ax, ay, az, V = face_inputs(N)
+    return ax, ay, az, V, synth.dof_vector(N, int(g["u_seed"]))
 
 
 def case_inputs(g: dict):

@@ -1,10 +1,12 @@
 """bench.py pieces that run on host cores (CPU).
 
 The reference arm (`bench.py --impl reference`) times the reference's own CPU
-build and must print one JSON line with the same metric, unit, config and
-direction as the GPU arm, a cpu_baseline describing the run and an e2e entry
-without host-device traffic. The serving arrivals are a seeded Poisson process
-whose mix the workload description states.
+build on the bench's operator and must print one JSON line with the GPU arm's
+metric and direction, a config and unit naming the size it actually ran (n = 32:
+the reference needs hours at n = 128), the number of steps it actually timed, a
+cpu_baseline describing the run and an e2e entry without host-device traffic.
+The serving arrivals are a seeded Poisson process whose mix the workload
+description states.
 """
 import json
 import os
@@ -28,21 +30,21 @@ def test_reference_arm_line():
     line = json.loads(out.strip().splitlines()[-1])
     assert line["impl"] == "reference"
     assert line["metric"] == bench.METRIC
-    assert line["unit"] == "factor+solve steps/s at n=128" and line["higher_is_better"] is True
+    n = bench.REF_N
+    assert line["unit"] == f"factor+solve steps/s at n={n}" and line["higher_is_better"] is True
     cfg = line["config"]
-    for k, v in bench.workload_config(128, 1e-6, 1).items():
+    for k, v in bench.workload_config(n, 1e-6, 1).items():
         assert cfg[k] == v
+    assert f"n={n} " in cfg["workload"]
+    assert line["steps"] == 1 and line["requested_steps"] == 1
     assert line["value"] > 0 and line["ms_per_step"] == pytest.approx(1e3 / line["value"])
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == line["value"]
+    assert "not scaled" in cb["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"],
                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
-
-
-def test_reference_units_scale_linearly_in_dofs():
-    assert bench.reference_units(10.0, 32, 32) == pytest.approx(0.1)
-    ratio = bench.dofs(128) / bench.dofs(32)
-    assert bench.reference_units(10.0, 32, 128) == pytest.approx(1.0 / (10.0 * ratio))
+    # the reference's own per-level times, every level of the n = 32 factorization
+    assert [lv["level"] for lv in line["per_level_s"]] == [0, 1, 2, 3]
 
 
 def test_serving_schedule_is_seeded_poisson_with_the_stated_mix():

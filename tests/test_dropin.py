@@ -13,7 +13,8 @@ import pytest
 
 from hifde3d_b200 import build as b
 
-REF = "/root/reference"
+# the reference's source tree (HIFDE3D_REFERENCE overrides the default location)
+REF = os.environ.get("HIFDE3D_REFERENCE", "/root/reference")
 
 
 @pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "tests", "HIFDE3D")),
