@@ -458,9 +458,9 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
   std::vector<Split> splits;
   for (size_t q = 0; q < gin.size(); ++q) {
     const GemmDesc& x = gin[q];
-    fl += 2.0 * x.m * x.n * x.k;
+    fl += x.a_lower ? 1.0 * x.m * x.n * (x.k + 1) : 2.0 * x.m * x.n * x.k;
     const int big = std::max(x.m, x.n);
-    if (force_tile == 0 && !x.lower && x.k >= 2048 && x.k >= 8 * big) {
+    if (force_tile == 0 && !x.lower && !x.a_lower && x.k >= 2048 && x.k >= 8 * big) {
       const int S = std::min(32, (x.k + 1023) / 1024);
       splits.push_back(Split{q, S});
       psz += (long long)S * x.m * x.n;
@@ -575,12 +575,14 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
     const int kt = (x.k + kOzK - 1) / kOzK;
     {
       const int tm = (x.m + 127) / 128, tn = (x.n + bn - 1) / bn;
-      long long tiles = (long long)tm * tn;
-      if (x.lower) {
-        tiles = 0;
-        for (int i = 0; i < tm; ++i) tiles += std::min(tn, (i * 128 + 128 + bn - 1) / bn);
+      // k tiles run, over the tiles computed
+      double tk = 0;
+      for (int i = 0; i < tm; ++i) {
+        const int cols = x.lower ? std::min(tn, (i * 128 + 128 + bn - 1) / bn) : tn;
+        const int kti = x.a_lower ? std::min(kt, (i * 128 + 128 + kOzK - 1) / kOzK) : kt;
+        tk += (double)cols * kti;
       }
-      fl += pairs * 2.0 * 128.0 * bn * kOzK * kt * (double)tiles;
+      fl += pairs * 2.0 * 128.0 * bn * kOzK * tk;
     }
     const int ta = (x.m + 127) / 128 * kt, tb = (x.n + 127) / 128 * kt;
     signed char* pa = cbuf + used * kOzPart;
@@ -600,7 +602,7 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
       if ((int)launches.size() <= c) launches.emplace_back();
       launches[c].push_back(OzGemm{pa, pb, ea, eb, x.C, x.ldc, x.m, x.n, kt, kt0,
                                    std::min(kChunkTiles, std::max(0, kt - kt0)), x.alpha,
-                                   c == 0 ? x.beta : 1.0, x.lower});
+                                   c == 0 ? x.beta : 1.0, x.lower, x.a_lower});
     }
   }
   timed(HIF_KCLASS_GEMM_INT8, fl, 0.0, [&] {
@@ -833,6 +835,7 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
     y.C = d.X;
     y.ldc = r;
     y.A = d.a22inv;
+    y.a_lower = 1;  // L^{-1}: half the product
     y.lda = r;
     y.B = d.B + (long long)r * d.n;
     y.ldb = d.n;
@@ -2062,7 +2065,7 @@ class Engine {
     for (int f = 0; f < nf; ++f) {
       const bool compressed = idM[f] != dM + o_M[f];
       const int n = idd[f].n;
-      if (chol && n > kCompressMinN && idd[f].m > n) {
+      if (chol && n > gram_min_n && idd[f].m > n) {
         chol_id.push_back(idd[f]);
         continue;
       }
@@ -2293,6 +2296,9 @@ class Engine {
   // 86-138); the skeleton test is the reference's |R_ii| > eps |R_00|.
   static constexpr int kPcholNB = 32;
   static constexpr double kGramMinEps = 1e-7;
+  // mixed precision: faces wider than this (and taller than wide) take the
+  // Gram-matrix ID; narrower ones the one-CTA pivoted QR (HIF_OPT_GRAM_MIN_N)
+  int gram_min_n = 64;
   void id_cholesky(const std::vector<IdDesc>& v, BufList& tmp) {
     Arena& work = *cur_work;
     const int nd = (int)v.size();
@@ -3655,6 +3661,10 @@ int hif_set_option(hif_handle h, int option, long long value) {
     case HIF_OPT_Y_SLICES:
       if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
       h->e->y_slices = (int)value;
+      return HIF_OK;
+    case HIF_OPT_GRAM_MIN_N:
+      if (value < 0) return HIF_ERR_ARG;
+      h->e->gram_min_n = (int)value;
       return HIF_OK;
     case HIF_OPT_ID_GROUP_MIN_N:
       if (value < 2) return HIF_ERR_ARG;

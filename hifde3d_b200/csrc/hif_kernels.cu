@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(256) k_dgemm(const GemmDesc* __restrict__ desc
     }
   };
 
-  const int nk = (g.k + kBK - 1) / kBK;
+  const int kend = g.a_lower ? min(g.k, m0 + kBM) : g.k;
+  const int nk = (kend + kBK - 1) / kBK;
   if (nk > 0) {
     load_a(0);
     load_b(0);
@@ -408,7 +409,8 @@ __global__ void __launch_bounds__(512, 1) k_dgemm128(const GemmDesc* __restrict_
       cp_async8(Cs + e, ok ? g.C + (m0 + i) + (long long)(n0 + j) * g.ldc : g.C, ok);
     }
   }
-  const int nk = (g.k + kLBK - 1) / kLBK;
+  const int kend = g.a_lower ? min(g.k, m0 + kLBM) : g.k;
+  const int nk = (kend + kLBK - 1) / kLBK;
 #pragma unroll
   for (int st = 0; st < kLStages - 1; ++st) {
     if (st < nk) issue(st, st * kLBK);
@@ -1011,6 +1013,11 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
   const int m0 = mt * 128, n0 = nt * BN;
   if (g.lower && n0 >= m0 + 128) return;  // whole CTA, before any barrier or allocation
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // k tiles of this CTA: all of the launch's, or with a lower-triangular A none
+  // past the tile's last row
+  const int kt_cnt = g.a_lower
+                         ? min(g.kt_cnt, max(0, (m0 + 128 + kOzK - 1) / kOzK - g.kt0))
+                         : g.kt_cnt;
 
   if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -1036,7 +1043,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
   if (warp == 0 && lane == 0) {
     // producer: the S slices of the A tile, then those of the B tile
     const int bt = n0 / 128, bhalf = (n0 / 64) & 1;
-    for (int i = 0; i < g.kt_cnt; ++i) {
+    for (int i = 0; i < kt_cnt; ++i) {
       const int kt = g.kt0 + i, s = i % NS;
       if (i >= NS && !mbar_wait(smem_u32(&empty[s]), (unsigned)((i / NS - 1) & 1), abort)) break;
       const unsigned fb = smem_u32(&full[s]);
@@ -1057,7 +1064,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
     }
   } else if (warp == 1 && lane == 0) {
     // tensor-core issue: slice pair (p, q) adds into the accumulator of diagonal p + q
-    for (int i = 0; i < g.kt_cnt; ++i) {
+    for (int i = 0; i < kt_cnt; ++i) {
       const int s = i % NS;
       if (!mbar_wait(smem_u32(&full[s]), (unsigned)((i / NS) & 1), abort)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -1086,7 +1093,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
               smem_u32(&empty[s]))
           : "memory");
     }
-    if (g.kt_cnt > 0)
+    if (kt_cnt > 0)
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
               smem_u32(done))
@@ -1097,7 +1104,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
     const int gm = m0 + 32 * q4 + lane;
     const unsigned lanes = (unsigned)(32 * q4) << 16;
     // k = 0: no products, nothing to wait for (C = beta C)
-    const bool ok = g.kt_cnt == 0 || (mbar_wait(smem_u32(done), 0u, abort) && !*abort);
+    const bool ok = kt_cnt == 0 || (mbar_wait(smem_u32(done), 0u, abort) && !*abort);
     if (ok) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int ea = gm < g.m ? max(g.ea[gm], -4096) : 0;
@@ -1106,7 +1113,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
         double h[16];
 #pragma unroll
         for (int e = 0; e < 16; ++e) h[e] = 0.0;
-        if (g.kt_cnt > 0) {
+        if (kt_cnt > 0) {
 #pragma unroll 1
           for (int d = S - 1; d >= 0; --d) {
             unsigned v[16];

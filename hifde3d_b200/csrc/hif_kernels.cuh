@@ -65,6 +65,7 @@ struct GemmDesc {
   double alpha, beta;
   int lower;  // 128 x 128 tiles only: skip the tiles above the diagonal (row tile < column tile)
   const int* skip;  // optional: the product is skipped when *skip != 0 (read on the device)
+  int a_lower;  // op(A) is lower triangular (m = k): a row tile reads no k past its last row
 };
 
 // Dense elimination block: B (n x n, ld n) in assembly order [red | skel].
@@ -308,6 +309,7 @@ struct OzGemm {
   int kt0, kt_cnt;  // k tiles of this product (kt_cnt * kOzK <= kOzMaxK)
   double alpha, beta;
   int lower;  // skip the tiles entirely above the diagonal
+  int a_lower;  // op(A) lower triangular: a 128-row tile reads no k tile past its last row
 };
 // C = alpha op(A) op(B) + beta C from converted operands with `slices` slices
 // (2..kOzMaxS); d_tile_off counts tiles of 128 x oz_tile_n(slices) columns.

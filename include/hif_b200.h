@@ -201,8 +201,10 @@ enum hif_option {
   HIF_OPT_X_SLICES = 9,       /* MIXED, Gauss-Jordan elimination: int8 slices (2..8) of
                                  X = A22^{-1} A21 (default 7); 0: FP64 */
   HIF_OPT_ELIMINATION = 10,   /* enum hif_elimination (default HIF_ELIM_AUTO) */
-  HIF_OPT_Y_SLICES = 11       /* MIXED, Cholesky elimination: int8 slices (2..8) of
+  HIF_OPT_Y_SLICES = 11,      /* MIXED, Cholesky elimination: int8 slices (2..8) of
                                  Y = L^{-1} A21 (default 6); 0: FP64 */
+  HIF_OPT_GRAM_MIN_N = 12     /* MIXED: faces with more columns than this (and more rows
+                                 than columns) take the Gram-matrix ID (default 64) */
 };
 /* Arithmetic of the factorization. MIXED: the long-K products of the eliminations
  * (S = A11 - A12 X, and X or Y) are FP64 products formed from exact int8 slice
