@@ -759,18 +759,24 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
         gu.push_back(u);
       }
       if (k0 > 0) {
-        GemmDesc t{};
-        t.C = T;
-        t.ldc = kSweepNB;
-        t.A = d.B + k0;  // L[K, 0:k0]
-        t.lda = d.n;
-        t.B = d.a22inv;  // L^{-1}[0:k0, 0:k0]
-        t.ldb = r;
-        t.m = nbk;
-        t.n = k0;
-        t.k = k0;
-        t.alpha = 1.0;
-        gt.push_back(t);
+        // T = L[K, 0:k0] L^{-1}[0:k0, 0:k0] by 128-column blocks J: L^{-1} is
+        // lower triangular, so block J needs only k in [J0, k0) (half the flops);
+        // each block's long reduction is split along k by gemm_batch, which keeps
+        // the GPU busy when there are few blocks (the top levels)
+        for (int j0 = 0; j0 < k0; j0 += kSweepNB) {
+          GemmDesc t{};
+          t.C = T + (long long)j0 * kSweepNB;
+          t.ldc = kSweepNB;
+          t.A = d.B + k0 + (long long)j0 * d.n;  // L[K, j0:k0]
+          t.lda = d.n;
+          t.B = d.a22inv + j0 + (long long)j0 * r;  // L^{-1}[j0:k0, j0:j0+128]
+          t.ldb = r;
+          t.m = nbk;
+          t.n = std::min(kSweepNB, k0 - j0);
+          t.k = k0 - j0;
+          t.alpha = 1.0;
+          gt.push_back(t);
+        }
         GemmDesc l{};
         l.C = d.a22inv + k0;
         l.ldc = r;
@@ -1687,6 +1693,7 @@ class Engine {
       part.cell_index(level, c, b.global, b.red_pos, b.skel_pos);
       b.cell = idx;
     });
+    mark("schur cell partition", level);
     // sizes and device layout
     std::vector<int> red_all, skel_all;
     long long bsz = 0, asz = 0;
@@ -1737,6 +1744,7 @@ class Engine {
     st.n_red = red_all.size();
     st.n_skel = skel_all.size();
     start_face_partition(level, red_all);
+    mark("schur index lists", level);
     t_host += wall() - th;
 
     track((bsz + asz) * 8);
@@ -1943,6 +1951,7 @@ class Engine {
     std::vector<BlockInfo>& blocks = st.blocks;
     if (!take_face_partition(level, blocks, rows_l))
       partition_faces(level, rem.data(), blocks, rows_l);
+    mark("skel face partition", level);
     const int nf = (int)blocks.size();
     // M blocks (rows x cols) and ID workspace
     std::vector<long long> o_rows(nf), o_cols(nf), o_M(nf), o_W(nf), o_i(nf);
@@ -1968,6 +1977,7 @@ class Engine {
       std::copy(rows_l[f].begin(), rows_l[f].end(), idx_all.begin() + o_rows[f]);
       std::copy(blocks[f].global.begin(), blocks[f].global.end(), idx_all.begin() + o_cols[f]);
     });
+    mark("skel index lists", level);
     t_host += wall() - th;
 
     BufList tmp;
@@ -2197,6 +2207,7 @@ class Engine {
     });
     st.n_red = red_all.size();
     st.n_skel = skel_all.size();
+    mark("skel ID index lists", level);
     t_host += wall() - th;
 
     track((bsz + asz) * 8);

@@ -12,8 +12,13 @@ cube, sigma 1, seed 2), eps = 1e-6. Two fixtures pin it (tests/golden/):
 
 Bars, as in test_gpu_parity.py:
 * level count, block counts and index data (global / redundant / skeleton
-  lists): bit-exact; skeleton sets exact, and pivot order exact (no exact ties
-  with a random field);
+  lists): bit-exact; the skeleton columns exact and in the reference's pivot
+  order. The redundant columns of a face are compared as a set: past the rank
+  the pivoted QR keeps choosing among residual column norms at rounding level
+  (below 1e-12 of the largest), so their order is set by last-bit rounding and
+  differs between LAPACK builds as between the reference and the GPU. W's
+  columns and the redundant rows / columns of the skeletonization blocks follow
+  that order; they are permuted to the reference's before the comparison;
 * dense factor blocks, compared through ||M||_F and a bilinear sketch
   zr^T M zc, both relative to ||M||_F: 1e-10 for the Schur (cell) blocks,
   1e-8 for the skeletonization blocks and W (W = R11^{-1} R12 carries
@@ -78,9 +83,12 @@ def test_index_data_and_skeletons(case):
                 ours = f.block(lev, kind, b)
                 assert ours["face"] == face
                 np.testing.assert_array_equal(ours["global"], gg)
-                # cell blocks: positions in scan order; faces: pivot order
-                np.testing.assert_array_equal(ours["red"], rr, err_msg=f"{name} L{lev} {kname} {b}")
+                # cell blocks: positions in scan order; faces: skeleton in pivot order
                 np.testing.assert_array_equal(ours["skel"], ss, err_msg=f"{name} L{lev} {kname} {b}")
+                if kind == 0:
+                    np.testing.assert_array_equal(ours["red"], rr)
+                else:
+                    assert sorted(ours["red"].tolist()) == sorted(rr.tolist()), (name, lev, b)
 
 
 def test_dense_blocks(case):
@@ -97,6 +105,14 @@ def test_dense_blocks(case):
                     continue
                 ours = f.block(lev, kind, b, matrices=True)
                 ours["S"] = f.schur_complement(lev, kind, b)
+                if kind == 1 and not np.array_equal(ours["red"], rr):
+                    # redundant columns in the reference's order (see the module note)
+                    pos = {int(v): i for i, v in enumerate(ours["red"])}
+                    p = np.array([pos[int(v)] for v in rr])
+                    ours["A22"] = ours["A22"][np.ix_(p, p)]
+                    ours["A22inv"] = ours["A22inv"][np.ix_(p, p)]
+                    ours["X"] = ours["X"][p, :]
+                    ours["W"] = ours["W"][:, p]
                 for m in mats:
                     shape, fro, bil = refm[m][b]
                     om = ours[m]
@@ -132,8 +148,8 @@ def test_mixed_precision_against_fp64_oracle(name):
     e = rel(y, g["Finv_u"])
     print(name, f"mixed F^-1 u vs FP64 oracle: relative difference {e:.2e}")
     assert e < MIXED_TOL, (name, e)
-    # the index data (partition) stays exact in mixed precision
-    for lev in range(int(g["L"])):
-        for b, (_, gg, _, _) in enumerate(goldens.blocks(g, lev, "schur")):
-            np.testing.assert_array_equal(f.block(lev, 0, b)["global"], gg)
+    # the level-0 cell partition does not depend on the arithmetic (later levels'
+    # lists follow the mixed-precision skeletons)
+    for b, (_, gg, _, _) in enumerate(goldens.blocks(g, 0, "schur")):
+        np.testing.assert_array_equal(f.block(0, 0, b)["global"], gg)
     f.close()
