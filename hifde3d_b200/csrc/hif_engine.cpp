@@ -37,6 +37,7 @@
 #include <memory>
 #include <string>
 #include <exception>
+#include <future>
 #include <thread>
 #include <vector>
 
@@ -144,8 +145,11 @@ void copy_to_device(void* d, const void* h, size_t bytes, cudaStream_t s) {
 }
 
 template <class T>
+T* desc_alloc(size_t count, cudaStream_t s);
+
+template <class T>
 T* upload(const std::vector<T>& v, cudaStream_t s) {
-  T* d = dalloc<T>(v.size(), s);
+  T* d = desc_alloc<T>(v.size(), s);
   copy_to_device(d, v.data(), v.size() * sizeof(T), s);
   return d;
 }
@@ -173,11 +177,20 @@ void parallel_for(int n, F&& f) {
 }
 
 // Keeps device buffers of one phase alive until released together.
+struct Arena;
+// Device memory for the small uploads of a factorization (descriptor arrays,
+// index lists): bump-allocated from chunks kept for the handle's life and
+// given back all at once when the next factorization starts, instead of one
+// stream-ordered allocation and free per upload (several driver calls per
+// launch, which set the pace of the many short launches of the lower levels).
+thread_local Arena* t_desc = nullptr;
+bool desc_owned(const void* x);
+
 struct BufList {
   std::vector<void*> p;
   template <class T>
   T* add(T* x) {
-    p.push_back(x);
+    if (!desc_owned(x)) p.push_back(x);
     return x;
   }
   void release(cudaStream_t s) {
@@ -229,8 +242,40 @@ struct Arena {
     return d;
   }
   void reset() {
+    size_t u = 0;
+    for (Chunk& c : chunks) {
+      u += c.used;
+      c.used = 0;
+    }
+    hw_cycle = std::max(hw_cycle, u);
+    cur = 0;
+  }
+  // Chunks are sized by the requests that first outgrew them, so a handle whose
+  // block sizes change (another precision, a refactorization with other
+  // skeleton ranks) can end with chunks none of which fits a later request.
+  // At a point where nothing on the device uses the arena, consolidate():
+  // when it holds several chunks, they are replaced by one of the largest
+  // total the arena was asked for in a cycle since the last consolidation.
+  size_t hw_cycle = 0;
+  void consolidate() {
+    size_t u = 0;
+    for (const Chunk& c : chunks) u += c.used;
+    hw_cycle = std::max(hw_cycle, u);
+    if (chunks.size() > 1 && hw_cycle > 0) {
+      release();
+      const size_t sz = ((hw_cycle + hw_cycle / 16) + 255) & ~size_t(255);
+      void* p = nullptr;
+      const double t0 = wall();
+      if (cudaMalloc(&p, sz) == cudaSuccess) {
+        chunks.push_back(Chunk{static_cast<char*>(p), sz, 0});
+      } else {
+        cudaGetLastError();  // leave it empty: alloc() grows it on demand
+      }
+      grow_s += wall() - t0;
+    }
     for (Chunk& c : chunks) c.used = 0;
     cur = 0;
+    hw_cycle = 0;
   }
   // Stack discipline for temporaries: everything allocated after mark() is
   // given back by rewind(). Users are on one stream, so memory handed out
@@ -249,12 +294,25 @@ struct Arena {
     for (const Chunk& c : chunks) t += c.size;
     return t;
   }
+  bool owns(const void* x) const {
+    const char* q = static_cast<const char*>(x);
+    for (const Chunk& c : chunks)
+      if (q >= c.p && q < c.p + c.size) return true;
+    return false;
+  }
   void release() {
     for (Chunk& c : chunks) cudaFree(c.p);
     chunks.clear();
     cur = 0;
   }
 };
+
+bool desc_owned(const void* x) { return t_desc != nullptr && t_desc->owns(x); }
+
+template <class T>
+T* desc_alloc(size_t count, cudaStream_t s) {
+  return t_desc ? t_desc->alloc<T>(count) : dalloc<T>(count, s);
+}
 
 }  // namespace
 
@@ -298,9 +356,15 @@ struct ApplyLaunch {
   std::vector<GemvDesc> hdesc;  // host copy of the descriptors
   int type = 0;  // 0 gemv, 1 reduce-scatter
   GemvDesc* d_desc = nullptr;
-  int* d_toff = nullptr;
-  int nd = 0, tiles = 0;
+  int nd = 0;
   int in_vec = 0, out_vec = 0;  // 0 = ua, 1 = ub, 2 = uc (Cholesky phases' L^{-1} u_r)
+  // GEMV layout (launch_gemv_fast) and its unit table; the serving loop binds
+  // the descriptors to a request's vectors and reuses the table
+  int layout = 0;
+  int2* d_tab = nullptr;
+  int units = 0;
+  GemvFastSeg* d_seg = nullptr;  // one segment: this launch's descriptors and table
+  int* d_segoff = nullptr;
   int* d_dof = nullptr;
   int* d_off = nullptr;
   int* d_slot = nullptr;
@@ -1241,8 +1305,9 @@ class Engine {
   bool have_op = false, initialized = false, factored = false;
   std::vector<uint8_t> rem;
   std::vector<StepData> steps;
-  // factor storage (persistent) and per-level workspace (alternating by level)
-  Arena arena_factor, arena_work[2];
+  // factor storage (persistent) and per-level workspace (alternating by level);
+  // arena_desc: the factorization's uploads (see t_desc), its apply plans' too
+  Arena arena_factor, arena_work[2], arena_desc;
   Arena* cur_work = &arena_work[0];
   bool keep_schur = false, verbose = false;
   int verbose_mode = 0;
@@ -1353,6 +1418,7 @@ class Engine {
 
   ~Engine() {
     join_face_partition();
+    join_cell_partition();
     sync_quiet();
     for (Pending& pd : pending) {
       cudaEventDestroy(pd.a);
@@ -1365,6 +1431,7 @@ class Engine {
     arena_factor.release();
     arena_work[0].release();
     arena_work[1].release();
+    arena_desc.release();
     dfree(d_band, stream);
     dfree(d_status, stream);
     dfree(d_dof_src, stream);
@@ -1565,6 +1632,8 @@ class Engine {
 
   void release_plans() {
     drop_graphs();
+    reduce_bufs.release(stream);
+    reduce_lists.clear();
     plan_inv.bufs.release(stream);
     plan_fwd.bufs.release(stream);
     plan_inv.launches.clear();
@@ -1574,6 +1643,9 @@ class Engine {
 
   void release_factor() {
     release_plans();
+    for (auto& kv : reduce_pending)
+      if (kv.second.valid()) kv.second.wait();
+    reduce_pending.clear();
     dfree(d_contrib, stream);
     d_contrib = nullptr;
     contrib_cap = 0;
@@ -1686,13 +1758,33 @@ class Engine {
     st.cpd = cpd;
     Partitioner part{N, P, NC, rem.data()};
     const int ncell = cpd * cpd * cpd;
-    st.blocks.resize(ncell);
-    parallel_for(ncell, [&](int idx) {
-      const int c[3] = {idx / (cpd * cpd), (idx / cpd) % cpd, idx % cpd};
-      BlockInfo& b = st.blocks[idx];
-      part.cell_index(level, c, b.global, b.red_pos, b.skel_pos);
-      b.cell = idx;
-    });
+    if (take_cell_partition(level, st.blocks)) {
+      // built before the last skeletonization's DOFs were removed: drop them
+      // (the scan order and the classification of the rest do not change)
+      parallel_for(ncell, [&](int idx) {
+        BlockInfo& b = st.blocks[idx];
+        std::vector<char> cls(b.global.size(), 0);
+        for (int q : b.red_pos) cls[q] = 1;
+        std::vector<int> g, r, k;
+        g.reserve(b.global.size());
+        for (size_t t = 0; t < b.global.size(); ++t) {
+          if (!rem[b.global[t]]) continue;
+          (cls[t] ? r : k).push_back((int)g.size());
+          g.push_back(b.global[t]);
+        }
+        b.global.swap(g);
+        b.red_pos.swap(r);
+        b.skel_pos.swap(k);
+      });
+    } else {
+      st.blocks.resize(ncell);
+      parallel_for(ncell, [&](int idx) {
+        const int c[3] = {idx / (cpd * cpd), (idx / cpd) % cpd, idx % cpd};
+        BlockInfo& b = st.blocks[idx];
+        part.cell_index(level, c, b.global, b.red_pos, b.skel_pos);
+        b.cell = idx;
+      });
+    }
     mark("schur cell partition", level);
     // sizes and device layout
     std::vector<int> red_all, skel_all;
@@ -1743,7 +1835,7 @@ class Engine {
     });
     st.n_red = red_all.size();
     st.n_skel = skel_all.size();
-    start_face_partition(level, red_all);
+    if (level > 0) start_face_partition(level, red_all);
     mark("schur index lists", level);
     t_host += wall() - th;
 
@@ -1861,6 +1953,7 @@ class Engine {
     // remove eliminated DOFs (UpdateRemainingDOFs, src/Factor.cpp:91-111)
     for (int p : red_all) rem[p] = 0;
     tmp.release(stream);
+    if (level < L - 1) start_reduce_lists(st, skel_all);
     steps.push_back(std::move(st));
     t_host += wall() - th;
   }
@@ -1928,6 +2021,83 @@ class Engine {
   void join_face_partition() {
     if (face_thread.joinable()) face_thread.join();
   }
+  // The next level's cell partition, built on a host thread while a
+  // skeletonization phase runs on the device: over the DOFs left before that
+  // phase, to be filtered by the ones it eliminates (take_cell_partition's
+  // caller does that).
+  struct CellPartition {
+    int level = -1;
+    std::vector<uint8_t> mask;
+    std::vector<BlockInfo> blocks;
+    std::exception_ptr err;
+  };
+  CellPartition cell_pre;
+  std::thread cell_thread;
+  void start_cell_partition(int level) {
+    join_cell_partition();
+    if (level >= L) return;
+    cell_pre = CellPartition{};
+    cell_pre.level = level;
+    cell_pre.mask = rem;
+    cell_thread = std::thread([this, level] {
+      try {
+        Partitioner part{N, P, NC, cell_pre.mask.data()};
+        const int cpd = cells_per_dir(level);
+        const int ncell = cpd * cpd * cpd;
+        cell_pre.blocks.resize(ncell);
+        parallel_for(ncell, [&](int idx) {
+          const int c[3] = {idx / (cpd * cpd), (idx / cpd) % cpd, idx % cpd};
+          BlockInfo& b = cell_pre.blocks[idx];
+          part.cell_index(level, c, b.global, b.red_pos, b.skel_pos);
+          b.cell = idx;
+        });
+      } catch (...) {
+        cell_pre.err = std::current_exception();
+      }
+    });
+  }
+  void join_cell_partition() {
+    if (cell_thread.joinable()) cell_thread.join();
+  }
+  bool take_cell_partition(int level, std::vector<BlockInfo>& blocks) {
+    join_cell_partition();
+    if (cell_pre.level != level) return false;
+    cell_pre.level = -1;
+    if (cell_pre.err) std::rethrow_exception(cell_pre.err);
+    blocks = std::move(cell_pre.blocks);
+    return true;
+  }
+
+  // Level 0's face partition depends on the grid alone: its DOF mask is the
+  // initial one less every DOF strictly inside a level-0 cell (all three
+  // coordinates interior to the cell width, src/Factor.cpp:314-320), which is
+  // exactly what level 0's cell phase eliminates. It starts at once, so the
+  // host thread builds it while the cell phase is assembled and eliminated.
+  void start_face_partition0() {
+    join_face_partition();
+    if (L <= 1) return;
+    face_pre = FacePartition{};
+    face_pre.level = 0;
+    face_pre.mask = rem;
+    face_thread = std::thread([this] {
+      try {
+        uint8_t* m = face_pre.mask.data();
+        Partitioner part{N, P, NC, m};
+        const int w = part.width(0);
+        parallel_for(NC, [&](int k) {
+          if (!part.interior(w, k)) return;
+          for (int j = 1; j < NC; ++j) {
+            if (!part.interior(w, j)) continue;
+            for (int i = 1; i < NC; ++i)
+              if (part.interior(w, i)) m[part.lin(i, j, k)] = 0;
+          }
+        });
+        partition_faces(0, m, face_pre.blocks, face_pre.rows_l);
+      } catch (...) {
+        face_pre.err = std::current_exception();
+      }
+    });
+  }
   bool take_face_partition(int level, std::vector<BlockInfo>& blocks,
                            std::vector<std::vector<int>>& rows_l) {
     join_face_partition();
@@ -1951,6 +2121,7 @@ class Engine {
     std::vector<BlockInfo>& blocks = st.blocks;
     if (!take_face_partition(level, blocks, rows_l))
       partition_faces(level, rem.data(), blocks, rows_l);
+    start_cell_partition(level + 1);
     mark("skel face partition", level);
     const int nf = (int)blocks.size();
     // M blocks (rows x cols) and ID workspace
@@ -1972,10 +2143,12 @@ class Engine {
       max_n = std::max(max_n, n);
     }
     // row and column lists of every face, filled in parallel
-    std::vector<int> idx_all(xsz);
+    // written straight into pinned staging memory: no host array to zero-fill
+    // and page in, and no second copy before the upload
+    int* idx_all = static_cast<int*>(stage.get(std::max<long long>(xsz, 1) * sizeof(int)));
     parallel_for(nf, [&](int f) {
-      std::copy(rows_l[f].begin(), rows_l[f].end(), idx_all.begin() + o_rows[f]);
-      std::copy(blocks[f].global.begin(), blocks[f].global.end(), idx_all.begin() + o_cols[f]);
+      std::copy(rows_l[f].begin(), rows_l[f].end(), idx_all + o_rows[f]);
+      std::copy(blocks[f].global.begin(), blocks[f].global.end(), idx_all + o_cols[f]);
     });
     mark("skel index lists", level);
     t_host += wall() - th;
@@ -1987,7 +2160,8 @@ class Engine {
     t_scratch = &work;
     double* dM = work.alloc<double>(msz);
     double* dWs = work.alloc<double>(wsz);
-    int* didx = tmp.add(upload(idx_all, stream));
+    int* didx = tmp.add(desc_alloc<int>(xsz, stream));
+    if (xsz) HIF_CK(cudaMemcpyAsync(didx, idx_all, xsz * sizeof(int), cudaMemcpyHostToDevice, stream));
     int* d_jp = tmp.add(dalloc<int>(isz + 1, stream));
     int* d_keep = tmp.add(dalloc<int>(isz + 1, stream));
     int* d_rank = tmp.add(dalloc<int>(nf + 1, stream));
@@ -2116,8 +2290,11 @@ class Engine {
     for (const IdDesc& d : idd) idfl += 4.0 * d.m * d.n * d.n - 4.0 / 3.0 * d.n * d.n * (double)d.n;
     if (!small_id.empty()) {
       IdDesc* d_idd = tmp.add(upload(small_id, stream));
-      timed(HIF_KCLASS_ID, idfl, 0,
-            [&] { launch_id(d_idd, (int)small_id.size(), small_n, eps, d_status, stream); });
+      long long max_mn = 0;
+      for (const IdDesc& d : small_id) max_mn = std::max(max_mn, (long long)d.m * d.n);
+      timed(HIF_KCLASS_ID, idfl, 0, [&] {
+        launch_id(d_idd, (int)small_id.size(), small_n, eps, d_status, stream, max_mn);
+      });
       idfl = 0;
     }
     if (!chol_id.empty()) id_cholesky(chol_id, tmp);
@@ -2753,15 +2930,18 @@ class Engine {
     PinnedStage* prev;
     Arena* prev_scratch;
     GemmTuner* prev_tuner;
-    StageScope(PinnedStage* s, GemmTuner* tu)
-        : prev(t_stage), prev_scratch(t_scratch), prev_tuner(t_tuner) {
+    Arena* prev_desc;
+    StageScope(PinnedStage* s, GemmTuner* tu, Arena* desc)
+        : prev(t_stage), prev_scratch(t_scratch), prev_tuner(t_tuner), prev_desc(t_desc) {
       t_stage = s;
       t_tuner = tu;
+      t_desc = desc;
     }
     ~StageScope() {
       t_stage = prev;
       t_scratch = prev_scratch;
       t_tuner = prev_tuner;
+      t_desc = prev_desc;
     }
   };
 
@@ -2771,12 +2951,22 @@ class Engine {
     // copies are complete
     sync();
     stage.reset();
-    StageScope scope(&stage, autotune ? &tuner : nullptr);
+    StageScope scope(&stage, autotune ? &tuner : nullptr, &arena_desc);
     join_face_partition();
     face_pre.level = -1;
+    join_cell_partition();
+    cell_pre.level = -1;
     if (partition == HIF_PARTITION_CLIPPED && NC % P != 0)
       throw Error{HIF_ERR_ARG, "clipped partition needs (N+1) divisible by P"};
     initialize();
+    // the previous factorization's descriptors (its apply plans included) were
+    // dropped with it, after the synchronisation above: nothing on the device
+    // uses the arenas now
+    arena_factor.consolidate();
+    arena_work[0].consolidate();
+    arena_work[1].consolidate();
+    arena_desc.consolidate();
+    start_face_partition0();
     // Cholesky elimination for symmetric operators: by default in mixed
     // precision; the FP64 default keeps the reference's explicit inverse
     // (getrf + getri, include/Schur.hpp:86)
@@ -2824,6 +3014,7 @@ class Engine {
     ensure_workspace(1);
     sync();
     t_plan = wall() - tp;
+    if (verbose) std::fprintf(stderr, "[hif]   apply plans built in %.3f ms\n", 1e3 * t_plan);
     if (profile) resolve_profile();
   }
 
@@ -2835,7 +3026,6 @@ class Engine {
                 bool out_red, double alpha, int mode, int in_vec, int out_vec, int tri = 0) {
     const long long my_key = plan_key++;  // taken even when the launch is empty
     std::vector<GemvDesc> dd;
-    std::vector<int> toff(1, 0);
     double mbytes = 0;
     for (size_t b = 0; b < st.blocks.size(); ++b) {
       const BlockInfo& bi = st.blocks[b];
@@ -2867,21 +3057,35 @@ class Engine {
       g.contrib = (mode == 1) ? d_contrib + st.o_skel[b] : nullptr;
       mbytes += 8.0 * g.m * g.n;
       dd.push_back(g);
-      toff.push_back(toff.back() + gemv_tiles(g.m, g.n, trans));
     }
     if (dd.empty()) return;
     ApplyLaunch l;
     l.type = 0;
     l.bytes = mbytes;
     l.nd = dd.size();
-    l.tiles = toff.back();
     l.in_vec = in_vec;
     l.out_vec = out_vec;
-    l.d_toff = plan.bufs.add(upload(toff, stream));
     l.d_desc = plan.bufs.add(upload(dd, stream));
-    l.hdesc = dd;
+    int big = 0;
+    for (const GemvDesc& g : dd) big = std::max(big, std::max(g.m, g.n));
+    if (big <= kGemvSmallMax) {
+      l.layout = kGemvSmall;
+      l.units = (int)dd.size();
+    } else {
+      l.layout = trans ? kGemvCols : kGemvRows;
+      std::vector<int2> tab;
+      for (size_t q = 0; q < dd.size(); ++q) {
+        const int nt = trans ? (dd[q].n + 31) / 32 : (dd[q].m + 63) / 64;
+        for (int t = 0; t < nt; ++t) tab.push_back(make_int2((int)q, t));
+      }
+      l.units = (int)tab.size();
+      l.d_tab = plan.bufs.add(upload(tab, stream));
+    }
+    l.d_seg = plan.bufs.add(upload(std::vector<GemvFastSeg>{{l.d_desc, l.d_tab}}, stream));
+    l.d_segoff = plan.bufs.add(upload(std::vector<int>{0, l.units}, stream));
+    l.hdesc = std::move(dd);
     l.key = my_key;
-    plan.launches.push_back(l);
+    plan.launches.push_back(std::move(l));
   }
 
   // A22 = L L^T, A22^{-1} = L^{-T} L^{-1} or X = L^{-T} Y (which 0 / 1 / 2) of
@@ -2918,10 +3122,89 @@ class Engine {
     sync();
   }
 
-  void add_reduce(ApplyPlan& plan, const StepData& st, double alpha, int vec) {
-    const long long my_key = plan_key++;
-    // every skeleton DOF of the level with its contribution slots, in block order
-    std::vector<int> head(n3, -1), dof, cnt;
+  // Host part of a Schur phase's reduction lists: every skeleton DOF of the
+  // level (blocks with redundant DOFs, in block order) with its contribution
+  // slots. Computed on a worker thread while the factorization goes on (the
+  // inputs are the phase's skeleton DOF list, its offsets and which blocks
+  // eliminate anything), so that the plans at the end only upload them.
+  struct ReduceHost {
+    std::vector<int> dof, off, slot;
+  };
+  static ReduceHost reduce_host(long long n3, std::vector<int> skel_all,
+                                std::vector<long long> o_skel, std::vector<char> has_r) {
+    ReduceHost h;
+    std::vector<int> head(n3, -1), cnt;
+    const size_t nb = o_skel.size();
+    auto range = [&](size_t b) {
+      const long long a = o_skel[b];
+      const long long e = b + 1 < nb ? o_skel[b + 1] : (long long)skel_all.size();
+      return std::make_pair(a, e);
+    };
+    for (size_t b = 0; b < nb; ++b) {
+      if (!has_r[b]) continue;
+      const auto re = range(b);
+      for (long long t = re.first; t < re.second; ++t) {
+        const int p = skel_all[t];
+        if (head[p] < 0) {
+          head[p] = (int)h.dof.size();
+          h.dof.push_back(p);
+          cnt.push_back(0);
+        }
+        ++cnt[head[p]];
+      }
+    }
+    if (h.dof.empty()) return h;
+    h.off.assign(h.dof.size() + 1, 0);
+    for (size_t d = 0; d < h.dof.size(); ++d) h.off[d + 1] = h.off[d] + cnt[d];
+    h.slot.resize(h.off.back());
+    std::vector<int> cur(h.off.begin(), h.off.end() - 1);
+    for (size_t b = 0; b < nb; ++b) {
+      if (!has_r[b]) continue;
+      const auto re = range(b);
+      for (long long t = re.first; t < re.second; ++t) h.slot[cur[head[skel_all[t]]]++] = (int)t;
+    }
+    return h;
+  }
+  std::map<int, std::future<ReduceHost>> reduce_pending;  // Schur phase level -> lists
+  void start_reduce_lists(const StepData& st, const std::vector<int>& skel_all) {
+    std::vector<char> has_r(st.blocks.size());
+    for (size_t b = 0; b < st.blocks.size(); ++b) has_r[b] = st.blocks[b].r() > 0;
+    reduce_pending[st.level] = std::async(std::launch::async, reduce_host, n3, skel_all,
+                                          st.o_skel, std::move(has_r));
+  }
+
+  // Reduction lists of a Schur phase (every skeleton DOF of the level with its
+  // contribution slots, in block order), built once per phase and shared by
+  // both plans.
+  struct ReduceLists {
+    int* d_dof = nullptr;
+    int* d_off = nullptr;
+    int* d_slot = nullptr;
+    int ndof = 0;
+  };
+  std::map<const StepData*, ReduceLists> reduce_lists;
+  std::vector<int> reduce_head;  // n3, all -1 between uses
+  BufList reduce_bufs;
+
+  const ReduceLists& reduce_lists_for(const StepData& st) {
+    auto it = reduce_lists.find(&st);
+    if (it != reduce_lists.end()) return it->second;
+    auto pend = reduce_pending.find(st.level);
+    if (!st.skel && pend != reduce_pending.end() && pend->second.valid()) {
+      ReduceHost h = pend->second.get();
+      reduce_pending.erase(pend);
+      ReduceLists rl;
+      if (!h.dof.empty()) {
+        rl.d_dof = reduce_bufs.add(upload(h.dof, stream));
+        rl.d_off = reduce_bufs.add(upload(h.off, stream));
+        rl.d_slot = reduce_bufs.add(upload(h.slot, stream));
+        rl.ndof = (int)h.dof.size();
+      }
+      return reduce_lists.emplace(&st, rl).first->second;
+    }
+    if ((long long)reduce_head.size() != n3) reduce_head.assign(n3, -1);
+    std::vector<int>& head = reduce_head;
+    std::vector<int> dof, cnt;
     for (size_t b = 0; b < st.blocks.size(); ++b) {
       const BlockInfo& bi = st.blocks[b];
       if (bi.r() == 0) continue;
@@ -2935,24 +3218,38 @@ class Engine {
         ++cnt[head[p]];
       }
     }
-    if (dof.empty()) return;
-    std::vector<int> off(dof.size() + 1, 0);
-    for (size_t d = 0; d < dof.size(); ++d) off[d + 1] = off[d] + cnt[d];
-    std::vector<int> slot(off.back()), cur(off.begin(), off.end() - 1);
-    for (size_t b = 0; b < st.blocks.size(); ++b) {
-      const BlockInfo& bi = st.blocks[b];
-      if (bi.r() == 0) continue;
-      for (int t = 0; t < bi.s(); ++t) {
-        const int p = bi.global[bi.skel_pos[t]];
-        slot[cur[head[p]]++] = (int)(st.o_skel[b] + t);
+    ReduceLists rl;
+    if (!dof.empty()) {
+      std::vector<int> off(dof.size() + 1, 0);
+      for (size_t d = 0; d < dof.size(); ++d) off[d + 1] = off[d] + cnt[d];
+      std::vector<int> slot(off.back()), cur(off.begin(), off.end() - 1);
+      for (size_t b = 0; b < st.blocks.size(); ++b) {
+        const BlockInfo& bi = st.blocks[b];
+        if (bi.r() == 0) continue;
+        for (int t = 0; t < bi.s(); ++t) {
+          const int p = bi.global[bi.skel_pos[t]];
+          slot[cur[head[p]]++] = (int)(st.o_skel[b] + t);
+        }
       }
+      rl.d_dof = reduce_bufs.add(upload(dof, stream));
+      rl.d_off = reduce_bufs.add(upload(off, stream));
+      rl.d_slot = reduce_bufs.add(upload(slot, stream));
+      rl.ndof = (int)dof.size();
     }
+    for (int p : dof) head[p] = -1;
+    return reduce_lists.emplace(&st, rl).first->second;
+  }
+
+  void add_reduce(ApplyPlan& plan, const StepData& st, double alpha, int vec) {
+    const long long my_key = plan_key++;
+    const ReduceLists& rl = reduce_lists_for(st);
+    if (rl.ndof == 0) return;
     ApplyLaunch l;
     l.type = 1;
-    l.d_dof = plan.bufs.add(upload(dof, stream));
-    l.d_off = plan.bufs.add(upload(off, stream));
-    l.d_slot = plan.bufs.add(upload(slot, stream));
-    l.ndof = dof.size();
+    l.d_dof = rl.d_dof;
+    l.d_off = rl.d_off;
+    l.d_slot = rl.d_slot;
+    l.ndof = rl.ndof;
     l.alpha = alpha;
     l.out_vec = vec;
     l.key = my_key;
@@ -3129,8 +3426,8 @@ class Engine {
       if (l.type == 0) {
         const double by = l.bytes * ((nrhs + 3) / 4);
         timed(HIF_KCLASS_GEMV, 2.0 * l.bytes / 8 * nrhs, by, [&] {
-          launch_gemv(l.d_desc, l.d_toff, l.nd, l.tiles, vec[l.in_vec], vec[l.out_vec], nrhs, n3,
-                      contrib_ld, stream);
+          launch_gemv_fast(l.d_seg, l.d_segoff, 1, l.units, l.layout, vec[l.in_vec],
+                           vec[l.out_vec], nrhs, n3, contrib_ld, stream);
         });
       } else {
         timed(HIF_KCLASS_VECTOR, 0, 0, [&] {
@@ -4011,7 +4308,9 @@ int hif_trim_device_pool(void) {
 
 int hif_memory(hif_handle h, long long* factor_bytes, long long* workspace_bytes) {
   if (!h) return HIF_ERR_ARG;
-  if (factor_bytes) *factor_bytes = (long long)h->e->arena_factor.reserved();
+  // the factor and the descriptors its apply plans read
+  if (factor_bytes)
+    *factor_bytes = (long long)(h->e->arena_factor.reserved() + h->e->arena_desc.reserved());
   if (workspace_bytes)
     *workspace_bytes = (long long)(h->e->arena_work[0].reserved() + h->e->arena_work[1].reserved());
   return HIF_OK;

@@ -258,6 +258,7 @@ void save_factor(Engine& e, const char* path) {
 void load_factor(Engine& e, const char* path) {
   e.sync();
   e.join_face_partition();
+  e.join_cell_partition();
   e.initialize();  // drops any factorization the handle held
   FactorReader rd(path);
   bool op_touched = false;

@@ -87,10 +87,14 @@ __device__ double block_sum(double v, double* scratch) {
 // ===========================================================================
 // Gather / assembly
 // ===========================================================================
-constexpr int kGT = 32;  // gather tile edge
+// Tiles of 32 rows x 64 columns: lane x of warp w assembles row x of columns
+// w, w + 8, ..., w + 56, so a thread's row, its stencil row and its row covers
+// (up to three sources, each turned into a pointer to the source's row) stay in
+// registers, and a column's covers are warp-uniform shared-memory reads.
+constexpr int kGTM = 32, kGTN = 64;
 
 int gather_tiles(int m, int n) {
-  return ((m + kGT - 1) / kGT) * ((n + kGT - 1) / kGT);
+  return ((m + kGTM - 1) / kGTM) * ((n + kGTN - 1) / kGTN);
 }
 
 __device__ __forceinline__ void resolve_cover(const GatherTarget& g, int p,
@@ -129,8 +133,10 @@ __global__ void __launch_bounds__(256) k_gather(const GatherTarget* __restrict__
   if (t0 >= t1) return;
   int d = find_desc(tile_off, ntg, t0);
   int dbeg = tile_off[d], dend = tile_off[d + 1];
-  __shared__ int s_row[kGT], s_col[kGT];
-  __shared__ CoverEntry s_rc[kGT][kCover], s_cc[kGT][kCover];
+  __shared__ int s_col[kGTN];
+  __shared__ CoverEntry s_cc[kGTN][kCover];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int NC2 = NC * NC;
   for (int t = t0; t < t1; ++t) {
     while (t >= dend) {
       ++d;
@@ -139,56 +145,65 @@ __global__ void __launch_bounds__(256) k_gather(const GatherTarget* __restrict__
     }
     const GatherTarget g = tg[d];
     const int local = t - dbeg;
-    const int tiles_m = (g.m + kGT - 1) / kGT;
-    const int i0 = (local % tiles_m) * kGT, j0 = (local / tiles_m) * kGT;
-    __syncthreads();  // the previous tile's readers of s_row / s_col / covers are done
-    for (int x = threadIdx.x; x < 2 * kGT; x += blockDim.x) {
-      if (x < kGT) {
-        const int i = i0 + x;
-        const int p = (i < g.m) ? g.rows[i] : -1;
-        s_row[x] = p;
-        resolve_cover(g, p, dof_src, src_owner, ncell3, s_rc[x]);
-      } else {
-        const int y = x - kGT, j = j0 + y;
-        const int q = (j < g.n) ? g.cols[j] : -1;
-        s_col[y] = q;
-        resolve_cover(g, q, dof_src, src_owner, ncell3, s_cc[y]);
+    const int tiles_m = (g.m + kGTM - 1) / kGTM;
+    const int i0 = (local % tiles_m) * kGTM, j0 = (local / tiles_m) * kGTN;
+    __syncthreads();  // the previous tile's readers of s_col / s_cc are done
+    if (threadIdx.x < kGTN) {
+      const int j = j0 + threadIdx.x;
+      const int q = (j < g.n) ? g.cols[j] : -1;
+      s_col[threadIdx.x] = q;
+      resolve_cover(g, q, dof_src, src_owner, ncell3, s_cc[threadIdx.x]);
+    }
+    // this thread's row: DOF, stencil row and source rows
+    const int i = i0 + lane;
+    const int p = (i < g.m) ? g.rows[i] : -1;
+    CoverEntry rc[kCover];
+    resolve_cover(g, p, dof_src, src_owner, ncell3, rc);
+    const double* rp[kCover];
+    long long rld[kCover];
+#pragma unroll
+    for (int a = 0; a < kCover; ++a) {
+      rp[a] = nullptr;
+      rld[a] = 0;
+      if (rc[a].src >= 0) {
+        const SourceDesc sd = src[rc[a].src];
+        rp[a] = sd.ptr + rc[a].pos;
+        rld[a] = sd.ld;
       }
     }
     __syncthreads();
-    const long long NC2 = (long long)NC * NC;
-    for (int e = threadIdx.x; e < kGT * kGT; e += blockDim.x) {
-      const int x = e % kGT, y = e / kGT;
-      const int i = i0 + x, j = j0 + y;
-      if (i >= g.m || j >= g.n) continue;
-      const long long p = s_row[x], q = s_col[y];
-      double v = 0.0;
-      if (!(i >= g.a0_skip && j >= g.a0_skip)) {
-        const long long dd = q - p;
-        int b = -1;
-        if (dd == 0) b = 0;
-        else if (dd == -1) b = 1;
-        else if (dd == 1) b = 2;
-        else if (dd == -NC) b = 3;
-        else if (dd == NC) b = 4;
-        else if (dd == -NC2) b = 5;
-        else if (dd == NC2) b = 6;
-        if (b >= 0) v = band[b * ncell3 + p];
-      }
-#pragma unroll
-      for (int a = 0; a < kCover; ++a) {
-        const int sa = s_rc[x][a].src;
-        if (sa < 0) continue;
+    if (i < g.m) {
+      const bool row_a0 = i < g.a0_skip;
+#pragma unroll 2
+      for (int cc = warp; cc < kGTN; cc += 8) {
+        const int j = j0 + cc;
+        if (j >= g.n) break;
+        const int q = s_col[cc];
+        double v = 0.0;
+        if (row_a0 || j < g.a0_skip) {
+          const int dd = q - p;
+          int b = -1;
+          if (dd == 0) b = 0;
+          else if (dd == -1) b = 1;
+          else if (dd == 1) b = 2;
+          else if (dd == -NC) b = 3;
+          else if (dd == NC) b = 4;
+          else if (dd == -NC2) b = 5;
+          else if (dd == NC2) b = 6;
+          if (b >= 0) v = band[b * ncell3 + p];
+        }
 #pragma unroll
         for (int c = 0; c < kCover; ++c) {
-          if (s_cc[y][c].src == sa) {
-            const SourceDesc sd = src[sa];
-            v += sd.ptr[(long long)s_rc[x][a].pos + (long long)s_cc[y][c].pos * sd.ld];
-          }
+          const int sc = s_cc[cc][c].src;
+          if (sc < 0) continue;
+          const long long pc = s_cc[cc][c].pos;
+#pragma unroll
+          for (int a = 0; a < kCover; ++a)
+            if (rc[a].src == sc) v += rp[a][pc * rld[a]];
         }
+        g.out[i + (long long)j * g.ld] = v;
+        if (g.a22_out != nullptr && i < g.r && j < g.r) g.a22_out[i + (long long)j * g.r] = v;
       }
-      g.out[i + (long long)j * g.ld] = v;
-      if (g.a22_out != nullptr && i < g.r && j < g.r) g.a22_out[i + (long long)j * g.r] = v;
     }
   }
 }
@@ -1522,20 +1537,40 @@ __global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__
     if (threadIdx.x == 0 && (!(p > 1e-300) || !isfinite(p))) bad = 1;
     const double dk = sqrt(fabs(p) > 1e-300 ? fabs(p) : 1.0);
     const double idk = 1.0 / dk;
-    double lj[8];
+    // l_i = a_ik / d below the pivot, 0 elsewhere: the rank-1 update is then a
+    // plain FMA on every entry (a no-op outside rows and columns > k)
+    double lj[8], li[4];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) lj[c] = colk[buf][8 * tx + c] * idk;
+    for (int c = 0; c < 8; ++c) lj[c] = (8 * tx + c > k) ? colk[buf][8 * tx + c] * idk : 0.0;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = 4 * ty + r;
-      const double li = colk[buf][i] * idk;
+    for (int r = 0; r < 4; ++r) li[r] = (4 * ty + r > k) ? colk[buf][4 * ty + r] * idk : 0.0;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const int j = 8 * tx + c;
-        if (i > k && j > k) a[r][c] = fma(-li, lj[c], a[r][c]);
-        else if (j == k && i >= k) a[r][c] = (i == k) ? dk : li;
-        else if (i == k && j > k) a[r][c] = 0.0;
-      }
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) a[r][c] = fma(-li[r], lj[c], a[r][c]);
+    // column k becomes l (d on the diagonal), row k right of it zero
+    if (tx == (k >> 3)) {
+      const int kc = k & 7;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c == kc) {
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int i = 4 * ty + r;
+            if (i == k) a[r][c] = dk;
+            else if (i > k) a[r][c] = li[r];
+          }
+        }
+    }
+    if (ty == (k >> 2)) {
+      const int kr = k & 3;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (r == kr) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (8 * tx + c > k) a[r][c] = 0.0;
+        }
     }
   }
   if (bad) atomicOr(status, kStatusTinyPivot);
@@ -1640,11 +1675,13 @@ void launch_chol_diag(const SweepDesc* d_desc, const int* d_active, int nact, in
 // columns, computed with the reference's construction of W_full and R_skel
 // (InterpDecomp.cpp:115-137).
 // ===========================================================================
+// stage_ld > 0: the face matrix is copied into shared memory (after the
+// work arrays, at offset stage_off doubles) and the QR runs there; it is
+// copied back at the end, so M ends overwritten as without staging.
 __global__ void __launch_bounds__(512) k_id(const IdDesc* __restrict__ descs, double eps,
-                                            int* __restrict__ status) {
+                                            int* __restrict__ status, int stage_off) {
   const IdDesc d = descs[blockIdx.x];
   const int m = d.m, n = d.n;
-  double* M = d.M;
   extern __shared__ double sm[];
   double* vn1 = sm;
   double* vn2 = vn1 + n;
@@ -1655,6 +1692,12 @@ __global__ void __launch_bounds__(512) k_id(const IdDesc* __restrict__ descs, do
   int* iscratch = pos + n;               // 32 (per-warp argmax indices)
   __shared__ int s_pvt;
   __shared__ int s_k;
+  double* M = d.M;
+  if (stage_off > 0) {
+    M = sm + stage_off;
+    for (long long e = threadIdx.x; e < (long long)m * n; e += blockDim.x) M[e] = d.M[e];
+    __syncthreads();
+  }
 
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nw = nthr >> 5;
@@ -1826,6 +1869,8 @@ __global__ void __launch_bounds__(512) k_id(const IdDesc* __restrict__ descs, do
       for (int t = 0; t < a; ++t) x[t] = fma(-M[pos[t] + (long long)a * m], xa, x[t]);
     }
   }
+  if (stage_off > 0)
+    for (long long e = threadIdx.x; e < (long long)m * n; e += blockDim.x) d.M[e] = M[e];
 }
 
 // ---------------------------------------------------------------------------
@@ -2107,12 +2152,22 @@ cudaError_t launch_id_group(const IdGroupDesc* d_desc, int nd, int group, double
 }
 
 void launch_id(const IdDesc* d_desc, int nd, int max_n, double eps, int* d_status,
-               cudaStream_t s) {
+               cudaStream_t s, long long max_mn) {
   if (nd <= 0) return;
-  const size_t smem = (size_t)max_n * 2 * sizeof(double) + 64 * sizeof(double) +
-                      (size_t)max_n * 3 * sizeof(int) + 32 * sizeof(int);
+  size_t smem = (size_t)max_n * 2 * sizeof(double) + 64 * sizeof(double) +
+                (size_t)max_n * 3 * sizeof(int) + 32 * sizeof(int);
+  // faces that fit run from shared memory (the Householder updates then read
+  // and write the face on chip instead of through L2)
+  int stage_off = 0;
+  const size_t off = (smem + sizeof(double) - 1) / sizeof(double);
+  if (max_mn > 0 && (off + (size_t)max_mn) * sizeof(double) <= (size_t)200 * 1024) {
+    stage_off = (int)off;
+    smem = (off + (size_t)max_mn) * sizeof(double);
+  }
+  // narrow faces: fewer threads per face, more faces per SM
+  const int threads = max_n <= 16 ? 128 : 512;
   if (smem > 48 * 1024) ensure_smem((const void*)k_id, smem);
-  k_id<<<nd, 512, smem, s>>>(d_desc, eps, d_status);
+  k_id<<<nd, threads, smem, s>>>(d_desc, eps, d_status, stage_off);
 }
 
 // ===========================================================================
@@ -2840,10 +2895,6 @@ void launch_member_faces(const int* d_skel, const long long* d_off, const int* d
 constexpr int kRhsGroup = 4;
 constexpr int kXChunk = 256;
 
-int gemv_tiles(int m, int n, int trans) {
-  if (m <= 0 || n <= 0) return 0;
-  return trans == 0 ? (m + 255) / 256 : (n + 31) / 32;
-}
 
 __device__ __forceinline__ void gemv_emit(const GemvDesc& g, int i, int c, double y,
                                           double* u_out, long long ldu, long long contrib_ld) {
@@ -2935,24 +2986,6 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
   }
 }
 
-__global__ void __launch_bounds__(256) k_gemv(const GemvDesc* __restrict__ descs,
-                                              const int* __restrict__ tile_off, int nd,
-                                              const double* __restrict__ u_in,
-                                              double* __restrict__ u_out, int nrhs,
-                                              long long ldu, long long contrib_ld) {
-  const int di = find_desc(tile_off, nd, blockIdx.x);
-  gemv_tile(descs[di], blockIdx.x - tile_off[di], u_in, u_out, nrhs, ldu, contrib_ld);
-}
-
-__global__ void __launch_bounds__(256) k_gemv_seg(const GemvSeg* __restrict__ segs,
-                                                  const int* __restrict__ seg_off, int nseg) {
-  const int si = find_desc(seg_off, nseg, blockIdx.x);
-  const GemvSeg sg = segs[si];
-  const int t = blockIdx.x - seg_off[si];
-  const int di = find_desc(sg.toff, sg.nd, t);
-  gemv_tile(sg.desc[di], t - sg.toff[di], nullptr, nullptr, 0, 0, 0);
-}
-
 __device__ __forceinline__ int find_desc_ll(const long long* __restrict__ off, int nd,
                                             long long t) {
   int lo = 0, hi = nd - 1;
@@ -3009,12 +3042,6 @@ void launch_apply_emit(const ApplyEmitDesc* d_desc, const long long* d_off, int 
   k_apply_emit<<<blocks, 256, 0, s>>>(d_desc, d_off, nd, total, u, ldu, contrib_ld);
 }
 
-void launch_gemv_seg(const GemvSeg* d_segs, const int* d_seg_off, int nseg, int total_tiles,
-                     cudaStream_t s) {
-  if (total_tiles <= 0) return;
-  k_gemv_seg<<<total_tiles, 256, 0, s>>>(d_segs, d_seg_off, nseg);
-}
-
 __global__ void k_reduce_seg(const ReduceSeg* __restrict__ segs, const int* __restrict__ seg_off,
                              int nseg) {
   const int total = seg_off[nseg];
@@ -3036,13 +3063,177 @@ void launch_reduce_seg(const ReduceSeg* d_segs, const int* d_seg_off, int nseg, 
   k_reduce_seg<<<blocks, 256, 0, s>>>(d_segs, d_seg_off, nseg);
 }
 
-void launch_gemv(const GemvDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
-                 const double* u_in, double* u_out, int nrhs, long long ldu,
-                 long long contrib_ld, cudaStream_t s) {
-  if (total_tiles <= 0) return;
-  k_gemv<<<total_tiles, 256, 0, s>>>(d_desc, d_tile_off, nd, u_in, u_out, nrhs, ldu,
-                                     contrib_ld);
+// ---- apply GEMV, the plans' layouts ----------------------------------------
+// A launch covers segments (one per operator / request: the serving loop runs
+// several requests' stages in one launch), each a descriptor array and, for
+// the larger layouts, a unit table; seg_off holds the units' prefix over
+// segments. Every descriptor's own vectors (uin, uout, nrhs, ldu, cld) apply
+// when set, else the launch's.
+struct GemvCtx {
+  const double* uin;
+  double* uout;
+  int nrhs;
+  long long ldu, cld;
+};
+__device__ __forceinline__ GemvCtx gemv_ctx(const GemvDesc& g, const double* u_in, double* u_out,
+                                            int nrhs, long long ldu, long long cld) {
+  return g.uin ? GemvCtx{g.uin, g.uout, g.nrhs, g.ldu, g.cld}
+               : GemvCtx{u_in, u_out, nrhs, ldu, cld};
 }
+
+// Small blocks (both dimensions at most 64): one warp per descriptor. y = M x:
+// lane = row, columns in order. y = M^T x: lanes over rows, one warp sum per
+// column (fixed shuffle order). Entries above the diagonal of a triangular M
+// are not read.
+__global__ void __launch_bounds__(256) k_gemv_small(const GemvFastSeg* __restrict__ segs,
+                                                    const int* __restrict__ seg_off, int nseg,
+                                                    const double* __restrict__ u_in,
+                                                    double* __restrict__ u_out, int nrhs_k,
+                                                    long long ldu_k, long long cld_k) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int unit = blockIdx.x * 8 + warp;
+  if (unit >= seg_off[nseg]) return;
+  const int si = find_desc(seg_off, nseg, unit);
+  const GemvDesc g = segs[si].desc[unit - seg_off[si]];
+  const GemvCtx x = gemv_ctx(g, u_in, u_out, nrhs_k, ldu_k, cld_k);
+  for (int c0 = 0; c0 < x.nrhs; c0 += kRhsGroup) {
+    const int nc = min(kRhsGroup, x.nrhs - c0);
+    if (g.trans == 0) {
+      for (int i = lane; i < g.m; i += 32) {
+        double acc[kRhsGroup] = {0.0, 0.0, 0.0, 0.0};
+        const int jend = g.tri ? min(g.n, i + 1) : g.n;
+        for (int j = 0; j < jend; ++j) {
+          const double mv = g.M[i + (long long)j * g.ld];
+          const long long xo = g.in_idx[j] + (long long)c0 * x.ldu;
+#pragma unroll
+          for (int cc = 0; cc < kRhsGroup; ++cc)
+            if (cc < nc) acc[cc] = fma(mv, x.uin[xo + (long long)cc * x.ldu], acc[cc]);
+        }
+        for (int cc = 0; cc < nc; ++cc) gemv_emit(g, i, c0 + cc, acc[cc], x.uout, x.ldu, x.cld);
+      }
+    } else {
+      double xr[2][kRhsGroup];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = lane + 32 * h;
+#pragma unroll
+        for (int cc = 0; cc < kRhsGroup; ++cc)
+          xr[h][cc] = (i < g.m && cc < nc)
+                          ? x.uin[g.in_idx[i] + (long long)(c0 + cc) * x.ldu] : 0.0;
+      }
+      for (int j = 0; j < g.n; ++j) {
+        double acc[kRhsGroup] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int i = lane + 32 * h;
+          if (i < g.m && (!g.tri || i >= j)) {
+            const double mv = g.M[i + (long long)j * g.ld];
+#pragma unroll
+            for (int cc = 0; cc < kRhsGroup; ++cc) acc[cc] = fma(mv, xr[h][cc], acc[cc]);
+          }
+        }
+#pragma unroll
+        for (int cc = 0; cc < kRhsGroup; ++cc) acc[cc] = warp_sum(acc[cc]);
+        if (lane == 0)
+          for (int cc = 0; cc < nc; ++cc) gemv_emit(g, j, c0 + cc, acc[cc], x.uout, x.ldu, x.cld);
+      }
+    }
+  }
+}
+
+// Larger blocks, y = M x: a CTA takes 64 rows (two per lane) of one
+// descriptor; its eight warps split the columns into contiguous ranges and
+// their partial sums are added in warp order through shared memory, so the
+// result does not depend on scheduling. Unit = (descriptor, row strip).
+__global__ void __launch_bounds__(256) k_gemv_rows(const GemvFastSeg* __restrict__ segs,
+                                                   const int* __restrict__ seg_off, int nseg,
+                                                   const double* __restrict__ u_in,
+                                                   double* __restrict__ u_out, int nrhs_k,
+                                                   long long ldu_k, long long cld_k) {
+  const int si = find_desc(seg_off, nseg, blockIdx.x);
+  const int2 t = segs[si].tab[blockIdx.x - seg_off[si]];
+  const GemvDesc g = segs[si].desc[t.x];
+  const GemvCtx x = gemv_ctx(g, u_in, u_out, nrhs_k, ldu_k, cld_k);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i0 = t.y * 64;
+  __shared__ double red[8][64][kRhsGroup];
+  // columns this strip needs (lower triangular: none right of its last row)
+  const int ncol = g.tri ? min(g.n, i0 + 64) : g.n;
+  const int per = (ncol + 7) / 8;
+  const int j0 = warp * per, j1 = min(ncol, j0 + per);
+  const int ia = i0 + lane, ib = i0 + 32 + lane;
+  const bool va = ia < g.m, vb = ib < g.m;
+  for (int c0 = 0; c0 < x.nrhs; c0 += kRhsGroup) {
+    const int nc = min(kRhsGroup, x.nrhs - c0);
+    double acc[2][kRhsGroup];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int cc = 0; cc < kRhsGroup; ++cc) acc[h][cc] = 0.0;
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+      const long long xo = g.in_idx[j] + (long long)c0 * x.ldu;
+      double xv[kRhsGroup];
+#pragma unroll
+      for (int cc = 0; cc < kRhsGroup; ++cc)
+        xv[cc] = cc < nc ? x.uin[xo + (long long)cc * x.ldu] : 0.0;
+      const long long jo = (long long)j * g.ld;
+      const double ma = va ? g.M[ia + jo] : 0.0;
+      const double mb = vb ? g.M[ib + jo] : 0.0;
+#pragma unroll
+      for (int cc = 0; cc < kRhsGroup; ++cc) {
+        acc[0][cc] = fma(ma, xv[cc], acc[0][cc]);
+        acc[1][cc] = fma(mb, xv[cc], acc[1][cc]);
+      }
+    }
+#pragma unroll
+    for (int cc = 0; cc < kRhsGroup; ++cc) {
+      red[warp][lane][cc] = acc[0][cc];
+      red[warp][32 + lane][cc] = acc[1][cc];
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+      const int i = i0 + threadIdx.x;
+      if (i < g.m) {
+        for (int cc = 0; cc < nc; ++cc) {
+          double y = 0.0;
+#pragma unroll
+          for (int w = 0; w < 8; ++w) y += red[w][threadIdx.x][cc];
+          gemv_emit(g, i, c0 + cc, y, x.uout, x.ldu, x.cld);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Larger blocks, y = M^T x: gemv_tile's 32-column tiles, located from the unit
+// table (descriptor, tile) rather than a search over tile offsets.
+__global__ void __launch_bounds__(256) k_gemv_cols(const GemvFastSeg* __restrict__ segs,
+                                                   const int* __restrict__ seg_off, int nseg,
+                                                   const double* __restrict__ u_in,
+                                                   double* __restrict__ u_out, int nrhs,
+                                                   long long ldu, long long contrib_ld) {
+  const int si = find_desc(seg_off, nseg, blockIdx.x);
+  const int2 t = segs[si].tab[blockIdx.x - seg_off[si]];
+  gemv_tile(segs[si].desc[t.x], t.y, u_in, u_out, nrhs, ldu, contrib_ld);
+}
+
+void launch_gemv_fast(const GemvFastSeg* d_segs, const int* d_seg_off, int nseg, int units,
+                      int layout, const double* u_in, double* u_out, int nrhs, long long ldu,
+                      long long contrib_ld, cudaStream_t s) {
+  if (units <= 0) return;
+  if (layout == kGemvSmall)
+    k_gemv_small<<<(units + 7) / 8, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
+                                                 contrib_ld);
+  else if (layout == kGemvRows)
+    k_gemv_rows<<<units, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
+                                      contrib_ld);
+  else
+    k_gemv_cols<<<units, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
+                                      contrib_ld);
+}
+
 
 __global__ void k_reduce_scatter(const int* __restrict__ dof, const int* __restrict__ off,
                                  const int* __restrict__ slot,

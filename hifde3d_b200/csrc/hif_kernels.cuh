@@ -176,16 +176,7 @@ struct GemvDesc {
   long long ldu, cld;
 };
 
-// A batch of descriptor arrays (one per request) in one launch: tiles are
-// counted over segments by seg_off (prefix, device), then within a segment by
-// its own tile offsets.
-struct GemvSeg {
-  const GemvDesc* desc;
-  const int* toff;
-  int nd;
-};
-void launch_gemv_seg(const GemvSeg* d_segs, const int* d_seg_off, int nseg, int total_tiles,
-                     cudaStream_t s);
+// The serving loop's batched reduce-scatter: one segment per request.
 struct ReduceSeg {
   const int* dof;
   const int* off;
@@ -342,7 +333,7 @@ void launch_sweep_setdiag(const SweepDesc* d_desc, const int* d_active, int nact
 // Column-pivoted Householder QR + rank + interpolation matrix, one CTA per face.
 // W is written to IdDesc::W, which must hold at least n*n/4 + n doubles.
 void launch_id(const IdDesc* d_desc, int nd, int max_n, double eps, int* d_status,
-               cudaStream_t s);
+               cudaStream_t s, long long max_mn = 0);
 
 void launch_copy(const CopyDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
                  cudaStream_t s);
@@ -421,10 +412,21 @@ void launch_trsm_upper(const double* R, long long ldr, int k, double* B, long lo
 int copy_tiles(int m, int n);
 
 // contrib_ld: stride between right-hand sides in the contribution buffer.
-void launch_gemv(const GemvDesc* d_desc, const int* d_tile_off, int nd, int total_tiles,
-                 const double* u_in, double* u_out, int nrhs, long long ldu,
-                 long long contrib_ld, cudaStream_t s);
-int gemv_tiles(int m, int n, int trans);
+// The apply's GEMV launches (the engine's plans and the serving loop's batched
+// stages). Layouts: kGemvSmall, one warp per descriptor (both dimensions <=
+// kGemvSmallMax; units = descriptors); kGemvRows, y = M x by 64-row strips;
+// kGemvCols, y = M^T x by 32-column tiles (units = entries (descriptor, strip /
+// tile) of the segment's table). A launch covers segments (one per operator or
+// request) of one layout; seg_off: prefix of the units over the segments.
+constexpr int kGemvSmall = 0, kGemvRows = 1, kGemvCols = 2;
+constexpr int kGemvSmallMax = 64;
+struct GemvFastSeg {
+  const GemvDesc* desc;
+  const int2* tab;  // null for kGemvSmall
+};
+void launch_gemv_fast(const GemvFastSeg* d_segs, const int* d_seg_off, int nseg, int units,
+                      int layout, const double* u_in, double* u_out, int nrhs, long long ldu,
+                      long long contrib_ld, cudaStream_t s);
 
 // u[dof[d]] += alpha * sum_{t in [off[d], off[d+1])} contrib[slot[t]], in order.
 void launch_reduce_scatter(const int* d_dof, const int* d_off, const int* d_slot,

@@ -238,12 +238,13 @@ class Server {
         e->factor();
         e->sync();
         peak = (long long)(e->arena_factor.reserved() + e->arena_work[0].reserved() +
-                           e->arena_work[1].reserved());
+                           e->arena_work[1].reserved() + e->arena_desc.reserved());
         e->stage.release();
         e->arena_work[0].release();
         e->arena_work[1].release();
         e->release_workspace();  // solves use their own vectors
-        keep = (long long)e->arena_factor.reserved() + 7LL * e->n3 * 8;
+        keep = (long long)(e->arena_factor.reserved() + e->arena_desc.reserved()) +
+               7LL * e->n3 * 8;
       } catch (const Error& x) {
         st = x.code;
         err = x.msg;
@@ -292,9 +293,10 @@ class Server {
     struct L {
       long long key;
       int type;
-      GemvSeg gs;
+      GemvFastSeg gs;  // descriptors bound to this request's vectors
+      int layout;
       ReduceSeg rs;
-      int tiles;
+      int tiles;  // units of the GEMV layout, or reduced entries
     };
     std::vector<L> launches;
     BufList bufs;
@@ -338,9 +340,9 @@ class Server {
           if (g.mode == 1) g.contrib = a.contrib + (g.contrib - e.d_contrib);
         }
         x.gs.desc = a.bufs.add(upload(dd, sstream_));
-        x.gs.toff = l.d_toff;
-        x.gs.nd = l.nd;
-        x.tiles = l.tiles;
+        x.gs.tab = l.d_tab;
+        x.layout = l.layout;
+        x.tiles = l.units;
       } else {
         x.rs = ReduceSeg{l.d_dof, l.d_off, l.d_slot, a.contrib, vec[l.out_vec], cl, a.n3, l.ndof,
                          a.nrhs, l.alpha};
@@ -367,24 +369,28 @@ class Server {
       for (size_t i = 0; i < a->launches.size(); ++i) stages[a->launches[i].key].push_back({a, i});
     BufList tick;
     for (auto& kv : stages) {
-      std::vector<GemvSeg> gs;
-      std::vector<int> goff(1, 0);
+      // one launch per GEMV layout present at this stage (the same kernels as
+      // hif_apply's, so each request computes exactly what it would alone)
+      std::vector<GemvFastSeg> gs[3];
+      std::vector<int> goff[3] = {{0}, {0}, {0}};
       std::vector<ReduceSeg> rs;
       std::vector<int> roff(1, 0);
       for (auto& pr : kv.second) {
         const Active::L& l = pr.first->launches[pr.second];
         if (l.type == 0) {
-          gs.push_back(l.gs);
-          goff.push_back(goff.back() + l.tiles);
+          gs[l.layout].push_back(l.gs);
+          goff[l.layout].push_back(goff[l.layout].back() + l.tiles);
         } else {
           rs.push_back(l.rs);
           roff.push_back(roff.back() + l.tiles);
         }
       }
-      if (!gs.empty() && goff.back() > 0) {
-        GemvSeg* dg = tick.add(upload(gs, sstream_));
-        int* dgo = tick.add(upload(goff, sstream_));
-        launch_gemv_seg(dg, dgo, (int)gs.size(), goff.back(), sstream_);
+      for (int lay = 0; lay < 3; ++lay) {
+        if (gs[lay].empty() || goff[lay].back() == 0) continue;
+        GemvFastSeg* dg = tick.add(upload(gs[lay], sstream_));
+        int* dgo = tick.add(upload(goff[lay], sstream_));
+        launch_gemv_fast(dg, dgo, (int)gs[lay].size(), goff[lay].back(), lay, nullptr, nullptr, 0,
+                         0, 0, sstream_);
         ++merged_launches_;
       }
       if (!rs.empty() && roff.back() > 0) {
