@@ -616,12 +616,17 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
   ScratchScope scope;
   const int bn = oz_tile_n(slices);
   constexpr int kChunkTiles = kOzMaxK / kOzK;
+  // op(B)^T = op(A) (the S = A11 - Y^T Y products): B's converted rows are A's
+  auto same_operand = [](const GemmDesc& x) {
+    return x.A == x.B && x.lda == x.ldb && x.transA == 1 && x.transB == 0 && x.m == x.n;
+  };
   long long parts = 0, nexp = 0;
   for (const GemmDesc& x : gin) {
     if (x.m <= 0 || x.n <= 0) continue;
     const long long kt = (x.k + kOzK - 1) / kOzK;
-    parts += ((x.m + 127) / 128 + (x.n + 127) / 128) * kt * slices;
-    nexp += x.m + x.n;
+    const bool same = same_operand(x);
+    parts += ((x.m + 127) / 128 + (same ? 0 : (x.n + 127) / 128)) * kt * slices;
+    nexp += x.m + (same ? 0 : x.n);
   }
   if (nexp == 0) return;
   signed char* cbuf = scratch_alloc<signed char>(std::max(1LL, parts) * kOzPart, tmp, stream);
@@ -648,19 +653,22 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
       }
       fl += pairs * 2.0 * 128.0 * bn * kOzK * tk;
     }
-    const int ta = (x.m + 127) / 128 * kt, tb = (x.n + 127) / 128 * kt;
+    const bool same = same_operand(x);
+    const int ta = (x.m + 127) / 128 * kt, tb = same ? 0 : (x.n + 127) / 128 * kt;
     signed char* pa = cbuf + used * kOzPart;
-    signed char* pb = cbuf + (used + (long long)ta * slices) * kOzPart;
+    signed char* pb = same ? pa : cbuf + (used + (long long)ta * slices) * kOzPart;
     used += (long long)(ta + tb) * slices;
     int* ea = ebuf + eo;
-    int* eb = ea + x.m;
-    eo += x.m + x.n;
+    int* eb = same ? ea : ea + x.m;
+    eo += x.m + (same ? 0 : x.n);
     if (kt > 0) {
       // A: element (i, kk) = op(A)[i, kk]; B: element (j, kk) = op(B)[kk, j]
       ops.push_back(OzOperand{x.A, x.lda, x.transA, x.m, x.k, pa, ea});
       ooff.push_back(ooff.back() + ta);
-      ops.push_back(OzOperand{x.B, x.ldb, x.transB ? 0 : 1, x.n, x.k, pb, eb});
-      ooff.push_back(ooff.back() + tb);
+      if (!same) {
+        ops.push_back(OzOperand{x.B, x.ldb, x.transB ? 0 : 1, x.n, x.k, pb, eb});
+        ooff.push_back(ooff.back() + tb);
+      }
     }
     for (int c = 0, kt0 = 0; kt0 < kt || c == 0; ++c, kt0 += kChunkTiles) {
       if ((int)launches.size() <= c) launches.emplace_back();
@@ -2997,10 +3005,17 @@ class Engine {
       }
     }
     mark("end", L);
+    // The apply sweeps are part of the factorization's output. Their plans
+    // depend on the index data and the factor's addresses only, all known on
+    // the host now: they are built while the device finishes the last levels.
+    const double tp = wall();
+    ensure_workspace(1);
+    t_plan = wall() - tp;
     sync();
     t_total = wall() - t0;
     tuner.resolve();
     report_marks();
+    if (verbose) std::fprintf(stderr, "[hif]   apply plans built in %.3f ms (host)\n", 1e3 * t_plan);
     int st = 0;
     HIF_CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
     factored = true;
@@ -3009,12 +3024,6 @@ class Engine {
     if (st & kStatusTimeout)
       throw Error{HIF_ERR_CUDA, "a bounded device wait timed out (grouped ID barrier or tensor-core "
                                 "pipeline)"};
-    // the apply sweeps are part of the factorization's output: build them now
-    const double tp = wall();
-    ensure_workspace(1);
-    sync();
-    t_plan = wall() - tp;
-    if (verbose) std::fprintf(stderr, "[hif]   apply plans built in %.3f ms\n", 1e3 * t_plan);
     if (profile) resolve_profile();
   }
 
@@ -4005,7 +4014,7 @@ int hif_factor_stats(hif_handle h, double* total_s, double* gather_s, double* el
                      double* id_s, double* host_s, long long* device_bytes) {
   if (!h) return HIF_ERR_ARG;
   hif::Engine& e = *h->e;
-  if (total_s) *total_s = e.t_total + e.t_plan;
+  if (total_s) *total_s = e.t_total;  // the apply plans included (built before its end)
   if (gather_s) *gather_s = e.t_gather;
   if (elim_s) *elim_s = e.t_elim;
   if (id_s) *id_s = e.t_id;

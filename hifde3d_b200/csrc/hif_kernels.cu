@@ -889,27 +889,46 @@ void launch_gemm_tc(const TcGemm* d_desc, const int* d_tile_off, int nd, int tot
 // tcgen05.commit; warps 4-7 wait for the last products and write C. Waits are
 // bounded as in k_gemm_tc.
 // ===========================================================================
+// Tile (128 rows x 64 k) of an operand into shared memory, read along the
+// operand's contiguous dimension: for trans = 0 lanes run over rows, for
+// trans = 1 over k, so that both layouts are read in whole cache lines.
+// T[i * kOzTs + k]; entries past the operand are zero.
+constexpr int kOzTs = kOzK + 1;
+constexpr size_t kOzConvSmem = (size_t)128 * kOzTs * sizeof(double);
+__device__ __forceinline__ void oz_load_tile(const OzOperand& o, int rt, int kt, double* T) {
+  const int r0 = rt * 128, k0 = kt * kOzK;
+  if (o.trans == 0) {
+    for (int e = threadIdx.x; e < 128 * kOzK; e += blockDim.x) {
+      const int i = e & 127, k = e >> 7;
+      const int gi = r0 + i, gk = k0 + k;
+      T[i * kOzTs + k] = (gi < o.rows && gk < o.kdim) ? o.X[gi + (long long)gk * o.ld] : 0.0;
+    }
+  } else {
+    for (int e = threadIdx.x; e < 128 * kOzK; e += blockDim.x) {
+      const int k = e & (kOzK - 1), i = e / kOzK;
+      const int gi = r0 + i, gk = k0 + k;
+      T[i * kOzTs + k] = (gi < o.rows && gk < o.kdim) ? o.X[gk + (long long)gi * o.ld] : 0.0;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) k_oz_exp(const OzOperand* __restrict__ ops,
                                                 const int* __restrict__ tile_off, int nops) {
+  extern __shared__ double oz_t[];
   const int oi = find_desc(tile_off, nops, blockIdx.x);
   const OzOperand o = ops[oi];
   const int local = blockIdx.x - tile_off[oi];
   const int kt_n = (o.kdim + kOzK - 1) / kOzK;
   const int rt = local / kt_n, kt = local % kt_n;
+  oz_load_tile(o, rt, kt, oz_t);
+  __syncthreads();
+  // two threads per row, 32 k each
   const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
   const int gi = rt * 128 + row;
-  if (gi >= o.rows) return;
-  const int k0 = kt * kOzK + 32 * half;
   double m = 0.0;
 #pragma unroll 8
-  for (int e = 0; e < 32; ++e) {
-    const int gk = k0 + e;
-    if (gk < o.kdim) {
-      const double x = o.trans ? o.X[gk + (long long)gi * o.ld] : o.X[gi + (long long)gk * o.ld];
-      m = fmax(m, fabs(x));
-    }
-  }
-  if (m > 0.0) {
+  for (int e = 0; e < 32; ++e) m = fmax(m, fabs(oz_t[row * kOzTs + 32 * half + e]));
+  if (gi < o.rows && m > 0.0) {
     int ex;
     frexp(m, &ex);  // m < 2^ex
     atomicMax(&o.rexp[gi], ex);
@@ -919,11 +938,14 @@ __global__ void __launch_bounds__(256) k_oz_exp(const OzOperand* __restrict__ op
 __global__ void __launch_bounds__(256) k_oz_slice(const OzOperand* __restrict__ ops,
                                                   const int* __restrict__ tile_off, int nops,
                                                   int S) {
+  extern __shared__ double oz_t[];
   const int oi = find_desc(tile_off, nops, blockIdx.x);
   const OzOperand o = ops[oi];
   const int local = blockIdx.x - tile_off[oi];
   const int kt_n = (o.kdim + kOzK - 1) / kOzK;
   const int rt = local / kt_n, kt = local % kt_n;
+  oz_load_tile(o, rt, kt, oz_t);
+  __syncthreads();
   const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
   const int gi = rt * 128 + row;
   // rows without a nonzero keep the cleared exponent; their slices are zero
@@ -939,11 +961,7 @@ __global__ void __launch_bounds__(256) k_oz_slice(const OzOperand* __restrict__ 
       for (int s = 0; s < kOzMaxS; ++s) w[s][q] = 0u;
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
-        const int gk = kt * kOzK + 16 * kc + 4 * q + b;
-        const double x = (gi < o.rows && gk < o.kdim)
-                             ? (o.trans ? o.X[gk + (long long)gi * o.ld]
-                                        : o.X[gi + (long long)gk * o.ld])
-                             : 0.0;
+        const double x = oz_t[row * kOzTs + 16 * kc + 4 * q + b];
         double v = ldexp(x, -ex);  // |v| < 1
 #pragma unroll
         for (int s = 0; s < kOzMaxS; ++s) {
@@ -970,8 +988,10 @@ void launch_oz_convert(const OzOperand* d_ops, const int* d_tile_off, int nops, 
   if (total_tiles <= 0) return;
   // 0x80808080: below every exponent a double can have
   cudaMemsetAsync(d_rexp, 0x80, (size_t)n_rexp * sizeof(int), s);
-  k_oz_exp<<<total_tiles, 256, 0, s>>>(d_ops, d_tile_off, nops);
-  k_oz_slice<<<total_tiles, 256, 0, s>>>(d_ops, d_tile_off, nops, slices);
+  ensure_smem((const void*)k_oz_exp, kOzConvSmem);
+  ensure_smem((const void*)k_oz_slice, kOzConvSmem);
+  k_oz_exp<<<total_tiles, 256, kOzConvSmem, s>>>(d_ops, d_tile_off, nops);
+  k_oz_slice<<<total_tiles, 256, kOzConvSmem, s>>>(d_ops, d_tile_off, nops, slices);
 }
 
 // Shared-memory matrix descriptor: K-major, no swizzle, LBO 128 B, SBO 512 B.
@@ -1488,15 +1508,22 @@ void launch_chol_small(const SweepDesc* d_desc, int nd, int max_n, int* d_status
   k_chol_small<<<nd, 256, smem, s>>>(d_desc, d_status);
 }
 
-// Pivot block of the blocked Cholesky, with the block in registers as in
-// k_sweep_diag (thread (tx, ty) of a 16 x 32 grid holds rows 4 ty.., columns
-// 8 tx..). The trailing part is kept symmetric (both triangles updated), so
-// column k is also row k: its owners publish it to shared memory (two
-// alternating buffers, one barrier per step). Step k: d = sqrt(a_kk),
-// l_i = a_ik / d; a_ij -= l_i l_j for i, j > k; column k = l (d on the
-// diagonal), row k right of the diagonal = 0. L goes back over B[K, K]; then
-// the same registers run the Gauss-Jordan inverse of L (lower triangular, so
-// its zeros stay zero) into dinv.
+// Pivot block of the blocked Cholesky: L_KK = chol(D) over B[K, K] (zeros
+// above the diagonal) and L_KK^{-1} into dinv, with D (128 x 128, lower
+// triangle read, padded with the identity past nb) in shared memory. Blocked
+// by 32-wide panels so that a block costs a few dozen barriers, not one per
+// pivot (this kernel is on the critical path of the top levels, where one or
+// a few blocks remain):
+//   for each panel p: warp 0 factors the 32 x 32 diagonal block and inverts
+//   it (warp-synchronous), the CTA solves the rows below against it and
+//   updates the trailing lower triangle;
+//   then L^{-1} in place, block column by block column from the left:
+//   X_jj = L_jj^{-1}, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj (i > j).
+constexpr int kCdP = 32;             // panel width
+constexpr int kCdXs = kCdP + 1;      // padded stride of the diagonal inverses
+constexpr size_t kCholDiagSmem =
+    (size_t)(kSweepNB * kSweepNB + 4 * kCdP * kCdXs + kCdP * kCdXs) * sizeof(double);
+
 __global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__ descs,
                                                    const int* __restrict__ active, int k0,
                                                    double* __restrict__ dinv,
@@ -1504,164 +1531,136 @@ __global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__
   const int di = active[blockIdx.x];
   const SweepDesc d = descs[di];
   const int nb = min(kSweepNB, d.r - k0);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  __shared__ double colk[2][kSweepNB];
-  extern __shared__ double dg_sm[];  // kSweepNB x kSweepNB staging
-  for (int e = threadIdx.x; e < kSweepNB * kSweepNB; e += blockDim.x) {
-    const int i = e & (kSweepNB - 1), j = e / kSweepNB;
-    const int ii = i < j ? j : i, jj = i < j ? i : j;
-    dg_sm[e] = (i < nb && j < nb) ? d.B[(k0 + ii) + (long long)(k0 + jj) * d.n] : 0.0;
+  constexpr int T = kSweepNB;  // tile edge; column-major S[i + j T]
+  extern __shared__ double cd_sm[];
+  double* S = cd_sm;
+  double* Xd = S + T * T;              // 4 diagonal inverses, [p][c][i] = X_pp(i, c)
+  double* Tb = Xd + 4 * kCdP * kCdXs;  // 32 x 32 product scratch, [c][i]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < T * T; e += blockDim.x) {
+    const int i = e % T, j = e / T;
+    double v;
+    if (i < nb && j < nb) v = d.B[(k0 + max(i, j)) + (long long)(k0 + min(i, j)) * d.n];
+    else v = (i == j) ? 1.0 : 0.0;
+    S[e] = v;
   }
   __syncthreads();
-  double a[4][8];
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 8; ++c) a[r][c] = dg_sm[(4 * ty + r) + (8 * tx + c) * kSweepNB];
   int bad = 0;
-  for (int k = 0; k < nb; ++k) {
-    const int buf = k & 1;
-    if (tx == (k >> 3)) {
-      const int kc = k & 7;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        double v = a[r][0];
-#pragma unroll
-        for (int c = 1; c < 8; ++c)
-          if (c == kc) v = a[r][c];
-        colk[buf][4 * ty + r] = v;
+  for (int p = 0; p < T / kCdP; ++p) {
+    const int o = p * kCdP;
+    double* X = Xd + p * kCdP * kCdXs;
+    if (warp == 0) {
+      // Cholesky of the 32 x 32 diagonal block, lane = row
+      for (int k = 0; k < kCdP; ++k) {
+        const double pv = S[(o + k) + (o + k) * T];
+        if (lane == 0 && o + k < nb && (!(pv > 1e-300) || !isfinite(pv))) bad = 1;
+        const double dk = sqrt(fabs(pv) > 1e-300 ? fabs(pv) : 1.0);
+        __syncwarp();
+        if (lane > k) S[(o + lane) + (o + k) * T] /= dk;
+        if (lane == k) S[(o + k) + (o + k) * T] = dk;
+        __syncwarp();
+        if (lane > k) {
+          const double lik = S[(o + lane) + (o + k) * T];
+          for (int j = k + 1; j <= lane; ++j)
+            S[(o + lane) + (o + j) * T] =
+                fma(-lik, S[(o + j) + (o + k) * T], S[(o + lane) + (o + j) * T]);
+        }
+        __syncwarp();
+      }
+      // its inverse, lane = column c: X(c, c) = 1 / l_cc,
+      // X(i, c) = -(sum_{k=c}^{i-1} l_ik X(k, c)) / l_ii
+      const int c = lane;
+      X[c * kCdXs + c] = 1.0 / S[(o + c) + (o + c) * T];
+      for (int i = 0; i < kCdP; ++i) {
+        if (i > c) {
+          double acc = 0.0;
+          for (int k = c; k < i; ++k) acc = fma(S[(o + i) + (o + k) * T], X[c * kCdXs + k], acc);
+          X[c * kCdXs + i] = -acc / S[(o + i) + (o + i) * T];
+        } else if (i < c) {
+          X[c * kCdXs + i] = 0.0;
+        }
       }
     }
     __syncthreads();
-    const double p = colk[buf][k];
-    if (threadIdx.x == 0 && (!(p > 1e-300) || !isfinite(p))) bad = 1;
-    const double dk = sqrt(fabs(p) > 1e-300 ? fabs(p) : 1.0);
-    const double idk = 1.0 / dk;
-    // l_i = a_ik / d below the pivot, 0 elsewhere: the rank-1 update is then a
-    // plain FMA on every entry (a no-op outside rows and columns > k)
-    double lj[8], li[4];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) lj[c] = (8 * tx + c > k) ? colk[buf][8 * tx + c] * idk : 0.0;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) li[r] = (4 * ty + r > k) ? colk[buf][4 * ty + r] * idk : 0.0;
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int c = 0; c < 8; ++c) a[r][c] = fma(-li[r], lj[c], a[r][c]);
-    // column k becomes l (d on the diagonal), row k right of it zero
-    if (tx == (k >> 3)) {
-      const int kc = k & 7;
-#pragma unroll
-      for (int c = 0; c < 8; ++c)
-        if (c == kc) {
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            const int i = 4 * ty + r;
-            if (i == k) a[r][c] = dk;
-            else if (i > k) a[r][c] = li[r];
-          }
-        }
-    }
-    if (ty == (k >> 2)) {
-      const int kr = k & 3;
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-        if (r == kr) {
-#pragma unroll
-          for (int c = 0; c < 8; ++c)
-            if (8 * tx + c > k) a[r][c] = 0.0;
-        }
+    const int r0 = o + kCdP, nrow = T - r0;
+    if (nrow > 0) {
+      // panel rows below: L_ip = A_ip X_pp^T (computed, then written)
+      double outv[6];
+      int cnt = 0;
+      for (int e = tid; e < nrow * kCdP; e += blockDim.x, ++cnt) {
+        const int i = r0 + e % nrow, c = e / nrow;
+        double acc = 0.0;
+        // (A_ip X^T)(i, c) = sum_{k <= c} A(i, k) X(c, k); X(c, k) at X[k * kCdXs + c]
+        for (int k = 0; k <= c; ++k) acc = fma(S[i + (o + k) * T], X[k * kCdXs + c], acc);
+        outv[cnt] = acc;
+      }
+      __syncthreads();
+      cnt = 0;
+      for (int e = tid; e < nrow * kCdP; e += blockDim.x, ++cnt) {
+        const int i = r0 + e % nrow, c = e / nrow;
+        S[i + (o + c) * T] = outv[cnt];
+      }
+      __syncthreads();
+      // trailing lower triangle: A_ij -= L_ip L_jp^T
+      for (int e = tid; e < nrow * nrow; e += blockDim.x) {
+        const int i = r0 + e % nrow, j = r0 + e / nrow;
+        if (i < j) continue;
+        double acc = S[i + j * T];
+#pragma unroll 8
+        for (int k = 0; k < kCdP; ++k) acc = fma(-S[i + (o + k) * T], S[j + (o + k) * T], acc);
+        S[i + j * T] = acc;
+      }
+      __syncthreads();
     }
   }
   if (bad) atomicOr(status, kStatusTinyPivot);
   // L over B[K, K]
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 8; ++c) dg_sm[(4 * ty + r) + (8 * tx + c) * kSweepNB] = a[r][c];
-  __syncthreads();
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+  for (int e = tid; e < nb * nb; e += blockDim.x) {
     const int i = e % nb, j = e / nb;
-    d.B[(k0 + i) + (long long)(k0 + j) * d.n] = dg_sm[i + j * kSweepNB];
+    d.B[(k0 + i) + (long long)(k0 + j) * d.n] = (i >= j) ? S[i + j * T] : 0.0;
   }
-  // L^{-1} by the Gauss-Jordan steps of k_sweep_diag (pivots are the positive
-  // diagonal of L; padding beyond nb is never pivoted)
-  __shared__ double rowk[2][kSweepNB];
-  for (int k = 0; k < nb; ++k) {
-    const int buf = k & 1;
-    if (ty == (k >> 2)) {
-      const int kr = k & 3;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        double v = a[0][c];
-#pragma unroll
-        for (int r = 1; r < 4; ++r)
-          if (r == kr) v = a[r][c];
-        rowk[buf][8 * tx + c] = v;
-      }
-    }
-    if (tx == (k >> 3)) {
-      const int kc = k & 7;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        double v = a[r][0];
-#pragma unroll
-        for (int c = 1; c < 8; ++c)
-          if (c == kc) v = a[r][c];
-        colk[buf][4 * ty + r] = v;
-      }
+  __syncthreads();
+  // L^{-1} in place, block columns from the left
+  for (int jb = 0; jb < T / kCdP; ++jb) {
+    const int oj = jb * kCdP;
+    for (int e = tid; e < kCdP * kCdP; e += blockDim.x) {
+      const int i = e % kCdP, c = e / kCdP;
+      S[(oj + i) + (oj + c) * T] = Xd[jb * kCdP * kCdXs + c * kCdXs + i];
     }
     __syncthreads();
-    const double ip = 1.0 / rowk[buf][k];
-    double rj[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) rj[c] = rowk[buf][8 * tx + c] * ip;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const double cir = colk[buf][4 * ty + r];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) a[r][c] = fma(-cir, rj[c], a[r][c]);
-    }
-    if (ty == (k >> 2)) {
-      const int kr = k & 3;
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-        if (r == kr) {
-#pragma unroll
-          for (int c = 0; c < 8; ++c) a[r][c] = rj[c];
-        }
-    }
-    if (tx == (k >> 3)) {
-      const int kc = k & 7;
-#pragma unroll
-      for (int c = 0; c < 8; ++c)
-        if (c == kc) {
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-            a[r][c] = (4 * ty + r == k) ? ip : colk[buf][4 * ty + r] * -ip;
-        }
+    for (int ib = jb + 1; ib < T / kCdP; ++ib) {
+      const int oi = ib * kCdP;
+      // Tb = sum_{k in [oj, oi)} L(oi.., k) X(k, oj..)
+      for (int e = tid; e < kCdP * kCdP; e += blockDim.x) {
+        const int i = e % kCdP, c = e / kCdP;
+        double acc = 0.0;
+        for (int k = oj; k < oi; ++k) acc = fma(S[(oi + i) + k * T], S[k + (oj + c) * T], acc);
+        Tb[c * kCdXs + i] = acc;
+      }
+      __syncthreads();
+      // X(ib, jb) = -X_ib,ib Tb
+      const double* Xi = Xd + ib * kCdP * kCdXs;
+      for (int e = tid; e < kCdP * kCdP; e += blockDim.x) {
+        const int i = e % kCdP, c = e / kCdP;
+        double acc = 0.0;
+        for (int k = 0; k <= i; ++k) acc = fma(Xi[k * kCdXs + i], Tb[c * kCdXs + k], acc);
+        S[(oi + i) + (oj + c) * T] = -acc;
+      }
+      __syncthreads();
     }
   }
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 8; ++c) dg_sm[(4 * ty + r) + (8 * tx + c) * kSweepNB] = a[r][c];
-  __syncthreads();
   double* out = dinv + (long long)di * kSweepNB * kSweepNB;
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+  for (int e = tid; e < nb * nb; e += blockDim.x) {
     const int i = e % nb, j = e / nb;
-    out[e] = (i >= j) ? dg_sm[i + j * kSweepNB] : 0.0;
+    out[e] = (i >= j) ? S[i + j * T] : 0.0;
   }
 }
 
 void launch_chol_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
                       double* d_dinv, int* d_status, cudaStream_t s) {
   if (nact <= 0) return;
-  const int smem = kSweepNB * kSweepNB * (int)sizeof(double);
-  ensure_smem((const void*)k_chol_diag, smem);
-  k_chol_diag<<<nact, 512, smem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
+  ensure_smem((const void*)k_chol_diag, kCholDiagSmem);
+  k_chol_diag<<<nact, 512, kCholDiagSmem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
 }
 
 // ===========================================================================
@@ -3133,7 +3132,8 @@ __global__ void __launch_bounds__(256) k_gemv_small(const GemvFastSeg* __restric
           }
         }
 #pragma unroll
-        for (int cc = 0; cc < kRhsGroup; ++cc) acc[cc] = warp_sum(acc[cc]);
+        for (int cc = 0; cc < kRhsGroup; ++cc)
+          if (cc < nc) acc[cc] = warp_sum(acc[cc]);  // nc is the same on every lane
         if (lane == 0)
           for (int cc = 0; cc < nc; ++cc) gemv_emit(g, j, c0 + cc, acc[cc], x.uout, x.ldu, x.cld);
       }
