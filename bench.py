@@ -723,9 +723,12 @@ def run_ours(args, rank: int, world: int):
         "data": "synthetic",
         "config": {**workload_config(n, eps, world),
                    "arithmetic": ("FP64" if head_prec == hb.PRECISION_FP64 else
-                                  "mixed: Schur complements from 5 and X from 7 int8 slices "
-                                  "per value on the tcgen05 tensor cores (exact int32 sums), "
-                                  "FP64 A22^-1 / pivots / storage / residual"),
+                                  "mixed: the long-K products of every elimination (S, and "
+                                  "Y = L^-1 A21 or X = A22^-1 A21) from int8 slices per value "
+                                  "(5 for S, 6 for Y, 7 for X) on the tcgen05 tensor cores "
+                                  "(exact int32 sums); FP64 diagonal-block factorization "
+                                  "(Cholesky or Gauss-Jordan, chosen per phase by the tuner), "
+                                  "ID pivots and rank, factor storage and PCG residual"),
                    "l2_flush": "256 MB write per step",
                    "inputs": "coefficients and rhs resident in HBM"},
         "factor_s": float(np.mean(fac)),

@@ -31,7 +31,7 @@ HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET, HIF_ERR_IO = 5, 6, 7, 8
 PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
 OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE, OPT_ID_GROUP_MIN_N = 1, 2, 3, 4, 5
 OPT_PRECISION, OPT_AUTOTUNE, OPT_SCHUR_SLICES, OPT_X_SLICES = 6, 7, 8, 9
-OPT_ELIMINATION, OPT_Y_SLICES, OPT_GRAM_MIN_N = 10, 11, 12
+OPT_ELIMINATION, OPT_Y_SLICES, OPT_GRAM_MIN_N, OPT_GRAM_SLICES = 10, 11, 12, 13
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 ELIM_AUTO, ELIM_GAUSS_JORDAN, ELIM_CHOLESKY = 0, 1, 2
 KCLASS_NAMES = ["gather", "gemm", "sweep_small", "sweep_panel", "id", "gemv", "copy", "vector",
@@ -82,6 +82,7 @@ _SIGNATURES = {
     "hif_factor_stats": [_p, _dp, _dp, _dp, _dp, _dp, _llp],
     "hif_kernel_stats": [_p, _i, _llp, _dp, _dp, _dp],
     "hif_autotune_stats": [_p, _ip, _ip, _ip],
+    "hif_autotune_elimination": [_p, _ip, _ip, _ip],
     "hif_memory": [_p, _llp, _llp],
     "hif_trim": [_p],
     "hif_trim_device_pool": [],
@@ -373,7 +374,12 @@ class HIFFactor:
         n, d, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(lib().hif_autotune_stats(self._h, ctypes.byref(n), ctypes.byref(d),
                                         ctypes.byref(c)))
-        return {"signatures": n.value, "decided": d.value, "chose_128": c.value}
+        e_n, e_d, e_c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().hif_autotune_elimination(self._h, ctypes.byref(e_n), ctypes.byref(e_d),
+                                              ctypes.byref(e_c)))
+        return {"signatures": n.value, "decided": d.value, "chose_128": c.value,
+                "elimination_phases": e_n.value, "elimination_decided": e_d.value,
+                "elimination_chose_cholesky": e_c.value}
 
     def memory(self) -> dict:
         fb, wb = ctypes.c_longlong(), ctypes.c_longlong()

@@ -1706,15 +1706,48 @@ class Engine {
   // ---- dense elimination of a batch of blocks ---------------------------
   // descs[b].B holds [A22 A21; A12 A11] (ld n); on return the compact
   // A22^{-1}, X are written and B's trailing block holds A11 - A12 X.
-  void run_sweep(const std::vector<SweepDesc>& descs, BufList& tmp) {
+  // Elimination of one phase's blocks. With HIF_OPT_AUTOTUNE in mixed precision
+  // on a symmetric operator (and HIF_ELIM_AUTO), the method is tuned per phase
+  // signature (kind, level, log2 buckets of the block count and mean size):
+  // the first factorizations run it once with each method, timed by CUDA
+  // events, and the faster is kept. st.chol records the method used.
+  static constexpr long long kTuneElimKey = 1LL << 62;
+  void run_sweep(const std::vector<SweepDesc>& descs, BufList& tmp, StepData& st) {
+    bool chol = use_chol;
+    GemmTuner::Pending tp{0, -1, nullptr, nullptr};
+    if (t_tuner && symmetric && precision == HIF_PRECISION_MIXED &&
+        elimination == HIF_ELIM_AUTO && !descs.empty()) {
+      double sn = 0;
+      for (const SweepDesc& d : descs) sn += d.n;
+      const long long key = kTuneElimKey | ((long long)(st.skel ? 1 : 0) << 40) |
+                            ((long long)st.level << 32) |
+                            ((long long)ilog2_bucket((double)descs.size()) << 16) |
+                            ilog2_bucket(sn / descs.size());
+      GemmTuner::Rec& r = t_tuner->recs[key];
+      if (r.choice >= 0) {
+        chol = r.choice == 1;
+      } else {
+        tp.key = key;
+        tp.cand = r.runs[0] == 0 ? 0 : 1;
+        chol = tp.cand == 1;
+        HIF_CK(cudaEventCreate(&tp.a));
+        HIF_CK(cudaEventCreate(&tp.b));
+        HIF_CK(cudaEventRecord(tp.a, stream));
+      }
+    }
+    st.chol = chol;
     ElimArith ar;
     if (precision == HIF_PRECISION_MIXED) {
       ar.schur = schur_slices;
-      ar.x = use_chol ? y_slices : x_slices;
+      ar.x = chol ? y_slices : x_slices;
     }
     auto tm = [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); };
-    if (use_chol) chol_blocks(descs, tmp, stream, d_status, tm, ar, cur_work);
+    if (chol) chol_blocks(descs, tmp, stream, d_status, tm, ar, cur_work);
     else sweep_blocks(descs, tmp, stream, d_status, tm, ar, symmetric, cur_work);
+    if (tp.cand >= 0) {
+      HIF_CK(cudaEventRecord(tp.b, stream));
+      t_tuner->pending.push_back(tp);
+    }
   }
 
   void gather(std::vector<GatherTarget>& tg, const Sources& src, const int* d_src_owner,
@@ -1918,7 +1951,7 @@ class Engine {
       d.r = bi.r();
       sd.push_back(d);
     }
-    run_sweep(sd, tmp);
+    run_sweep(sd, tmp, st);
     if (verbose && verbose_mode != 2) sync();
     t_elim += wall() - te0;
     mark("schur eliminate", level);
@@ -2495,6 +2528,7 @@ class Engine {
   // mixed precision: faces wider than this (and taller than wide) take the
   // Gram-matrix ID; narrower ones the one-CTA pivoted QR (HIF_OPT_GRAM_MIN_N)
   int gram_min_n = 64;
+  int gram_slices = 0;  // HIF_OPT_GRAM_SLICES
   void id_cholesky(const std::vector<IdDesc>& v, BufList& tmp) {
     Arena& work = *cur_work;
     const int nd = (int)v.size();
@@ -2541,7 +2575,11 @@ class Engine {
       gram.push_back(g);
     }
     auto tm = [&](int cls, double fl, double by, auto&& f, int n) { timed(cls, fl, by, f, n); };
-    gemm_batch(gram, tmp, stream, HIF_KCLASS_QR, tm, 128);
+    // G in FP64 on DMMA, or (HIF_OPT_GRAM_SLICES) from int8 slices: with 8
+    // slices the product's error, about k 2^-56 max|M|^2, is below an FP64
+    // product's k u |M|^2 bound, so the pivots and rank see FP64 accuracy
+    if (gram_slices > 0) gemm_batch_int8(gram, tmp, stream, tm, gram_slices, d_status);
+    else gemm_batch(gram, tmp, stream, HIF_KCLASS_QR, tm, 128);
     PcholDesc* dpd = tmp.add(upload(pd, stream));
     // a fixed sequence of panels without host synchronisation: a face whose
     // rank is known skips its later panels and updates on the device
@@ -2919,7 +2957,7 @@ class Engine {
       d.r = b.r();
       sd.push_back(d);
     }
-    run_sweep(sd, tmp);
+    run_sweep(sd, tmp, st);
     if (verbose && verbose_mode != 2) sync();
     t_elim += wall() - te0;
   }
@@ -3081,10 +3119,10 @@ class Engine {
       l.layout = kGemvSmall;
       l.units = (int)dd.size();
     } else {
-      l.layout = trans ? kGemvCols : kGemvRows;
+      l.layout = kGemvTiles;
       std::vector<int2> tab;
       for (size_t q = 0; q < dd.size(); ++q) {
-        const int nt = trans ? (dd[q].n + 31) / 32 : (dd[q].m + 63) / 64;
+        const int nt = gemv_tile_count(dd[q].m, dd[q].n, trans);
         for (int t = 0; t < nt; ++t) tab.push_back(make_int2((int)q, t));
       }
       l.units = (int)tab.size();
@@ -3979,6 +4017,10 @@ int hif_set_option(hif_handle h, int option, long long value) {
       if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
       h->e->y_slices = (int)value;
       return HIF_OK;
+    case HIF_OPT_GRAM_SLICES:
+      if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
+      h->e->gram_slices = (int)value;
+      return HIF_OK;
     case HIF_OPT_GRAM_MIN_N:
       if (value < 0) return HIF_ERR_ARG;
       h->e->gram_min_n = (int)value;
@@ -4315,6 +4357,24 @@ int hif_trim_device_pool(void) {
   });
 }
 
+int hif_autotune_elimination(hif_handle h, int* signatures, int* decided, int* chose_cholesky) {
+  if (!h) return HIF_ERR_ARG;
+  return guarded([&] {
+    h->e->sync();
+    h->e->tuner.resolve();
+    int n = 0, d = 0, c = 0;
+    for (const auto& kv : h->e->tuner.recs) {
+      if (!(kv.first & hif::Engine::kTuneElimKey)) continue;
+      ++n;
+      if (kv.second.choice >= 0) ++d;
+      if (kv.second.choice == 1) ++c;
+    }
+    if (signatures) *signatures = n;
+    if (decided) *decided = d;
+    if (chose_cholesky) *chose_cholesky = c;
+  });
+}
+
 int hif_memory(hif_handle h, long long* factor_bytes, long long* workspace_bytes) {
   if (!h) return HIF_ERR_ARG;
   // the factor and the descriptors its apply plans read
@@ -4346,6 +4406,7 @@ int hif_autotune_stats(hif_handle h, int* signatures, int* decided, int* chose_1
     h->e->tuner.resolve();
     int n = 0, d = 0, c = 0;
     for (const auto& kv : h->e->tuner.recs) {
+      if (kv.first & hif::Engine::kTuneElimKey) continue;
       ++n;
       if (kv.second.choice >= 0) ++d;
       if (kv.second.choice == 1) ++c;

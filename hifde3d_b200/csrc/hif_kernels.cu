@@ -39,6 +39,21 @@ std::map<std::pair<int, const void*>, size_t> g_attr_smem;
 
 // Raises `fn`'s dynamic shared-memory limit on the current device to at least
 // `bytes` (never lowers it).
+// Multiprocessor count of the current device (cached per device).
+int sm_count() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  static std::map<int, int> sms;
+  auto it = sms.find(dev);
+  if (it != sms.end()) return it->second;
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  if (n <= 0) n = 1;
+  sms[dev] = n;
+  return n;
+}
+
 void ensure_smem(const void* fn, size_t bytes) {
   int dev = 0;
   cudaGetDevice(&dev);
@@ -891,47 +906,95 @@ void launch_gemm_tc(const TcGemm* d_desc, const int* d_tile_off, int nd, int tot
 // ===========================================================================
 // Tile (128 rows x 64 k) of an operand into shared memory, read along the
 // operand's contiguous dimension: for trans = 0 lanes run over rows, for
-// trans = 1 over k, so that both layouts are read in whole cache lines.
-// T[i * kOzTs + k]; entries past the operand are zero.
+// trans = 1 over k, so that both layouts are read in whole cache lines. Each
+// thread issues its 32 loads before the first store, so that they are in
+// flight together. T[i * kOzTs + k]; entries past the operand are zero.
 constexpr int kOzTs = kOzK + 1;
 constexpr size_t kOzConvSmem = (size_t)128 * kOzTs * sizeof(double);
+static_assert(128 * kOzK == 256 * 32, "tile loader: 256 threads x 32 elements");
 __device__ __forceinline__ void oz_load_tile(const OzOperand& o, int rt, int kt, double* T) {
   const int r0 = rt * 128, k0 = kt * kOzK;
+  double v[32];
   if (o.trans == 0) {
-    for (int e = threadIdx.x; e < 128 * kOzK; e += blockDim.x) {
-      const int i = e & 127, k = e >> 7;
-      const int gi = r0 + i, gk = k0 + k;
-      T[i * kOzTs + k] = (gi < o.rows && gk < o.kdim) ? o.X[gi + (long long)gk * o.ld] : 0.0;
+    // thread: row i = tid & 127, k = (tid >> 7) + 2 j
+    const int i = threadIdx.x & 127, kb = threadIdx.x >> 7;
+    const int gi = r0 + i;
+    const double* src = o.X + gi;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int gk = k0 + kb + 2 * j;
+      v[j] = (gi < o.rows && gk < o.kdim) ? __ldg(src + (long long)gk * o.ld) : 0.0;
     }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) T[i * kOzTs + kb + 2 * j] = v[j];
   } else {
-    for (int e = threadIdx.x; e < 128 * kOzK; e += blockDim.x) {
-      const int k = e & (kOzK - 1), i = e / kOzK;
-      const int gi = r0 + i, gk = k0 + k;
-      T[i * kOzTs + k] = (gi < o.rows && gk < o.kdim) ? o.X[gk + (long long)gi * o.ld] : 0.0;
+    // thread: k = tid & 63, row i = (tid >> 6) + 4 j
+    const int k = threadIdx.x & (kOzK - 1), ib = threadIdx.x >> 6;
+    const int gk = k0 + k;
+    const double* src = o.X + gk;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int gi = r0 + ib + 4 * j;
+      v[j] = (gi < o.rows && gk < o.kdim) ? __ldg(src + (long long)gi * o.ld) : 0.0;
     }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) T[(ib + 4 * j) * kOzTs + k] = v[j];
   }
 }
 
+// Row exponents, read in place along the operand's contiguous dimension:
+// trans = 0, two threads per row (lanes over consecutive rows), 32 k each;
+// trans = 1, a warp per row (lanes over consecutive k), 16 rows per warp. The
+// 32 loads of a thread are issued before the first maximum.
 __global__ void __launch_bounds__(256) k_oz_exp(const OzOperand* __restrict__ ops,
                                                 const int* __restrict__ tile_off, int nops) {
-  extern __shared__ double oz_t[];
   const int oi = find_desc(tile_off, nops, blockIdx.x);
   const OzOperand o = ops[oi];
   const int local = blockIdx.x - tile_off[oi];
   const int kt_n = (o.kdim + kOzK - 1) / kOzK;
   const int rt = local / kt_n, kt = local % kt_n;
-  oz_load_tile(o, rt, kt, oz_t);
-  __syncthreads();
-  // two threads per row, 32 k each
-  const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
-  const int gi = rt * 128 + row;
-  double m = 0.0;
-#pragma unroll 8
-  for (int e = 0; e < 32; ++e) m = fmax(m, fabs(oz_t[row * kOzTs + 32 * half + e]));
-  if (gi < o.rows && m > 0.0) {
-    int ex;
-    frexp(m, &ex);  // m < 2^ex
-    atomicMax(&o.rexp[gi], ex);
+  const int k0 = kt * kOzK;
+  double v[32];
+  if (o.trans == 0) {
+    const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
+    const int gi = rt * 128 + row;
+    if (gi >= o.rows) return;
+    const double* src = o.X + gi;
+#pragma unroll
+    for (int e = 0; e < 32; ++e) {
+      const int gk = k0 + 32 * half + e;
+      v[e] = gk < o.kdim ? __ldg(src + (long long)gk * o.ld) : 0.0;
+    }
+    double m = 0.0;
+#pragma unroll
+    for (int e = 0; e < 32; ++e) m = fmax(m, fabs(v[e]));
+    if (m > 0.0) {
+      int ex;
+      frexp(m, &ex);  // m < 2^ex
+      atomicMax(&o.rexp[gi], ex);
+    }
+  } else {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gk0 = k0 + lane, gk1 = k0 + 32 + lane;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int gi = rt * 128 + warp + 8 * j;
+      const double* src = o.X + (long long)gi * o.ld;
+      v[2 * j] = (gi < o.rows && gk0 < o.kdim) ? __ldg(src + gk0) : 0.0;
+      v[2 * j + 1] = (gi < o.rows && gk1 < o.kdim) ? __ldg(src + gk1) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int gi = rt * 128 + warp + 8 * j;
+      double m = fmax(fabs(v[2 * j]), fabs(v[2 * j + 1]));
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+      if (lane == 0 && gi < o.rows && m > 0.0) {
+        int ex;
+        frexp(m, &ex);
+        atomicMax(&o.rexp[gi], ex);
+      }
+    }
   }
 }
 
@@ -988,9 +1051,8 @@ void launch_oz_convert(const OzOperand* d_ops, const int* d_tile_off, int nops, 
   if (total_tiles <= 0) return;
   // 0x80808080: below every exponent a double can have
   cudaMemsetAsync(d_rexp, 0x80, (size_t)n_rexp * sizeof(int), s);
-  ensure_smem((const void*)k_oz_exp, kOzConvSmem);
   ensure_smem((const void*)k_oz_slice, kOzConvSmem);
-  k_oz_exp<<<total_tiles, 256, kOzConvSmem, s>>>(d_ops, d_tile_off, nops);
+  k_oz_exp<<<total_tiles, 256, 0, s>>>(d_ops, d_tile_off, nops);
   k_oz_slice<<<total_tiles, 256, kOzConvSmem, s>>>(d_ops, d_tile_off, nops, slices);
 }
 
@@ -1027,32 +1089,75 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, int byte
       : "memory");
 }
 
+// One int8 slice product; U selects the A collector buffer's use: 0 read A
+// from shared memory only, 1 read it and keep it (fill), 2 reuse the kept A,
+// 3 reuse it for the last time.
+template <int U>
+__device__ __forceinline__ void oz_mma(unsigned d, unsigned long long da, unsigned long long db,
+                                       unsigned idesc, unsigned acc) {
+  if (U == 0)
+    asm volatile(
+        "{\n\t.reg .pred r;\n\tsetp.ne.b32 r, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, r;\n\t}\n" ::"r"(d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+  else if (U == 1)
+    asm volatile(
+        "{\n\t.reg .pred r;\n\tsetp.ne.b32 r, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::fill [%0], %1, %2, %3, r;\n\t}\n" ::"r"(
+            d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+  else if (U == 2)
+    asm volatile(
+        "{\n\t.reg .pred r;\n\tsetp.ne.b32 r, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::use [%0], %1, %2, %3, r;\n\t}\n" ::"r"(d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred r;\n\tsetp.ne.b32 r, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::lastuse [%0], %1, %2, %3, r;\n\t}\n" ::"r"(
+            d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+// Persistent: one CTA per SM walks the launch's tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ...; the tensor memory is allocated and the barriers
+// set up once. The stage ring runs on across tiles. The accumulators of a tile
+// are released (tempty) as soon as the epilogue warps have read them, so its
+// C writes overlap the next tile's products.
 template <int S, int BN>
 __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ descs,
                                                     const int* __restrict__ tile_off, int nd,
-                                                    int* __restrict__ status) {
+                                                    int total_tiles, int* __restrict__ status) {
   using Cfg = OzCfg<S, BN>;
   constexpr int NS = Cfg::kStages;
   extern __shared__ __align__(1024) unsigned char oz_smem[];
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(oz_smem + NS * Cfg::kStage);
   unsigned long long* full = bars;        // [NS]
   unsigned long long* empty = bars + NS;  // [NS]
-  unsigned long long* done = bars + 2 * NS;
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(done + 1);
+  unsigned long long* tfull = bars + 2 * NS;
+  unsigned long long* tempty = tfull + 1;
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(tempty + 1);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  const int di = find_desc(tile_off, nd, blockIdx.x);
-  const OzGemm g = descs[di];
-  const int local = blockIdx.x - tile_off[di];
-  const int tiles_m = (g.m + 127) / 128;
-  const int mt = local % tiles_m, nt = local / tiles_m;
-  const int m0 = mt * 128, n0 = nt * BN;
-  if (g.lower && n0 >= m0 + 128) return;  // whole CTA, before any barrier or allocation
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // k tiles of this CTA: all of the launch's, or with a lower-triangular A none
-  // past the tile's last row
-  const int kt_cnt = g.a_lower
-                         ? min(g.kt_cnt, max(0, (m0 + 128 + kOzK - 1) / kOzK - g.kt0))
-                         : g.kt_cnt;
+
+  // tile decode shared by the roles
+  auto tile = [&](int t, OzGemm& g, int& mt, int& nt, int& kt_cnt) -> bool {
+    const int di = find_desc(tile_off, nd, t);
+    g = descs[di];
+    const int local = t - tile_off[di];
+    const int tiles_m = (g.m + 127) / 128;
+    mt = local % tiles_m;
+    nt = local / tiles_m;
+    const int m0 = mt * 128, n0 = nt * BN;
+    if (g.lower && n0 >= m0 + 128) return false;
+    // with a lower-triangular A no k tile past the tile's last row
+    kt_cnt = g.a_lower ? min(g.kt_cnt, max(0, (m0 + 128 + kOzK - 1) / kOzK - g.kt0)) : g.kt_cnt;
+    return true;
+  };
 
   if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -1066,7 +1171,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[q])) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[q])) : "memory");
     }
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(done)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(tfull)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(tempty)) : "memory");
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -1076,99 +1182,148 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
   const unsigned tmem = *tmem_slot;
 
   if (warp == 0 && lane == 0) {
-    // producer: the S slices of the A tile, then those of the B tile
-    const int bt = n0 / 128, bhalf = (n0 / 64) & 1;
-    for (int i = 0; i < kt_cnt; ++i) {
-      const int kt = g.kt0 + i, s = i % NS;
-      if (i >= NS && !mbar_wait(smem_u32(&empty[s]), (unsigned)((i / NS - 1) & 1), abort)) break;
-      const unsigned fb = smem_u32(&full[s]);
-      const unsigned dst = smem_u32(oz_smem + s * Cfg::kStage);
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
-                   "r"(Cfg::kStage)
-                   : "memory");
-      bulk_g2s(dst, g.A + ((size_t)mt * g.kt_total + kt) * S * kOzPart, Cfg::kA, fb);
-      const signed char* b = g.B + ((size_t)bt * g.kt_total + kt) * S * kOzPart;
-      if (BN == 128) {
-        bulk_g2s(dst + Cfg::kA, b, Cfg::kB, fb);
-      } else {
+    // producer: per k tile, the S slices of the A tile, then those of the B tile
+    int it = 0;
+    for (int t = blockIdx.x; t < total_tiles && !*abort; t += gridDim.x) {
+      OzGemm g;
+      int mt, nt, kt_cnt;
+      if (!tile(t, g, mt, nt, kt_cnt)) continue;
+      const int n0 = nt * BN, bt = n0 / 128, bhalf = (n0 / 64) & 1;
+      bool ok = true;
+      for (int i = 0; i < kt_cnt; ++i, ++it) {
+        const int kt = g.kt0 + i, s = it % NS;
+        if (it >= NS && !mbar_wait(smem_u32(&empty[s]), (unsigned)((it / NS - 1) & 1), abort)) {
+          ok = false;
+          break;
+        }
+        const unsigned fb = smem_u32(&full[s]);
+        const unsigned dst = smem_u32(oz_smem + s * Cfg::kStage);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                     "r"(Cfg::kStage)
+                     : "memory");
+        bulk_g2s(dst, g.A + ((size_t)mt * g.kt_total + kt) * S * kOzPart, Cfg::kA, fb);
+        const signed char* b = g.B + ((size_t)bt * g.kt_total + kt) * S * kOzPart;
+        if (BN == 128) {
+          bulk_g2s(dst + Cfg::kA, b, Cfg::kB, fb);
+        } else {
 #pragma unroll
-        for (int q = 0; q < S; ++q)
-          bulk_g2s(dst + Cfg::kA + q * BN * kOzK, b + (size_t)q * kOzPart + bhalf * BN * kOzK,
-                   BN * kOzK, fb);
+          for (int q = 0; q < S; ++q)
+            bulk_g2s(dst + Cfg::kA + q * BN * kOzK, b + (size_t)q * kOzPart + bhalf * BN * kOzK,
+                     BN * kOzK, fb);
+        }
       }
+      if (!ok) break;
     }
   } else if (warp == 1 && lane == 0) {
     // tensor-core issue: slice pair (p, q) adds into the accumulator of diagonal p + q
-    for (int i = 0; i < kt_cnt; ++i) {
-      const int s = i % NS;
-      if (!mbar_wait(smem_u32(&full[s]), (unsigned)((i / NS) & 1), abort)) break;
+    int it = 0, a = 0;
+    for (int t = blockIdx.x; t < total_tiles && !*abort; t += gridDim.x) {
+      OzGemm g;
+      int mt, nt, kt_cnt;
+      if (!tile(t, g, mt, nt, kt_cnt) || kt_cnt == 0) continue;
+      // the previous tile's accumulators have been read
+      if (a > 0 && !mbar_wait(smem_u32(tempty), (unsigned)((a - 1) & 1), abort)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const unsigned base = smem_u32(oz_smem + s * Cfg::kStage);
+      bool ok = true;
+      for (int i = 0; i < kt_cnt; ++i, ++it) {
+        const int s = it % NS;
+        if (!mbar_wait(smem_u32(&full[s]), (unsigned)((it / NS) & 1), abort)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned base = smem_u32(oz_smem + s * Cfg::kStage);
 #pragma unroll
-      for (int j = 0; j < kOzK / 32; ++j) {
+        for (int j = 0; j < kOzK / 32; ++j) {
 #pragma unroll
-        for (int p = 0; p < S; ++p) {
-          const unsigned long long da = oz_desc(base + p * kOzPart + 256 * j);
+          for (int p = 0; p < S; ++p) {
+            const unsigned long long da = oz_desc(base + p * kOzPart + 256 * j);
 #pragma unroll
-          for (int q = 0; p + q < S; ++q) {
-            const unsigned long long db = oz_desc(base + Cfg::kA + q * BN * kOzK + 256 * j);
-            const unsigned acc = (i > 0 || j > 0 || p > 0) ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred r;\n\t"
-                "setp.ne.b32 r, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, r;\n\t}\n" ::"r"(
-                    tmem + (unsigned)((p + q) * BN)),
-                "l"(da), "l"(db), "r"(Cfg::kIdesc), "r"(acc)
-                : "memory");
+            for (int q = 0; p + q < S; ++q) {
+              const unsigned long long db = oz_desc(base + Cfg::kA + q * BN * kOzK + 256 * j);
+              const unsigned acc = (i > 0 || j > 0 || p > 0) ? 1u : 0u;
+              const unsigned d = tmem + (unsigned)((p + q) * BN);
+              // A slice p is read from shared memory once per 32-k step and kept
+              // in the collector buffer for its other slice pairs
+              if (p == S - 1)
+                oz_mma<0>(d, da, db, Cfg::kIdesc, acc);
+              else if (q == 0)
+                oz_mma<1>(d, da, db, Cfg::kIdesc, acc);
+              else if (p + q < S - 1)
+                oz_mma<2>(d, da, db, Cfg::kIdesc, acc);
+              else
+                oz_mma<3>(d, da, db, Cfg::kIdesc, acc);
+            }
           }
         }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(&empty[s]))
+            : "memory");
       }
+      if (!ok) break;
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(&empty[s]))
+              smem_u32(tfull))
           : "memory");
+      ++a;
     }
-    if (kt_cnt > 0)
-      asm volatile(
-          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(done))
-          : "memory");
   } else if (warp >= 4) {
-    // epilogue: C = alpha 2^{e_i + f_j - 14} sum_d 2^{-7d} P_d + beta C
+    // epilogue: C = alpha 2^{e_i + f_j - 14} sum_d 2^{-7d} P_d + beta C, the
+    // diagonals combined 64 columns at a time in registers
     const int q4 = warp - 4;
-    const int gm = m0 + 32 * q4 + lane;
     const unsigned lanes = (unsigned)(32 * q4) << 16;
-    // k = 0: no products, nothing to wait for (C = beta C)
-    const bool ok = kt_cnt == 0 || (mbar_wait(smem_u32(done), 0u, abort) && !*abort);
-    if (ok) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    int a = 0;
+    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+      OzGemm g;
+      int mt, nt, kt_cnt;
+      if (!tile(t, g, mt, nt, kt_cnt)) continue;
+      const int gm = mt * 128 + 32 * q4 + lane, n0 = nt * BN;
+      bool ok = true;
+      if (kt_cnt > 0) {
+        ok = mbar_wait(smem_u32(tfull), (unsigned)(a & 1), abort) && !*abort;
+        if (ok) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      }
+      if (!ok) break;
       const int ea = gm < g.m ? max(g.ea[gm], -4096) : 0;
-#pragma unroll 1
-      for (int cc = 0; cc < BN / 16; ++cc) {
-        double h[16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) h[e] = 0.0;
+      for (int half = 0; half < BN / 64; ++half) {
+        double h[64];
+#pragma unroll
+        for (int e = 0; e < 64; ++e) h[e] = 0.0;
         if (kt_cnt > 0) {
-#pragma unroll 1
-          for (int d = S - 1; d >= 0; --d) {
-            unsigned v[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
-                "%12,%13,%14,%15}, [%16];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(tmem + lanes + (unsigned)(d * BN + 16 * cc))
-                : "memory");
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int e = 0; e < 16; ++e) h[e] = fma(h[e], 0.0078125, (double)(int)v[e]);
+          for (int cc = 0; cc < 4; ++cc) {
+#pragma unroll
+            for (int d = S - 1; d >= 0; --d) {
+              unsigned v[16];
+              asm volatile(
+                  "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,"
+                  "%11,%12,%13,%14,%15}, [%16];"
+                  : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                    "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                    "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                  : "r"(tmem + lanes + (unsigned)(d * BN + 64 * half + 16 * cc))
+                  : "memory");
+              asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+              for (int e = 0; e < 16; ++e)
+                h[16 * cc + e] = fma(h[16 * cc + e], 0.0078125, (double)(int)v[e]);
+            }
+          }
+          if (half == BN / 64 - 1) {
+            // every accumulator of the tile is read: release them to the next tile
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+              asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(tempty))
+                           : "memory");
           }
         }
         if (gm < g.m) {
 #pragma unroll
-          for (int e = 0; e < 16; ++e) {
-            const int gn = n0 + 16 * cc + e;
+          for (int e = 0; e < 64; ++e) {
+            const int gn = n0 + 64 * half + e;
             if (gn < g.n) {
               double* cp = g.C + gm + (long long)gn * g.ldc;
               const double val = g.alpha * ldexp(h[e], ea + max(g.eb[gn], -4096) - 14);
@@ -1177,6 +1332,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
           }
         }
       }
+      if (kt_cnt > 0) ++a;
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1196,7 +1352,9 @@ template <int S, int BN>
 static void launch_gemm_oz_t(const OzGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
                              int* d_status, cudaStream_t s) {
   ensure_smem((const void*)k_gemm_oz<S, BN>, OzCfg<S, BN>::kSmem);
-  k_gemm_oz<S, BN><<<total_tiles, 256, OzCfg<S, BN>::kSmem, s>>>(d_desc, d_tile_off, nd, d_status);
+  const int grid = std::min(total_tiles, sm_count());
+  k_gemm_oz<S, BN><<<grid, 256, OzCfg<S, BN>::kSmem, s>>>(d_desc, d_tile_off, nd, total_tiles,
+                                                           d_status);
 }
 
 void launch_gemm_oz(const OzGemm* d_desc, const int* d_tile_off, int nd, int total_tiles,
@@ -1537,11 +1695,15 @@ __global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__
   double* Xd = S + T * T;              // 4 diagonal inverses, [p][c][i] = X_pp(i, c)
   double* Tb = Xd + 4 * kCdP * kCdXs;  // 32 x 32 product scratch, [c][i]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // the lower triangle only (the only one read), in whole columns
   for (int e = tid; e < T * T; e += blockDim.x) {
     const int i = e % T, j = e / T;
-    double v;
-    if (i < nb && j < nb) v = d.B[(k0 + max(i, j)) + (long long)(k0 + min(i, j)) * d.n];
-    else v = (i == j) ? 1.0 : 0.0;
+    double v = 0.0;
+    if (i < nb && j < nb) {
+      if (i >= j) v = d.B[(k0 + i) + (long long)(k0 + j) * d.n];
+    } else if (i == j) {
+      v = 1.0;
+    }
     S[e] = v;
   }
   __syncthreads();
@@ -3084,7 +3246,7 @@ __device__ __forceinline__ GemvCtx gemv_ctx(const GemvDesc& g, const double* u_i
 // lane = row, columns in order. y = M^T x: lanes over rows, one warp sum per
 // column (fixed shuffle order). Entries above the diagonal of a triangular M
 // are not read.
-__global__ void __launch_bounds__(256) k_gemv_small(const GemvFastSeg* __restrict__ segs,
+__global__ void __launch_bounds__(256, 3) k_gemv_small(const GemvFastSeg* __restrict__ segs,
                                                     const int* __restrict__ seg_off, int nseg,
                                                     const double* __restrict__ u_in,
                                                     double* __restrict__ u_out, int nrhs_k,
@@ -3141,75 +3303,11 @@ __global__ void __launch_bounds__(256) k_gemv_small(const GemvFastSeg* __restric
   }
 }
 
-// Larger blocks, y = M x: a CTA takes 64 rows (two per lane) of one
-// descriptor; its eight warps split the columns into contiguous ranges and
-// their partial sums are added in warp order through shared memory, so the
-// result does not depend on scheduling. Unit = (descriptor, row strip).
-__global__ void __launch_bounds__(256) k_gemv_rows(const GemvFastSeg* __restrict__ segs,
-                                                   const int* __restrict__ seg_off, int nseg,
-                                                   const double* __restrict__ u_in,
-                                                   double* __restrict__ u_out, int nrhs_k,
-                                                   long long ldu_k, long long cld_k) {
-  const int si = find_desc(seg_off, nseg, blockIdx.x);
-  const int2 t = segs[si].tab[blockIdx.x - seg_off[si]];
-  const GemvDesc g = segs[si].desc[t.x];
-  const GemvCtx x = gemv_ctx(g, u_in, u_out, nrhs_k, ldu_k, cld_k);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i0 = t.y * 64;
-  __shared__ double red[8][64][kRhsGroup];
-  // columns this strip needs (lower triangular: none right of its last row)
-  const int ncol = g.tri ? min(g.n, i0 + 64) : g.n;
-  const int per = (ncol + 7) / 8;
-  const int j0 = warp * per, j1 = min(ncol, j0 + per);
-  const int ia = i0 + lane, ib = i0 + 32 + lane;
-  const bool va = ia < g.m, vb = ib < g.m;
-  for (int c0 = 0; c0 < x.nrhs; c0 += kRhsGroup) {
-    const int nc = min(kRhsGroup, x.nrhs - c0);
-    double acc[2][kRhsGroup];
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-      for (int cc = 0; cc < kRhsGroup; ++cc) acc[h][cc] = 0.0;
-#pragma unroll 4
-    for (int j = j0; j < j1; ++j) {
-      const long long xo = g.in_idx[j] + (long long)c0 * x.ldu;
-      double xv[kRhsGroup];
-#pragma unroll
-      for (int cc = 0; cc < kRhsGroup; ++cc)
-        xv[cc] = cc < nc ? x.uin[xo + (long long)cc * x.ldu] : 0.0;
-      const long long jo = (long long)j * g.ld;
-      const double ma = va ? g.M[ia + jo] : 0.0;
-      const double mb = vb ? g.M[ib + jo] : 0.0;
-#pragma unroll
-      for (int cc = 0; cc < kRhsGroup; ++cc) {
-        acc[0][cc] = fma(ma, xv[cc], acc[0][cc]);
-        acc[1][cc] = fma(mb, xv[cc], acc[1][cc]);
-      }
-    }
-#pragma unroll
-    for (int cc = 0; cc < kRhsGroup; ++cc) {
-      red[warp][lane][cc] = acc[0][cc];
-      red[warp][32 + lane][cc] = acc[1][cc];
-    }
-    __syncthreads();
-    if (threadIdx.x < 64) {
-      const int i = i0 + threadIdx.x;
-      if (i < g.m) {
-        for (int cc = 0; cc < nc; ++cc) {
-          double y = 0.0;
-#pragma unroll
-          for (int w = 0; w < 8; ++w) y += red[w][threadIdx.x][cc];
-          gemv_emit(g, i, c0 + cc, y, x.uout, x.ldu, x.cld);
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Larger blocks, y = M^T x: gemv_tile's 32-column tiles, located from the unit
-// table (descriptor, tile) rather than a search over tile offsets.
-__global__ void __launch_bounds__(256) k_gemv_cols(const GemvFastSeg* __restrict__ segs,
+// Larger blocks: gemv_tile's tiles (y = M x: 256-row strips; y = M^T x:
+// 32-column tiles), located from the unit table (descriptor, tile) rather than
+// a search over tile offsets. Three CTAs per SM (the register cap keeps the
+// occupancy of this memory-bound kernel).
+__global__ void __launch_bounds__(256, 3) k_gemv_tiles(const GemvFastSeg* __restrict__ segs,
                                                    const int* __restrict__ seg_off, int nseg,
                                                    const double* __restrict__ u_in,
                                                    double* __restrict__ u_out, int nrhs,
@@ -3219,6 +3317,11 @@ __global__ void __launch_bounds__(256) k_gemv_cols(const GemvFastSeg* __restrict
   gemv_tile(segs[si].desc[t.x], t.y, u_in, u_out, nrhs, ldu, contrib_ld);
 }
 
+int gemv_tile_count(int m, int n, int trans) {
+  if (m <= 0 || n <= 0) return 0;
+  return trans == 0 ? (m + 255) / 256 : (n + 31) / 32;
+}
+
 void launch_gemv_fast(const GemvFastSeg* d_segs, const int* d_seg_off, int nseg, int units,
                       int layout, const double* u_in, double* u_out, int nrhs, long long ldu,
                       long long contrib_ld, cudaStream_t s) {
@@ -3226,12 +3329,9 @@ void launch_gemv_fast(const GemvFastSeg* d_segs, const int* d_seg_off, int nseg,
   if (layout == kGemvSmall)
     k_gemv_small<<<(units + 7) / 8, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
                                                  contrib_ld);
-  else if (layout == kGemvRows)
-    k_gemv_rows<<<units, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
-                                      contrib_ld);
   else
-    k_gemv_cols<<<units, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
-                                      contrib_ld);
+    k_gemv_tiles<<<units, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
+                                       contrib_ld);
 }
 
 

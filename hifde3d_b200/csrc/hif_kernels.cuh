@@ -281,7 +281,7 @@ struct OzOperand {
   int trans;  // 0: element (i, kk) at X[i + kk ld]; 1: at X[kk + i ld]
   int rows, kdim;
   signed char* out;
-  int* rexp;  // per-row exponent, ceil(rows / 128) * 128 entries
+  int* rexp;  // per-row exponent, rows entries
 };
 // d_tile_off: prefix over operands of ceil(rows / 128) * ceil(kdim / 64).
 // Every rexp lies in [d_rexp, d_rexp + n_rexp): it is cleared, then the
@@ -414,11 +414,13 @@ int copy_tiles(int m, int n);
 // contrib_ld: stride between right-hand sides in the contribution buffer.
 // The apply's GEMV launches (the engine's plans and the serving loop's batched
 // stages). Layouts: kGemvSmall, one warp per descriptor (both dimensions <=
-// kGemvSmallMax; units = descriptors); kGemvRows, y = M x by 64-row strips;
-// kGemvCols, y = M^T x by 32-column tiles (units = entries (descriptor, strip /
-// tile) of the segment's table). A launch covers segments (one per operator or
-// request) of one layout; seg_off: prefix of the units over the segments.
-constexpr int kGemvSmall = 0, kGemvRows = 1, kGemvCols = 2;
+// kGemvSmallMax; units = descriptors); kGemvTiles, y = M x by 256-row strips or
+// y = M^T x by 32-column tiles (units = entries (descriptor, tile) of the
+// segment's table, gemv_tile_count tiles per descriptor). A launch covers
+// segments (one per operator or request) of one layout; seg_off: prefix of the
+// units over the segments.
+constexpr int kGemvSmall = 0, kGemvTiles = 1, kGemvLayouts = 2;
+int gemv_tile_count(int m, int n, int trans);
 constexpr int kGemvSmallMax = 64;
 struct GemvFastSeg {
   const GemvDesc* desc;

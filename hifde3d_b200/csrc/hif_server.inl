@@ -371,8 +371,8 @@ class Server {
     for (auto& kv : stages) {
       // one launch per GEMV layout present at this stage (the same kernels as
       // hif_apply's, so each request computes exactly what it would alone)
-      std::vector<GemvFastSeg> gs[3];
-      std::vector<int> goff[3] = {{0}, {0}, {0}};
+      std::vector<GemvFastSeg> gs[kGemvLayouts];
+      std::vector<int> goff[kGemvLayouts] = {{0}, {0}};
       std::vector<ReduceSeg> rs;
       std::vector<int> roff(1, 0);
       for (auto& pr : kv.second) {
@@ -385,7 +385,7 @@ class Server {
           roff.push_back(roff.back() + l.tiles);
         }
       }
-      for (int lay = 0; lay < 3; ++lay) {
+      for (int lay = 0; lay < kGemvLayouts; ++lay) {
         if (gs[lay].empty() || goff[lay].back() == 0) continue;
         GemvFastSeg* dg = tick.add(upload(gs[lay], sstream_));
         int* dgo = tick.add(upload(goff[lay], sstream_));

@@ -192,9 +192,11 @@ enum hif_option {
   HIF_OPT_PROFILE = 4,       /* time every launch with CUDA events (resets the counters) */
   HIF_OPT_ID_GROUP_MIN_N = 5, /* faces with at least this many columns get a CTA group (default 512) */
   HIF_OPT_PRECISION = 6,      /* HIF_PRECISION_FP64 (default) or HIF_PRECISION_MIXED */
-  HIF_OPT_AUTOTUNE = 7,       /* 1: tune the tile shape of the batched FP64 products online
-                                 (each batch signature tries both tiles on the first
-                                 factorizations, then keeps the faster); results may then
+  HIF_OPT_AUTOTUNE = 7,       /* 1: tune online: the tile shape of the batched FP64
+                                 products per batch signature, and in mixed precision on
+                                 a symmetric operator (HIF_ELIM_AUTO) the elimination
+                                 method per phase; each candidate runs once on the first
+                                 factorizations, then the faster is kept; results may then
                                  differ in the last bits between those factorizations */
   HIF_OPT_SCHUR_SLICES = 8,   /* MIXED: int8 slices (2..8) of the Schur-complement products
                                  S = A11 - A12 X (default 5); 0: split TF32 */
@@ -203,8 +205,10 @@ enum hif_option {
   HIF_OPT_ELIMINATION = 10,   /* enum hif_elimination (default HIF_ELIM_AUTO) */
   HIF_OPT_Y_SLICES = 11,      /* MIXED, Cholesky elimination: int8 slices (2..8) of
                                  Y = L^{-1} A21 (default 6); 0: FP64 */
-  HIF_OPT_GRAM_MIN_N = 12     /* MIXED: faces with more columns than this (and more rows
+  HIF_OPT_GRAM_MIN_N = 12,    /* MIXED: faces with more columns than this (and more rows
                                  than columns) take the Gram-matrix ID (default 64) */
+  HIF_OPT_GRAM_SLICES = 13    /* MIXED: the Gram matrices M^T M of that ID from int8 slices
+                                 (2..8); 0 (default): FP64 products */
 };
 /* Arithmetic of the factorization. MIXED: the long-K products of the eliminations
  * (S = A11 - A12 X, and X or Y) are FP64 products formed from exact int8 slice
@@ -271,6 +275,10 @@ int hif_kernel_stats(hif_handle h, int kclass, long long* launches, double* ms, 
 /* State of the HIF_OPT_AUTOTUNE tuner: batch signatures seen, signatures with a
  * decision, and how many of those chose the 128 x 128 tensor-core tile. */
 int hif_autotune_stats(hif_handle h, int* signatures, int* decided, int* chose_128);
+/* The tuner's per-phase elimination choices (mixed precision, symmetric operator,
+ * HIF_ELIM_AUTO): phase signatures seen, decided, and how many chose Cholesky over
+ * Gauss-Jordan. No reference counterpart. */
+int hif_autotune_elimination(hif_handle h, int* signatures, int* decided, int* chose_cholesky);
 
 /* Device memory held by the handle: the factor (kept until the next hif_factor or
  * hif_destroy) and the factorization workspace (kept for reuse by later

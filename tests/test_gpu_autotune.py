@@ -55,6 +55,43 @@ def test_autotune_off_by_default():
     f, _ = make(16, 3, False)
     try:
         f.Factor()
-        assert f.autotune_stats() == {"signatures": 0, "decided": 0, "chose_128": 0}
+        st = f.autotune_stats()
+        assert (st["signatures"], st["decided"], st["chose_128"]) == (0, 0, 0)
+        assert st["elimination_phases"] == 0
     finally:
         f.close()
+
+
+def test_autotune_picks_the_elimination_per_phase_in_mixed_precision():
+    """Mixed precision on the symmetric operator: each phase signature runs once
+    with Gauss-Jordan and once with Cholesky, then keeps the faster. Both are
+    the same factorization up to the mixed-precision error, so every tuned
+    factor's inverse apply stays within 1e-5 of the FP64 one and PCG converges
+    as with the untuned mixed factor."""
+    ref, N = make(32, 22, False)
+    tuned, _ = make(32, 22, True)
+    mixed, _ = make(32, 22, False)
+    try:
+        ref.Factor()
+        mixed.set_option(hb.OPT_PRECISION, hb.PRECISION_MIXED)
+        mixed.Factor()
+        tuned.set_option(hb.OPT_PRECISION, hb.PRECISION_MIXED)
+        b = synth.dof_vector(N, 6)
+        y_ref = b.copy()
+        ref.Apply(y_ref, True)
+        _, it_mixed, _ = mixed.solve_pcg(b, tol=1e-10, maxit=60)
+        for rep in range(3):
+            tuned.Factor()
+            st = tuned.autotune_stats()
+            assert st["elimination_phases"] > 0
+            if rep >= 1:
+                assert st["elimination_decided"] == st["elimination_phases"], st
+            y = b.copy()
+            tuned.Apply(y, True)
+            assert np.linalg.norm(y - y_ref) <= 1e-5 * np.linalg.norm(y_ref), rep
+            _, it, rr = tuned.solve_pcg(b, tol=1e-10, maxit=60)
+            assert rr <= 1e-10 and abs(it - it_mixed) <= 1
+    finally:
+        ref.close()
+        tuned.close()
+        mixed.close()
