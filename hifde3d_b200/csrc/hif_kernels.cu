@@ -1668,24 +1668,31 @@ void launch_chol_small(const SweepDesc* d_desc, int nd, int max_n, int* d_status
 
 // Pivot block of the blocked Cholesky: L_KK = chol(D) over B[K, K] (zeros
 // above the diagonal) and L_KK^{-1} into dinv, with D (128 x 128, lower
-// triangle read, padded with the identity past nb) in shared memory. Blocked
-// by 32-wide panels so that a block costs a few dozen barriers, not one per
-// pivot (this kernel is on the critical path of the top levels, where one or
-// a few blocks remain):
-//   for each panel p: warp 0 factors the 32 x 32 diagonal block and inverts
-//   it (warp-synchronous), the CTA solves the rows below against it and
-//   updates the trailing lower triangle;
-//   then L^{-1} in place, block column by block column from the left:
-//   X_jj = L_jj^{-1}, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj (i > j).
+// triangle read, padded with the identity past nb) in shared memory. This
+// kernel is on the critical path of the top levels, where one or a few blocks
+// remain, so it is built for latency:
+//   for each 32-wide panel p: warp 0 factors the 32 x 32 diagonal block with
+//   its rows in registers (pivots and multipliers passed by shuffles) and
+//   inverts it by forward substitution, lane = column; the CTA then solves the
+//   rows below against the inverse and updates the trailing lower triangle,
+//   each thread holding a 16-strided micro-tile of the outputs in registers
+//   (rows tx + 16a, columns ty + 16b), so that a warp's loads are 16
+//   consecutive doubles or broadcasts;
+//   then L^{-1} in place, block row ib by block row: for every block column
+//   jb < ib at once, Tb = L(ib, jb:ib) X(jb:ib, jb), then X(ib, jb) = -X_ib Tb.
+// Every sum runs over k in the same increasing order as the unblocked
+// elimination; terms added past a triangle's edge are exact zeros.
 constexpr int kCdP = 32;             // panel width
 constexpr int kCdXs = kCdP + 1;      // padded stride of the diagonal inverses
+constexpr int kCdThreads = 256;
 constexpr size_t kCholDiagSmem =
-    (size_t)(kSweepNB * kSweepNB + 4 * kCdP * kCdXs + kCdP * kCdXs) * sizeof(double);
+    (size_t)(kSweepNB * kSweepNB + 4 * kCdP * kCdXs + 3 * kCdP * kCdXs) * sizeof(double);
+static_assert(kSweepNB == 4 * kCdP && kCdThreads == 256, "16 x 16 thread grid over 32-row panels");
 
-__global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__ descs,
-                                                   const int* __restrict__ active, int k0,
-                                                   double* __restrict__ dinv,
-                                                   int* __restrict__ status) {
+__global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __restrict__ descs,
+                                                          const int* __restrict__ active, int k0,
+                                                          double* __restrict__ dinv,
+                                                          int* __restrict__ status) {
   const int di = active[blockIdx.x];
   const SweepDesc d = descs[di];
   const int nb = min(kSweepNB, d.r - k0);
@@ -1693,18 +1700,25 @@ __global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__
   extern __shared__ double cd_sm[];
   double* S = cd_sm;
   double* Xd = S + T * T;              // 4 diagonal inverses, [p][c][i] = X_pp(i, c)
-  double* Tb = Xd + 4 * kCdP * kCdXs;  // 32 x 32 product scratch, [c][i]
+  double* Tb = Xd + 4 * kCdP * kCdXs;  // 3 products of the inverse, [jb][c][k]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // the lower triangle only (the only one read), in whole columns
-  for (int e = tid; e < T * T; e += blockDim.x) {
-    const int i = e % T, j = e / T;
-    double v = 0.0;
-    if (i < nb && j < nb) {
-      if (i >= j) v = d.B[(k0 + i) + (long long)(k0 + j) * d.n];
-    } else if (i == j) {
-      v = 1.0;
+  const int tx = tid & 15, ty = tid >> 4;
+  // the lower triangle only (the only one read), in whole columns; 16 loads
+  // of a thread in flight at once
+  {
+    const double* Bk = d.B + k0 + (long long)k0 * d.n;
+#pragma unroll 1
+    for (int base = 0; base < T * T; base += kCdThreads * 16) {
+      double v[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int e = base + u * kCdThreads + tid, i = e % T, j = e / T;
+        v[u] = (i < nb && j < nb) ? (i >= j ? Bk[i + (long long)j * d.n] : 0.0)
+                                  : (i == j ? 1.0 : 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < 16; ++u) S[base + u * kCdThreads + tid] = v[u];
     }
-    S[e] = v;
   }
   __syncthreads();
   int bad = 0;
@@ -1712,66 +1726,99 @@ __global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__
     const int o = p * kCdP;
     double* X = Xd + p * kCdP * kCdXs;
     if (warp == 0) {
-      // Cholesky of the 32 x 32 diagonal block, lane = row
+      // Cholesky of the 32 x 32 diagonal block: lane = row, a[j] = D(lane, j)
+      double a[kCdP];
+#pragma unroll
+      for (int j = 0; j < kCdP; ++j) a[j] = S[(o + lane) + (o + j) * T];
+#pragma unroll
       for (int k = 0; k < kCdP; ++k) {
-        const double pv = S[(o + k) + (o + k) * T];
+        const double pv = __shfl_sync(0xffffffffu, a[k], k);
         if (lane == 0 && o + k < nb && (!(pv > 1e-300) || !isfinite(pv))) bad = 1;
         const double dk = sqrt(fabs(pv) > 1e-300 ? fabs(pv) : 1.0);
-        __syncwarp();
-        if (lane > k) S[(o + lane) + (o + k) * T] /= dk;
-        if (lane == k) S[(o + k) + (o + k) * T] = dk;
-        __syncwarp();
-        if (lane > k) {
-          const double lik = S[(o + lane) + (o + k) * T];
-          for (int j = k + 1; j <= lane; ++j)
-            S[(o + lane) + (o + j) * T] =
-                fma(-lik, S[(o + j) + (o + k) * T], S[(o + lane) + (o + j) * T]);
+        if (lane > k) a[k] /= dk;
+        if (lane == k) a[k] = dk;
+        // D(lane, j) -= L(lane, k) L(j, k), k < j <= lane
+#pragma unroll
+        for (int j = 1; j < kCdP; ++j) {
+          if (j > k) {  // fixed trip count: a[] stays in registers
+            const double ljk = __shfl_sync(0xffffffffu, a[k], j);
+            if (lane >= j) a[j] = fma(-a[k], ljk, a[j]);
+          }
         }
-        __syncwarp();
       }
+#pragma unroll
+      for (int j = 0; j < kCdP; ++j) S[(o + lane) + (o + j) * T] = a[j];
+      __syncwarp();
       // its inverse, lane = column c: X(c, c) = 1 / l_cc,
-      // X(i, c) = -(sum_{k=c}^{i-1} l_ik X(k, c)) / l_ii
+      // X(i, c) = -(sum_{k=c}^{i-1} l_ik X(k, c)) / l_ii, zero above
       const int c = lane;
-      X[c * kCdXs + c] = 1.0 / S[(o + c) + (o + c) * T];
+      double x[kCdP];
+#pragma unroll
       for (int i = 0; i < kCdP; ++i) {
-        if (i > c) {
-          double acc = 0.0;
-          for (int k = c; k < i; ++k) acc = fma(S[(o + i) + (o + k) * T], X[c * kCdXs + k], acc);
-          X[c * kCdXs + i] = -acc / S[(o + i) + (o + i) * T];
-        } else if (i < c) {
-          X[c * kCdXs + i] = 0.0;
-        }
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < kCdP - 1; ++k)
+          if (k < i) acc = fma(S[(o + i) + (o + k) * T], x[k], acc);
+        const double lii = S[(o + i) + (o + i) * T];
+        x[i] = i == c ? 1.0 / lii : (i > c ? -acc / lii : 0.0);
       }
+#pragma unroll
+      for (int i = 0; i < kCdP; ++i) X[c * kCdXs + i] = x[i];
     }
     __syncthreads();
     const int r0 = o + kCdP, nrow = T - r0;
     if (nrow > 0) {
-      // panel rows below: L_ip = A_ip X_pp^T (computed, then written)
-      double outv[6];
-      int cnt = 0;
-      for (int e = tid; e < nrow * kCdP; e += blockDim.x, ++cnt) {
-        const int i = r0 + e % nrow, c = e / nrow;
-        double acc = 0.0;
-        // (A_ip X^T)(i, c) = sum_{k <= c} A(i, k) X(c, k); X(c, k) at X[k * kCdXs + c]
-        for (int k = 0; k <= c; ++k) acc = fma(S[i + (o + k) * T], X[k * kCdXs + c], acc);
-        outv[cnt] = acc;
+      const int na = nrow / 16;  // 6, 4 or 2 row strides
+      // panel rows below: L(i, c) = sum_k A(i, k) X(c, k), X(c, k) = X[k kCdXs + c]
+      double acc[6][2];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) acc[a][0] = acc[a][1] = 0.0;
+#pragma unroll 4
+      for (int k = 0; k < kCdP; ++k) {
+        const double x0 = X[k * kCdXs + ty], x1 = X[k * kCdXs + ty + 16];
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+          if (a < na) {
+            const double av = S[(r0 + tx + 16 * a) + (o + k) * T];
+            acc[a][0] = fma(av, x0, acc[a][0]);
+            acc[a][1] = fma(av, x1, acc[a][1]);
+          }
       }
       __syncthreads();
-      cnt = 0;
-      for (int e = tid; e < nrow * kCdP; e += blockDim.x, ++cnt) {
-        const int i = r0 + e % nrow, c = e / nrow;
-        S[i + (o + c) * T] = outv[cnt];
-      }
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+        if (a < na) {
+          S[(r0 + tx + 16 * a) + (o + ty) * T] = acc[a][0];
+          S[(r0 + tx + 16 * a) + (o + ty + 16) * T] = acc[a][1];
+        }
       __syncthreads();
-      // trailing lower triangle: A_ij -= L_ip L_jp^T
-      for (int e = tid; e < nrow * nrow; e += blockDim.x) {
-        const int i = r0 + e % nrow, j = r0 + e / nrow;
-        if (i < j) continue;
-        double acc = S[i + j * T];
-#pragma unroll 8
-        for (int k = 0; k < kCdP; ++k) acc = fma(-S[i + (o + k) * T], S[j + (o + k) * T], acc);
-        S[i + j * T] = acc;
+      // trailing lower triangle: A(i, j) -= sum_k L(i, k) L(j, k)
+      double t[6][6];
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int b = 0; b < 6; ++b)
+          t[a][b] = (a < na && b < na) ? S[(r0 + tx + 16 * a) + (r0 + ty + 16 * b) * T] : 0.0;
+#pragma unroll 2
+      for (int k = 0; k < kCdP; ++k) {
+        double li[6], lj[6];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+          li[a] = a < na ? S[(r0 + tx + 16 * a) + (o + k) * T] : 0.0;
+          lj[a] = a < na ? S[(r0 + ty + 16 * a) + (o + k) * T] : 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+          for (int b = 0; b < 6; ++b)
+            if (a < na && b < na) t[a][b] = fma(-li[a], lj[b], t[a][b]);
       }
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int b = 0; b < 6; ++b)
+          if (a < na && b < na && tx + 16 * a >= ty + 16 * b)
+            S[(r0 + tx + 16 * a) + (r0 + ty + 16 * b) * T] = t[a][b];
       __syncthreads();
     }
   }
@@ -1781,35 +1828,55 @@ __global__ void __launch_bounds__(512) k_chol_diag(const SweepDesc* __restrict__
     const int i = e % nb, j = e / nb;
     d.B[(k0 + i) + (long long)(k0 + j) * d.n] = (i >= j) ? S[i + j * T] : 0.0;
   }
+  // L^{-1} in place: the diagonal blocks first (X_jj, zeros above)
+  for (int e = tid; e < 4 * kCdP * kCdP; e += blockDim.x) {
+    const int jb = e / (kCdP * kCdP), r = e % (kCdP * kCdP), i = r % kCdP, c = r / kCdP;
+    S[(jb * kCdP + i) + (jb * kCdP + c) * T] = Xd[jb * kCdP * kCdXs + c * kCdXs + i];
+  }
   __syncthreads();
-  // L^{-1} in place, block columns from the left
-  for (int jb = 0; jb < T / kCdP; ++jb) {
-    const int oj = jb * kCdP;
-    for (int e = tid; e < kCdP * kCdP; e += blockDim.x) {
-      const int i = e % kCdP, c = e / kCdP;
-      S[(oj + i) + (oj + c) * T] = Xd[jb * kCdP * kCdXs + c * kCdXs + i];
+  for (int ib = 1; ib < T / kCdP; ++ib) {
+    const int oi = ib * kCdP;
+    // Tb[jb](i, c) = sum_{k in [jb 32, oi)} L(oi + i, k) X(k, jb 32 + c)
+    for (int jb = 0; jb < ib; ++jb) {
+      const int oj = jb * kCdP;
+      double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll 4
+      for (int k = oj; k < oi; ++k) {
+        const double l0 = S[(oi + tx) + k * T], l1 = S[(oi + tx + 16) + k * T];
+        const double x0 = S[k + (oj + ty) * T], x1 = S[k + (oj + ty + 16) * T];
+        acc[0][0] = fma(l0, x0, acc[0][0]);
+        acc[0][1] = fma(l0, x1, acc[0][1]);
+        acc[1][0] = fma(l1, x0, acc[1][0]);
+        acc[1][1] = fma(l1, x1, acc[1][1]);
+      }
+      double* Tj = Tb + jb * kCdP * kCdXs;
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) Tj[(ty + 16 * b) * kCdXs + tx + 16 * a] = acc[a][b];
     }
     __syncthreads();
-    for (int ib = jb + 1; ib < T / kCdP; ++ib) {
-      const int oi = ib * kCdP;
-      // Tb = sum_{k in [oj, oi)} L(oi.., k) X(k, oj..)
-      for (int e = tid; e < kCdP * kCdP; e += blockDim.x) {
-        const int i = e % kCdP, c = e / kCdP;
-        double acc = 0.0;
-        for (int k = oj; k < oi; ++k) acc = fma(S[(oi + i) + k * T], S[k + (oj + c) * T], acc);
-        Tb[c * kCdXs + i] = acc;
+    // X(ib, jb) = -X_ib Tb[jb]
+    const double* Xi = Xd + ib * kCdP * kCdXs;
+    for (int jb = 0; jb < ib; ++jb) {
+      const int oj = jb * kCdP;
+      const double* Tj = Tb + jb * kCdP * kCdXs;
+      double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll 4
+      for (int k = 0; k < kCdP; ++k) {
+        const double x0 = Xi[k * kCdXs + tx], x1 = Xi[k * kCdXs + tx + 16];
+        const double t0 = Tj[ty * kCdXs + k], t1 = Tj[(ty + 16) * kCdXs + k];
+        acc[0][0] = fma(x0, t0, acc[0][0]);
+        acc[0][1] = fma(x0, t1, acc[0][1]);
+        acc[1][0] = fma(x1, t0, acc[1][0]);
+        acc[1][1] = fma(x1, t1, acc[1][1]);
       }
-      __syncthreads();
-      // X(ib, jb) = -X_ib,ib Tb
-      const double* Xi = Xd + ib * kCdP * kCdXs;
-      for (int e = tid; e < kCdP * kCdP; e += blockDim.x) {
-        const int i = e % kCdP, c = e / kCdP;
-        double acc = 0.0;
-        for (int k = 0; k <= i; ++k) acc = fma(Xi[k * kCdXs + i], Tb[c * kCdXs + k], acc);
-        S[(oi + i) + (oj + c) * T] = -acc;
-      }
-      __syncthreads();
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) S[(oi + tx + 16 * a) + (oj + ty + 16 * b) * T] = -acc[a][b];
     }
+    __syncthreads();
   }
   double* out = dinv + (long long)di * kSweepNB * kSweepNB;
   for (int e = tid; e < nb * nb; e += blockDim.x) {
@@ -1822,7 +1889,7 @@ void launch_chol_diag(const SweepDesc* d_desc, const int* d_active, int nact, in
                       double* d_dinv, int* d_status, cudaStream_t s) {
   if (nact <= 0) return;
   ensure_smem((const void*)k_chol_diag, kCholDiagSmem);
-  k_chol_diag<<<nact, 512, kCholDiagSmem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
+  k_chol_diag<<<nact, kCdThreads, kCholDiagSmem, s>>>(d_desc, d_active, k0, d_dinv, d_status);
 }
 
 // ===========================================================================
