@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -522,9 +523,10 @@ void gemm_batch(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_t str
   std::vector<Split> splits;
   for (size_t q = 0; q < gin.size(); ++q) {
     const GemmDesc& x = gin[q];
-    fl += x.a_lower ? 1.0 * x.m * x.n * (x.k + 1) : 2.0 * x.m * x.n * x.k;
+    fl += (x.a_lower || x.b_lower) ? 1.0 * x.m * x.n * (x.k + 1) : 2.0 * x.m * x.n * x.k;
     const int big = std::max(x.m, x.n);
-    if (force_tile == 0 && !x.lower && !x.a_lower && x.k >= 2048 && x.k >= 8 * big) {
+    if (force_tile == 0 && !x.lower && !x.a_lower && !x.b_lower && x.k >= 2048 &&
+        x.k >= 8 * big) {
       const int S = std::min(32, (x.k + 1023) / 1024);
       splits.push_back(Split{q, S});
       psz += (long long)S * x.m * x.n;
@@ -720,7 +722,9 @@ struct ElimArith {
 //     L_KK = chol(B[K, K]) and L_KK^{-1} (k_chol_diag),
 //     panel  B[K1:r, K] = B[K1:r, K] L_KK^{-T},
 //     update B[K1:r, K1:r] -= panel panel^T (lower tiles),
-//     row block K of L^{-1}: -L_KK^{-1} (L[K, 0:K0] L^{-1}[0:K0, 0:K0]), and L_KK^{-1};
+//     L_KK^{-1} into the diagonal block K of L^{-1};
+//   then the rest of L^{-1} by a halving of the 128-blocks (X21 = -X22 L21 X11,
+//   bottom up, every node of a depth in two batched products),
 //   then Y = L^{-1} A21 and S = A11 - Y^T Y as long-K products (FP64, or from
 //   int8 slices in mixed precision: ar.x slices for Y, ar.schur for S).
 // 2r^3/3 + 2r^2 s + r s^2 flops against the Gauss-Jordan path's
@@ -769,7 +773,6 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
     qsz += (long long)large[b].r * kSweepNB;
   }
   double* Qb = big(qsz);  // per block: old panel (r x 128, ld r)
-  double* Tb = big(qsz);  // per block: L[K, 0:K0] L^{-1}[0:K0, 0:K0] (128 x r, ld 128)
   // L and L^{-1} read as zero above their diagonals
   {
     std::vector<GemmDesc> z;
@@ -789,7 +792,7 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
     std::vector<int> active;
     std::vector<CopyDesc> cq, cdg;
     std::vector<int> ocq(1, 0), ocd(1, 0);
-    std::vector<GemmDesc> gp, gu, gt, gl;
+    std::vector<GemmDesc> gp, gu;
     for (int b = 0; b < nl; ++b) {
       const SweepDesc& d = large[b];
       if (d.r <= k0) continue;
@@ -797,7 +800,6 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
       const int r = d.r, k1 = std::min(r, k0 + kSweepNB), nbk = k1 - k0;
       const double* Dv = dinv + (long long)b * kSweepNB * kSweepNB;  // nbk x nbk, ld nbk
       double* Q = Qb + oq[b];
-      double* T = Tb + oq[b];
       double* P = d.B + k1 + (long long)k0 * d.n;  // panel rows k1..r of column block K
       if (r > k1) {
         cq.push_back(CopyDesc{P, Q, d.n, r, r - k1, nbk});
@@ -830,38 +832,6 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
         u.lower = 1;
         gu.push_back(u);
       }
-      if (k0 > 0) {
-        // T = L[K, 0:k0] L^{-1}[0:k0, 0:k0] by 128-column blocks J: L^{-1} is
-        // lower triangular, so block J needs only k in [J0, k0) (half the flops);
-        // each block's long reduction is split along k by gemm_batch, which keeps
-        // the GPU busy when there are few blocks (the top levels)
-        for (int j0 = 0; j0 < k0; j0 += kSweepNB) {
-          GemmDesc t{};
-          t.C = T + (long long)j0 * kSweepNB;
-          t.ldc = kSweepNB;
-          t.A = d.B + k0 + (long long)j0 * d.n;  // L[K, j0:k0]
-          t.lda = d.n;
-          t.B = d.a22inv + j0 + (long long)j0 * r;  // L^{-1}[j0:k0, j0:j0+128]
-          t.ldb = r;
-          t.m = nbk;
-          t.n = std::min(kSweepNB, k0 - j0);
-          t.k = k0 - j0;
-          t.alpha = 1.0;
-          gt.push_back(t);
-        }
-        GemmDesc l{};
-        l.C = d.a22inv + k0;
-        l.ldc = r;
-        l.A = Dv;
-        l.lda = nbk;
-        l.B = T;
-        l.ldb = kSweepNB;
-        l.m = nbk;
-        l.n = k0;
-        l.k = nbk;
-        l.alpha = -1.0;
-        gl.push_back(l);
-      }
       cdg.push_back(CopyDesc{Dv, d.a22inv + k0 + (long long)k0 * r, nbk, r, nbk, nbk});
       ocd.push_back(ocd.back() + copy_tiles(nbk, nbk));
     }
@@ -877,8 +847,6 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
     }
     gemm_batch(gp, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
     gemm_batch(gu, step, stream, HIF_KCLASS_GEMM, timed, 128);
-    gemm_batch(gt, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
-    gemm_batch(gl, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
     {
       CopyDesc* dc = step.add(upload(cdg, stream));
       int* doc = step.add(upload(ocd, stream));
@@ -903,6 +871,71 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
     int* doc = tmp.add(upload(ocl, stream));
     timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dc, doc, (int)cl.size(), ocl.back(), stream); });
     HIF_CK(cudaGetLastError());
+  }
+  // L^{-1} off the diagonal blocks (which hold L_KK^{-1}), bottom up over a
+  // halving of each block's 128-blocks: for a node [b0, b1) split at mid,
+  //   X21 = -X22 (L21 X11),
+  // X11 and X22 being the inverses of its halves, done one depth before. The
+  // nodes of one depth, over all blocks, are two batched products.
+  {
+    struct Node {
+      int b, o1, r1, o2, r2;  // block, first row / size of each half
+    };
+    std::vector<std::vector<Node>> depth;
+    std::function<void(int, int, int, int)> split = [&](int b, int b0, int b1, int dep) {
+      if (b1 - b0 < 2) return;
+      const int mid = b0 + (b1 - b0) / 2, r = large[b].r;
+      if ((int)depth.size() <= dep) depth.resize(dep + 1);
+      depth[dep].push_back(Node{b, b0 * kSweepNB, (mid - b0) * kSweepNB, mid * kSweepNB,
+                                std::min(r, b1 * kSweepNB) - mid * kSweepNB});
+      split(b, b0, mid, dep + 1);
+      split(b, mid, b1, dep + 1);
+    };
+    for (int b = 0; b < nl; ++b) split(b, 0, (large[b].r + kSweepNB - 1) / kSweepNB, 0);
+    long long tmax = 0;
+    for (const std::vector<Node>& v : depth) {
+      long long t = 0;
+      for (const Node& q : v) t += (long long)q.r1 * q.r2;
+      tmax = std::max(tmax, t);
+    }
+    double* Tsc = tmax ? big(tmax) : nullptr;
+    for (int dep = (int)depth.size() - 1; dep >= 0; --dep) {
+      std::vector<GemmDesc> g1, g2;
+      long long to = 0;
+      for (const Node& q : depth[dep]) {
+        const SweepDesc& d = large[q.b];
+        double* T = Tsc + to;  // r2 x r1, ld r2
+        to += (long long)q.r1 * q.r2;
+        GemmDesc t{};  // T = L21 X11 (X11 lower triangular)
+        t.C = T;
+        t.ldc = q.r2;
+        t.A = d.B + q.o2 + (long long)q.o1 * d.n;
+        t.lda = d.n;
+        t.B = d.a22inv + q.o1 + (long long)q.o1 * d.r;
+        t.ldb = d.r;
+        t.b_lower = 1;
+        t.m = q.r2;
+        t.n = q.r1;
+        t.k = q.r1;
+        t.alpha = 1.0;
+        g1.push_back(t);
+        GemmDesc x{};  // X21 = -X22 T (X22 lower triangular)
+        x.C = d.a22inv + q.o2 + (long long)q.o1 * d.r;
+        x.ldc = d.r;
+        x.A = d.a22inv + q.o2 + (long long)q.o2 * d.r;
+        x.lda = d.r;
+        x.a_lower = 1;
+        x.B = T;
+        x.ldb = q.r2;
+        x.m = q.r2;
+        x.n = q.r1;
+        x.k = q.r2;
+        x.alpha = -1.0;
+        g2.push_back(x);
+      }
+      gemm_batch(g1, tmp, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+      gemm_batch(g2, tmp, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+    }
   }
   // Y = L^{-1} A21 and S = A11 - Y^T Y
   std::vector<GemmDesc> gy, gs;

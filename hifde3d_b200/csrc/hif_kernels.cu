@@ -306,18 +306,19 @@ __global__ void __launch_bounds__(256) k_dgemm(const GemmDesc* __restrict__ desc
   };
 
   const int kend = g.a_lower ? min(g.k, m0 + kBM) : g.k;
-  const int nk = (kend + kBK - 1) / kBK;
+  const int kbeg = g.b_lower ? min(kend, n0) : 0;  // n0: a multiple of kBK
+  const int nk = (kend - kbeg + kBK - 1) / kBK;
   if (nk > 0) {
-    load_a(0);
-    load_b(0);
+    load_a(kbeg);
+    load_b(kbeg);
     store(0);
   }
   __syncthreads();
   for (int t = 0; t < nk; ++t) {
     const int buf = t & 1;
     if (t + 1 < nk) {
-      load_a((t + 1) * kBK);
-      load_b((t + 1) * kBK);
+      load_a(kbeg + (t + 1) * kBK);
+      load_b(kbeg + (t + 1) * kBK);
     }
 #pragma unroll
     for (int kk = 0; kk < kBK; ++kk) {
@@ -440,17 +441,18 @@ __global__ void __launch_bounds__(512, 1) k_dgemm128(const GemmDesc* __restrict_
     }
   }
   const int kend = g.a_lower ? min(g.k, m0 + kLBM) : g.k;
-  const int nk = (kend + kLBK - 1) / kLBK;
+  const int kbeg = g.b_lower ? min(kend, n0) : 0;  // n0: a multiple of kLBK
+  const int nk = (kend - kbeg + kLBK - 1) / kLBK;
 #pragma unroll
   for (int st = 0; st < kLStages - 1; ++st) {
-    if (st < nk) issue(st, st * kLBK);
+    if (st < nk) issue(st, kbeg + st * kLBK);
     cp_async_commit();  // the first group also carries the C tile
   }
   for (int t = 0; t < nk; ++t) {
     cp_async_wait<kLStages - 2>();
     __syncthreads();
     const int nt = t + kLStages - 1;
-    if (nt < nk) issue(nt % kLStages, nt * kLBK);
+    if (nt < nk) issue(nt % kLStages, kbeg + nt * kLBK);
     cp_async_commit();
     const double* as = As + (t % kLStages) * kLBK * kLAStride;
     const double* bs = Bs + (t % kLStages) * kLBK * kLBStride;
@@ -1670,23 +1672,24 @@ void launch_chol_small(const SweepDesc* d_desc, int nd, int max_n, int* d_status
 // above the diagonal) and L_KK^{-1} into dinv, with D (128 x 128, lower
 // triangle read, padded with the identity past nb) in shared memory. This
 // kernel is on the critical path of the top levels, where one or a few blocks
-// remain, so it is built for latency:
-//   for each 32-wide panel p: warp 0 factors the 32 x 32 diagonal block with
-//   its rows in registers (pivots and multipliers passed by shuffles) and
-//   inverts it by forward substitution, lane = column; the CTA then solves the
-//   rows below against the inverse and updates the trailing lower triangle,
-//   each thread holding a 16-strided micro-tile of the outputs in registers
-//   (rows tx + 16a, columns ty + 16b), so that a warp's loads are 16
-//   consecutive doubles or broadcasts;
-//   then L^{-1} in place, block row ib by block row: for every block column
-//   jb < ib at once, Tb = L(ib, jb:ib) X(jb:ib, jb), then X(ib, jb) = -X_ib Tb.
-// Every sum runs over k in the same increasing order as the unblocked
-// elimination; terms added past a triangle's edge are exact zeros.
+// remain, so it is built for latency: the only serial work is the pivot chain
+// of each 32-wide panel.
+//   for each panel p: warp 0 factors the 32 x 32 diagonal block with its rows
+//   in registers (pivot and multipliers passed by shuffles; one reciprocal
+//   square root per pivot, kept for the rest); the rows below are solved
+//   against it by forward substitution, a thread per row; the trailing lower
+//   triangle is updated with each thread holding a 16-strided micro-tile of
+//   the outputs in registers (rows tx + 16a, columns ty + 16b), so that a
+//   warp's loads are 16 consecutive doubles or broadcasts;
+//   then the four 32 x 32 diagonal inverses, one warp each, and L^{-1} in
+//   place, block row ib by block row: for every block column jb < ib at once,
+//   Tb = L(ib, jb:ib) X(jb:ib, jb), then X(ib, jb) = -X_ib Tb.
 constexpr int kCdP = 32;             // panel width
 constexpr int kCdXs = kCdP + 1;      // padded stride of the diagonal inverses
 constexpr int kCdThreads = 256;
 constexpr size_t kCholDiagSmem =
-    (size_t)(kSweepNB * kSweepNB + 4 * kCdP * kCdXs + 3 * kCdP * kCdXs) * sizeof(double);
+    (size_t)(kSweepNB * kSweepNB + 4 * kCdP * kCdXs + 3 * kCdP * kCdXs + kSweepNB) *
+    sizeof(double);
 static_assert(kSweepNB == 4 * kCdP && kCdThreads == 256, "16 x 16 thread grid over 32-row panels");
 
 __global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __restrict__ descs,
@@ -1701,6 +1704,7 @@ __global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __res
   double* S = cd_sm;
   double* Xd = S + T * T;              // 4 diagonal inverses, [p][c][i] = X_pp(i, c)
   double* Tb = Xd + 4 * kCdP * kCdXs;  // 3 products of the inverse, [jb][c][k]
+  double* rd = Tb + 3 * kCdP * kCdXs;  // 1 / L(i, i)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tx = tid & 15, ty = tid >> 4;
   // the lower triangle only (the only one read), in whole columns; 16 loads
@@ -1724,19 +1728,23 @@ __global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __res
   int bad = 0;
   for (int p = 0; p < T / kCdP; ++p) {
     const int o = p * kCdP;
-    double* X = Xd + p * kCdP * kCdXs;
     if (warp == 0) {
       // Cholesky of the 32 x 32 diagonal block: lane = row, a[j] = D(lane, j)
       double a[kCdP];
 #pragma unroll
       for (int j = 0; j < kCdP; ++j) a[j] = S[(o + lane) + (o + j) * T];
+      double rmine = 1.0;  // 1 / L(lane, lane)
 #pragma unroll
       for (int k = 0; k < kCdP; ++k) {
         const double pv = __shfl_sync(0xffffffffu, a[k], k);
         if (lane == 0 && o + k < nb && (!(pv > 1e-300) || !isfinite(pv))) bad = 1;
-        const double dk = sqrt(fabs(pv) > 1e-300 ? fabs(pv) : 1.0);
-        if (lane > k) a[k] /= dk;
-        if (lane == k) a[k] = dk;
+        const double q = fabs(pv) > 1e-300 ? fabs(pv) : 1.0;
+        const double rk = rsqrt(q);
+        if (lane > k) a[k] *= rk;
+        if (lane == k) {
+          a[k] = q * rk;
+          rmine = rk;
+        }
         // D(lane, j) -= L(lane, k) L(j, k), k < j <= lane
 #pragma unroll
         for (int j = 1; j < kCdP; ++j) {
@@ -1748,51 +1756,31 @@ __global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __res
       }
 #pragma unroll
       for (int j = 0; j < kCdP; ++j) S[(o + lane) + (o + j) * T] = a[j];
-      __syncwarp();
-      // its inverse, lane = column c: X(c, c) = 1 / l_cc,
-      // X(i, c) = -(sum_{k=c}^{i-1} l_ik X(k, c)) / l_ii, zero above
-      const int c = lane;
-      double x[kCdP];
-#pragma unroll
-      for (int i = 0; i < kCdP; ++i) {
-        double acc = 0.0;
-#pragma unroll
-        for (int k = 0; k < kCdP - 1; ++k)
-          if (k < i) acc = fma(S[(o + i) + (o + k) * T], x[k], acc);
-        const double lii = S[(o + i) + (o + i) * T];
-        x[i] = i == c ? 1.0 / lii : (i > c ? -acc / lii : 0.0);
-      }
-#pragma unroll
-      for (int i = 0; i < kCdP; ++i) X[c * kCdXs + i] = x[i];
+      rd[o + lane] = rmine;
     }
     __syncthreads();
     const int r0 = o + kCdP, nrow = T - r0;
     if (nrow > 0) {
-      const int na = nrow / 16;  // 6, 4 or 2 row strides
-      // panel rows below: L(i, c) = sum_k A(i, k) X(c, k), X(c, k) = X[k kCdXs + c]
-      double acc[6][2];
+      // panel rows below, a thread per row: L(i, c) = (A(i, c) - sum_{k<c} L(i, k) L(c, k)) / L(c, c)
+      if (tid < nrow) {
+        const int i = r0 + tid;
+        double l[kCdP];
 #pragma unroll
-      for (int a = 0; a < 6; ++a) acc[a][0] = acc[a][1] = 0.0;
-#pragma unroll 4
-      for (int k = 0; k < kCdP; ++k) {
-        const double x0 = X[k * kCdXs + ty], x1 = X[k * kCdXs + ty + 16];
+        for (int c = 0; c < kCdP; ++c) l[c] = S[i + (o + c) * T];
 #pragma unroll
-        for (int a = 0; a < 6; ++a)
-          if (a < na) {
-            const double av = S[(r0 + tx + 16 * a) + (o + k) * T];
-            acc[a][0] = fma(av, x0, acc[a][0]);
-            acc[a][1] = fma(av, x1, acc[a][1]);
-          }
+        for (int c = 0; c < kCdP; ++c) {
+          double acc = l[c];
+#pragma unroll
+          for (int k = 0; k < kCdP - 1; ++k)
+            if (k < c) acc = fma(-l[k], S[(o + c) + (o + k) * T], acc);
+          l[c] = acc * rd[o + c];
+        }
+#pragma unroll
+        for (int c = 0; c < kCdP; ++c) S[i + (o + c) * T] = l[c];
       }
       __syncthreads();
-#pragma unroll
-      for (int a = 0; a < 6; ++a)
-        if (a < na) {
-          S[(r0 + tx + 16 * a) + (o + ty) * T] = acc[a][0];
-          S[(r0 + tx + 16 * a) + (o + ty + 16) * T] = acc[a][1];
-        }
-      __syncthreads();
       // trailing lower triangle: A(i, j) -= sum_k L(i, k) L(j, k)
+      const int na = nrow / 16;  // 6, 4 or 2 row strides
       double t[6][6];
 #pragma unroll
       for (int a = 0; a < 6; ++a)
@@ -1823,11 +1811,28 @@ __global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __res
     }
   }
   if (bad) atomicOr(status, kStatusTinyPivot);
-  // L over B[K, K]
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    d.B[(k0 + i) + (long long)(k0 + j) * d.n] = (i >= j) ? S[i + j * T] : 0.0;
+  // L over B[K, K]: warp per column
+  for (int j = warp; j < nb; j += kCdThreads / 32)
+    for (int i = lane; i < nb; i += 32)
+      d.B[(k0 + i) + (long long)(k0 + j) * d.n] = (i >= j) ? S[i + j * T] : 0.0;
+  // the diagonal inverses, warp p for block p, lane = column c:
+  // X(c, c) = 1 / l_cc, X(i, c) = -(sum_{k=c}^{i-1} l_ik X(k, c)) / l_ii, zero above
+  if (warp < T / kCdP) {
+    const int o = warp * kCdP, c = lane;
+    double x[kCdP];
+#pragma unroll
+    for (int i = 0; i < kCdP; ++i) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < kCdP - 1; ++k)
+        if (k < i) acc = fma(S[(o + i) + (o + k) * T], x[k], acc);
+      x[i] = i == c ? rd[o + i] : (i > c ? -acc * rd[o + i] : 0.0);
+    }
+    double* X = Xd + warp * kCdP * kCdXs;
+#pragma unroll
+    for (int i = 0; i < kCdP; ++i) X[c * kCdXs + i] = x[i];
   }
+  __syncthreads();
   // L^{-1} in place: the diagonal blocks first (X_jj, zeros above)
   for (int e = tid; e < 4 * kCdP * kCdP; e += blockDim.x) {
     const int jb = e / (kCdP * kCdP), r = e % (kCdP * kCdP), i = r % kCdP, c = r / kCdP;
@@ -1879,10 +1884,8 @@ __global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __res
     __syncthreads();
   }
   double* out = dinv + (long long)di * kSweepNB * kSweepNB;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    out[e] = (i >= j) ? S[i + j * T] : 0.0;
-  }
+  for (int j = warp; j < nb; j += kCdThreads / 32)
+    for (int i = lane; i < nb; i += 32) out[i + j * nb] = (i >= j) ? S[i + j * T] : 0.0;
 }
 
 void launch_chol_diag(const SweepDesc* d_desc, const int* d_active, int nact, int k0,
@@ -3142,14 +3145,19 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
   const long long ldu = g.uin ? g.ldu : ldu_k;
   const long long contrib_ld = g.uin ? g.cld : contrib_ld_k;
   __shared__ double xs[kXChunk][kRhsGroup];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (g.trans == 0) {
-    const int i = local * 256 + tid;
+    // 32-row strip, lane = row; of every staged chunk of x, warp w takes the
+    // 32 columns [32 w, 32 w + 32), so that a warp's loads are whole 256-byte
+    // column segments and several are in flight; the eight partial sums are
+    // added in warp order
+    __shared__ double red[8][32][kRhsGroup];
+    const int i = local * 32 + lane;
     for (int c0 = 0; c0 < nrhs; c0 += kRhsGroup) {
       const int nc = min(kRhsGroup, nrhs - c0);
       double acc[kRhsGroup] = {0.0, 0.0, 0.0, 0.0};
       // lower triangular: this strip's rows need no column right of its last row
-      const int jend = g.tri ? min(g.n, (local + 1) * 256) : g.n;
+      const int jend = g.tri ? min(g.n, (local + 1) * 32) : g.n;
       for (int j0 = 0; j0 < jend; j0 += kXChunk) {
         const int nj = min(kXChunk, jend - j0);
         __syncthreads();
@@ -3158,20 +3166,31 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
           xs[jj][cc] = (cc < nc) ? u_in[g.in_idx[j0 + jj] + (long long)(c0 + cc) * ldu] : 0.0;
         }
         __syncthreads();
-        if (i < g.m) {
-          const double* col = g.M + i + (long long)j0 * g.ld;
-          for (int jj = 0; jj < nj; ++jj) {
+        const int jb = warp * 32, cnt = min(32, nj - jb);
+        if (i < g.m && cnt > 0) {
+          const double* col = g.M + i + (long long)(j0 + jb) * g.ld;
+#pragma unroll 8
+          for (int jj = 0; jj < cnt; ++jj) {
             const double mv = col[(long long)jj * g.ld];
 #pragma unroll
-            for (int cc = 0; cc < kRhsGroup; ++cc) acc[cc] = fma(mv, xs[jj][cc], acc[cc]);
+            for (int cc = 0; cc < kRhsGroup; ++cc)
+              acc[cc] = fma(mv, xs[jb + jj][cc], acc[cc]);
           }
         }
       }
-      if (i < g.m)
-        for (int cc = 0; cc < nc; ++cc) gemv_emit(g, i, c0 + cc, acc[cc], u_out, ldu, contrib_ld);
+#pragma unroll
+      for (int cc = 0; cc < kRhsGroup; ++cc) red[warp][lane][cc] = acc[cc];
+      __syncthreads();
+      if (warp == 0 && i < g.m) {
+        for (int cc = 0; cc < nc; ++cc) {
+          double y = red[0][lane][cc];
+#pragma unroll
+          for (int w = 1; w < 8; ++w) y += red[w][lane][cc];
+          gemv_emit(g, i, c0 + cc, y, u_out, ldu, contrib_ld);
+        }
+      }
     }
   } else {
-    const int lane = tid & 31, warp = tid >> 5;
     for (int c0 = 0; c0 < nrhs; c0 += kRhsGroup) {
       const int nc = min(kRhsGroup, nrhs - c0);
       double acc[4][kRhsGroup];
@@ -3181,6 +3200,7 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
         for (int cc = 0; cc < kRhsGroup; ++cc) acc[q][cc] = 0.0;
       // lower triangular: these columns have no entry above their first column
       const int ibeg = g.tri ? ((local * 32) / kXChunk) * kXChunk : 0;
+      const int jw = local * 32 + warp * 4;  // this warp's first column
       for (int i0 = ibeg; i0 < g.m; i0 += kXChunk) {
         const int ni = min(kXChunk, g.m - i0);
         __syncthreads();
@@ -3189,21 +3209,22 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
           xs[ii][cc] = (cc < nc) ? u_in[g.in_idx[i0 + ii] + (long long)(c0 + cc) * ldu] : 0.0;
         }
         __syncthreads();
+        // the warp's four columns at each row: four independent loads a step
+#pragma unroll 2
+        for (int ii = lane; ii < ni; ii += 32) {
+          double mv[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int j = local * 32 + warp * 4 + q;
-          if (j >= g.n) continue;
-          const double* col = g.M + (long long)j * g.ld + i0;
-          for (int ii = lane; ii < ni; ii += 32) {
-            const double mv = col[ii];
+          for (int q = 0; q < 4; ++q)
+            mv[q] = jw + q < g.n ? g.M[(long long)(jw + q) * g.ld + i0 + ii] : 0.0;
 #pragma unroll
-            for (int cc = 0; cc < kRhsGroup; ++cc) acc[q][cc] = fma(mv, xs[ii][cc], acc[q][cc]);
-          }
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int cc = 0; cc < kRhsGroup; ++cc) acc[q][cc] = fma(mv[q], xs[ii][cc], acc[q][cc]);
         }
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int j = local * 32 + warp * 4 + q;
+        const int j = jw + q;
 #pragma unroll
         for (int cc = 0; cc < kRhsGroup; ++cc) {
           const double y = warp_sum(acc[q][cc]);
@@ -3370,11 +3391,11 @@ __global__ void __launch_bounds__(256, 3) k_gemv_small(const GemvFastSeg* __rest
   }
 }
 
-// Larger blocks: gemv_tile's tiles (y = M x: 256-row strips; y = M^T x:
+// Larger blocks: gemv_tile's tiles (y = M x: 32-row strips; y = M^T x:
 // 32-column tiles), located from the unit table (descriptor, tile) rather than
-// a search over tile offsets. Three CTAs per SM (the register cap keeps the
-// occupancy of this memory-bound kernel).
-__global__ void __launch_bounds__(256, 3) k_gemv_tiles(const GemvFastSeg* __restrict__ segs,
+// a search over tile offsets. Two CTAs per SM: each warp keeps eight column
+// loads in flight, which covers the memory latency at this occupancy.
+__global__ void __launch_bounds__(256, 2) k_gemv_tiles(const GemvFastSeg* __restrict__ segs,
                                                    const int* __restrict__ seg_off, int nseg,
                                                    const double* __restrict__ u_in,
                                                    double* __restrict__ u_out, int nrhs,
@@ -3386,7 +3407,8 @@ __global__ void __launch_bounds__(256, 3) k_gemv_tiles(const GemvFastSeg* __rest
 
 int gemv_tile_count(int m, int n, int trans) {
   if (m <= 0 || n <= 0) return 0;
-  return trans == 0 ? (m + 255) / 256 : (n + 31) / 32;
+  // y = M x: 32-row strips; y = M^T x: 32-column tiles
+  return ((trans == 0 ? m : n) + 31) / 32;
 }
 
 void launch_gemv_fast(const GemvFastSeg* d_segs, const int* d_seg_off, int nseg, int units,

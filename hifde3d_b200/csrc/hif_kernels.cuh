@@ -66,6 +66,7 @@ struct GemmDesc {
   int lower;  // 128 x 128 tiles only: skip the tiles above the diagonal (row tile < column tile)
   const int* skip;  // optional: the product is skipped when *skip != 0 (read on the device)
   int a_lower;  // op(A) is lower triangular (m = k): a row tile reads no k past its last row
+  int b_lower;  // op(B) is lower triangular (k = n): a column tile reads no k before its first column
 };
 
 // Dense elimination block: B (n x n, ld n) in assembly order [red | skel].
@@ -414,7 +415,7 @@ int copy_tiles(int m, int n);
 // contrib_ld: stride between right-hand sides in the contribution buffer.
 // The apply's GEMV launches (the engine's plans and the serving loop's batched
 // stages). Layouts: kGemvSmall, one warp per descriptor (both dimensions <=
-// kGemvSmallMax; units = descriptors); kGemvTiles, y = M x by 256-row strips or
+// kGemvSmallMax; units = descriptors); kGemvTiles, y = M x by 32-row strips or
 // y = M^T x by 32-column tiles (units = entries (descriptor, tile) of the
 // segment's table, gemv_tile_count tiles per descriptor). A launch covers
 // segments (one per operator or request) of one layout; seg_off: prefix of the
