@@ -31,7 +31,7 @@ HIF_ERR_STATE, HIF_ERR_NODEVICE, HIF_ERR_BUDGET, HIF_ERR_IO = 5, 6, 7, 8
 PARTITION_REFERENCE, PARTITION_CLIPPED = 0, 1
 OPT_KEEP_SCHUR, OPT_VERBOSE, OPT_MEM_BUDGET_MB, OPT_PROFILE, OPT_ID_GROUP_MIN_N = 1, 2, 3, 4, 5
 OPT_PRECISION, OPT_AUTOTUNE, OPT_SCHUR_SLICES, OPT_X_SLICES = 6, 7, 8, 9
-OPT_ELIMINATION, OPT_Y_SLICES, OPT_GRAM_MIN_N, OPT_GRAM_SLICES = 10, 11, 12, 13
+OPT_ELIMINATION, OPT_Y_SLICES, OPT_GRAM_MIN_N, OPT_GRAM_SLICES, OPT_CHOL_SLICES = 10, 11, 12, 13, 14
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 ELIM_AUTO, ELIM_GAUSS_JORDAN, ELIM_CHOLESKY = 0, 1, 2
 KCLASS_NAMES = ["gather", "gemm", "sweep_small", "sweep_panel", "id", "gemv", "copy", "vector",

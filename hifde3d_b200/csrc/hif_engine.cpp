@@ -155,26 +155,93 @@ T* upload(const std::vector<T>& v, cudaStream_t s) {
   return d;
 }
 
+// Host worker pool for parallel_for, started on first use and kept for the
+// process (several host threads run parallel loops at once: a factorization's
+// partition threads, the serving loop's factor workers). A loop is a job on
+// its caller's stack; idle workers take 64-index chunks of any open job, the
+// caller takes chunks too, and it returns once every chunk has run and no
+// worker holds the job. Workers are created once, not per loop: the lower
+// levels run dozens of loops per factorization.
+class HostPool {
+ public:
+  struct Job {
+    const std::function<void(int)>* f;
+    int n;
+    std::atomic<int> next{0};
+    int holders = 0;  // workers inside the job (guarded by mu_)
+  };
+  static HostPool& get() {
+    static HostPool* p = new HostPool;  // never destroyed: workers live for the process
+    return *p;
+  }
+  int workers() const { return (int)workers_.size(); }
+  void run(Job& job) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      jobs_.push_back(&job);
+    }
+    cv_.notify_all();
+    work(job);
+    std::unique_lock<std::mutex> lk(mu_);
+    jobs_.erase(std::find(jobs_.begin(), jobs_.end(), &job));
+    done_cv_.wait(lk, [&] { return job.holders == 0; });
+  }
+
+ private:
+  HostPool() {
+    const int nt = std::min<int>(std::max(1u, std::thread::hardware_concurrency()), 32) - 1;
+    for (int t = 0; t < nt; ++t) workers_.emplace_back([this] { loop(); });
+  }
+  static void work(Job& j) {
+    for (;;) {
+      const int i0 = j.next.fetch_add(64);
+      if (i0 >= j.n) break;
+      const int i1 = std::min(j.n, i0 + 64);
+      for (int i = i0; i < i1; ++i) (*j.f)(i);
+    }
+  }
+  Job* open_job() {
+    for (Job* j : jobs_)
+      if (j->next.load() < j->n) return j;
+    return nullptr;
+  }
+  void loop() {
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      // the job found by the wait is the one taken: `next` moves without the
+      // lock, so a second search could find none
+      Job* j = nullptr;
+      cv_.wait(lk, [&] { return (j = open_job()) != nullptr; });
+      ++j->holders;
+      lk.unlock();
+      work(*j);
+      lk.lock();
+      if (--j->holders == 0) done_cv_.notify_all();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  std::vector<Job*> jobs_;
+  std::vector<std::thread> workers_;
+};
+
 // Host parallel loop over [0, n) in chunks (partitioning of cells / faces).
 template <class F>
 void parallel_for(int n, F&& f) {
-  const int nt = std::min<int>(std::max(1u, std::thread::hardware_concurrency()), 32);
-  if (n < 256 || nt <= 1) {
+  if (n < 256) {
     for (int i = 0; i < n; ++i) f(i);
     return;
   }
-  std::atomic<int> next(0);
-  std::vector<std::thread> th;
-  for (int t = 0; t < nt; ++t)
-    th.emplace_back([&] {
-      for (;;) {
-        const int i0 = next.fetch_add(64);
-        if (i0 >= n) break;
-        const int i1 = std::min(n, i0 + 64);
-        for (int i = i0; i < i1; ++i) f(i);
-      }
-    });
-  for (std::thread& x : th) x.join();
+  HostPool& pool = HostPool::get();
+  if (pool.workers() == 0) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  const std::function<void(int)> fn = [&](int i) { f(i); };
+  HostPool::Job job;
+  job.f = &fn;
+  job.n = n;
+  pool.run(job);
 }
 
 // Keeps device buffers of one phase alive until released together.
@@ -618,9 +685,11 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
   ScratchScope scope;
   const int bn = oz_tile_n(slices);
   constexpr int kChunkTiles = kOzMaxK / kOzK;
-  // op(B)^T = op(A) (the S = A11 - Y^T Y products): B's converted rows are A's
+  // op(B)^T = op(A) (S = A11 - Y^T Y, and the Cholesky updates P P^T): B's
+  // converted rows are A's
   auto same_operand = [](const GemmDesc& x) {
-    return x.A == x.B && x.lda == x.ldb && x.transA == 1 && x.transB == 0 && x.m == x.n;
+    return x.A == x.B && x.lda == x.ldb && x.m == x.n &&
+           ((x.transA == 1 && x.transB == 0) || (x.transA == 0 && x.transB == 1));
   };
   long long parts = 0, nexp = 0;
   for (const GemmDesc& x : gin) {
@@ -651,7 +720,10 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
       for (int i = 0; i < tm; ++i) {
         const int cols = x.lower ? std::min(tn, (i * 128 + 128 + bn - 1) / bn) : tn;
         const int kti = x.a_lower ? std::min(kt, (i * 128 + 128 + kOzK - 1) / kOzK) : kt;
-        tk += (double)cols * kti;
+        if (x.b_lower)
+          for (int j = 0; j < cols; ++j) tk += std::max(0, kti - j * bn / kOzK);
+        else
+          tk += (double)cols * kti;
       }
       fl += pairs * 2.0 * 128.0 * bn * kOzK * tk;
     }
@@ -676,7 +748,7 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
       if ((int)launches.size() <= c) launches.emplace_back();
       launches[c].push_back(OzGemm{pa, pb, ea, eb, x.C, x.ldc, x.m, x.n, kt, kt0,
                                    std::min(kChunkTiles, std::max(0, kt - kt0)), x.alpha,
-                                   c == 0 ? x.beta : 1.0, x.lower, x.a_lower});
+                                   c == 0 ? x.beta : 1.0, x.lower, x.a_lower, x.b_lower});
     }
   }
   timed(HIF_KCLASS_GEMM_INT8, fl, 0.0, [&] {
@@ -709,9 +781,13 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
 // (0) or from `x` int8 slices. The Gauss-Jordan updates of A22^{-1} are rank-128
 // products, bound by the traffic of their target rather than by arithmetic, and
 // stay FP64.
+// chol: in the Cholesky elimination, the trailing updates of the pivot-block
+// factorization and the products forming L^{-1} in FP64 (0) or from `chol`
+// int8 slices.
 struct ElimArith {
   int schur = -1;
   int x = 0;
+  int chol = 0;
 };
 
 // Cholesky elimination of a batch of symmetric positive definite interiors
@@ -846,7 +922,8 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
       timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dq, doq, (int)cq.size(), ocq.back(), stream); });
     }
     gemm_batch(gp, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
-    gemm_batch(gu, step, stream, HIF_KCLASS_GEMM, timed, 128);
+    if (ar.chol > 0) gemm_batch_int8(gu, step, stream, timed, ar.chol, d_status);
+    else gemm_batch(gu, step, stream, HIF_KCLASS_GEMM, timed, 128);
     {
       CopyDesc* dc = step.add(upload(cdg, stream));
       int* doc = step.add(upload(ocd, stream));
@@ -933,8 +1010,13 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
         x.alpha = -1.0;
         g2.push_back(x);
       }
-      gemm_batch(g1, tmp, stream, HIF_KCLASS_SWEEP_PANEL, timed);
-      gemm_batch(g2, tmp, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+      if (ar.chol > 0) {
+        gemm_batch_int8(g1, tmp, stream, timed, ar.chol, d_status);
+        gemm_batch_int8(g2, tmp, stream, timed, ar.chol, d_status);
+      } else {
+        gemm_batch(g1, tmp, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+        gemm_batch(g2, tmp, stream, HIF_KCLASS_SWEEP_PANEL, timed);
+      }
     }
   }
   // Y = L^{-1} A21 and S = A11 - Y^T Y
@@ -1773,6 +1855,7 @@ class Engine {
     if (precision == HIF_PRECISION_MIXED) {
       ar.schur = schur_slices;
       ar.x = chol ? y_slices : x_slices;
+      ar.chol = chol ? chol_slices : 0;
     }
     auto tm = [&](int cls, double fl, double by, auto&& f, int n = 1) { timed(cls, fl, by, f, n); };
     if (chol) chol_blocks(descs, tmp, stream, d_status, tm, ar, cur_work);
@@ -3001,7 +3084,7 @@ class Engine {
   bool autotune = false;
   // HIF_PRECISION_MIXED: int8 slices of the Schur products (0: split TF32) and
   // of the X products (0: FP64)
-  int schur_slices = 5, x_slices = 7, y_slices = 6;
+  int schur_slices = 5, x_slices = 7, y_slices = 6, chol_slices = 0;
   // HIF_OPT_ELIMINATION, and the choice made for the factorization in progress
   int elimination = HIF_ELIM_AUTO;
   bool use_chol = false;
@@ -4049,6 +4132,10 @@ int hif_set_option(hif_handle h, int option, long long value) {
     case HIF_OPT_Y_SLICES:
       if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
       h->e->y_slices = (int)value;
+      return HIF_OK;
+    case HIF_OPT_CHOL_SLICES:
+      if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;
+      h->e->chol_slices = (int)value;
       return HIF_OK;
     case HIF_OPT_GRAM_SLICES:
       if (value != 0 && (value < 2 || value > hif::kOzMaxS)) return HIF_ERR_ARG;

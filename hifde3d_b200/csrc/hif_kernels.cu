@@ -169,55 +169,56 @@ __global__ void __launch_bounds__(256) k_gather(const GatherTarget* __restrict__
       s_col[threadIdx.x] = q;
       resolve_cover(g, q, dof_src, src_owner, ncell3, s_cc[threadIdx.x]);
     }
-    // this thread's row: DOF, stencil row and source rows
+    // this thread's row: DOF, stencil row and source rows (a source's entries
+    // are addressed with 32-bit positions times its leading dimension)
     const int i = i0 + lane;
     const int p = (i < g.m) ? g.rows[i] : -1;
     CoverEntry rc[kCover];
     resolve_cover(g, p, dof_src, src_owner, ncell3, rc);
     const double* rp[kCover];
-    long long rld[kCover];
+    int rs[kCover], rld[kCover];
 #pragma unroll
     for (int a = 0; a < kCover; ++a) {
+      rs[a] = rc[a].src;
       rp[a] = nullptr;
       rld[a] = 0;
       if (rc[a].src >= 0) {
         const SourceDesc sd = src[rc[a].src];
         rp[a] = sd.ptr + rc[a].pos;
-        rld[a] = sd.ld;
+        rld[a] = (int)sd.ld;
       }
     }
     __syncthreads();
     if (i < g.m) {
       const bool row_a0 = i < g.a0_skip;
+      const bool row_a22 = g.a22_out != nullptr && i < g.r;
+      const int ld = (int)g.ld;
+      double* orow = g.out + i;
 #pragma unroll 2
       for (int cc = warp; cc < kGTN; cc += 8) {
         const int j = j0 + cc;
         if (j >= g.n) break;
-        const int q = s_col[cc];
         double v = 0.0;
         if (row_a0 || j < g.a0_skip) {
-          const int dd = q - p;
-          int b = -1;
-          if (dd == 0) b = 0;
-          else if (dd == -1) b = 1;
-          else if (dd == 1) b = 2;
-          else if (dd == -NC) b = 3;
-          else if (dd == NC) b = 4;
-          else if (dd == -NC2) b = 5;
-          else if (dd == NC2) b = 6;
-          if (b >= 0) v = band[b * ncell3 + p];
+          // stencil term: q - p in {0, -1, 1, -NC, NC, -NC^2, NC^2} -> bands 0..6
+          const int dd = s_col[cc] - p, ad = abs(dd);
+          if (ad == 0 || ad == 1 || ad == NC || ad == NC2) {
+            const int b = (ad == 0 ? 0 : (ad == 1 ? 1 : (ad == NC ? 3 : 5))) + (dd > 0 ? 1 : 0);
+            v = band[b * ncell3 + p];
+          }
         }
+        // sources holding both DOFs, in the column's cover order (a column cover
+        // is warp-uniform, so an empty one is skipped by the whole warp)
 #pragma unroll
         for (int c = 0; c < kCover; ++c) {
-          const int sc = s_cc[cc][c].src;
-          if (sc < 0) continue;
-          const long long pc = s_cc[cc][c].pos;
+          const CoverEntry ce = s_cc[cc][c];
+          if (ce.src < 0) continue;
 #pragma unroll
           for (int a = 0; a < kCover; ++a)
-            if (rc[a].src == sc) v += rp[a][pc * rld[a]];
+            if (rs[a] == ce.src) v += rp[a][(long long)ce.pos * rld[a]];
         }
-        g.out[i + (long long)j * g.ld] = v;
-        if (g.a22_out != nullptr && i < g.r && j < g.r) g.a22_out[i + (long long)j * g.r] = v;
+        orow[(long long)j * ld] = v;
+        if (row_a22 && j < g.r) g.a22_out[i + (long long)j * g.r] = v;
       }
     }
   }
@@ -335,6 +336,16 @@ __global__ void __launch_bounds__(256) k_dgemm(const GemmDesc* __restrict__ desc
     if (t + 1 < nk) store(buf ^ 1);
     __syncthreads();
   }
+  // with beta != 0 every C entry is loaded before the first store, so that the
+  // 16 loads are in flight together
+  double cv[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int gm = m0 + tx + 16 * a, gn = n0 + ty + 16 * b;
+      cv[a][b] = (g.beta != 0.0 && gm < g.m && gn < g.n) ? g.C[gm + (long long)gn * g.ldc] : 0.0;
+    }
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
     const int gn = n0 + ty + 16 * b;
@@ -343,9 +354,8 @@ __global__ void __launch_bounds__(256) k_dgemm(const GemmDesc* __restrict__ desc
     for (int a = 0; a < 4; ++a) {
       const int gm = m0 + tx + 16 * a;
       if (gm >= g.m) continue;
-      double* c = g.C + gm + (long long)gn * g.ldc;
       const double v = g.alpha * acc[a][b];
-      *c = (g.beta == 0.0) ? v : fma(g.beta, *c, v);
+      g.C[gm + (long long)gn * g.ldc] = (g.beta == 0.0) ? v : fma(g.beta, cv[a][b], v);
     }
   }
 }
@@ -829,13 +839,19 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const TcGemm* __restrict__ d
               : "memory");
           asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         } else if (gm < g.m) {
+          // the 16 C entries loaded before the first store (in flight together)
+          double cv[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int gn = n0 + 16 * cc + e;
+            cv[e] = (g.beta != 0.0 && gn < g.n) ? g.C[gm + (long long)gn * g.ldc] : 0.0;
+          }
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
             const int gn = n0 + 16 * cc + e;
             if (gn < g.n) {
-              double* cp = g.C + gm + (long long)gn * g.ldc;
               const double val = g.alpha * acc[e];
-              *cp = (g.beta == 0.0) ? val : fma(g.beta, *cp, val);
+              g.C[gm + (long long)gn * g.ldc] = (g.beta == 0.0) ? val : fma(g.beta, cv[e], val);
             }
           }
         }
@@ -1147,7 +1163,10 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   // tile decode shared by the roles
-  auto tile = [&](int t, OzGemm& g, int& mt, int& nt, int& kt_cnt) -> bool {
+  // k tiles [kf, kt_cnt) of the launch's range run: with a lower-triangular A
+  // none past the tile's last row, with a lower-triangular B none before its
+  // first column
+  auto tile = [&](int t, OzGemm& g, int& mt, int& nt, int& kf, int& kt_cnt) -> bool {
     const int di = find_desc(tile_off, nd, t);
     g = descs[di];
     const int local = t - tile_off[di];
@@ -1156,8 +1175,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
     nt = local / tiles_m;
     const int m0 = mt * 128, n0 = nt * BN;
     if (g.lower && n0 >= m0 + 128) return false;
-    // with a lower-triangular A no k tile past the tile's last row
     kt_cnt = g.a_lower ? min(g.kt_cnt, max(0, (m0 + 128 + kOzK - 1) / kOzK - g.kt0)) : g.kt_cnt;
+    kf = g.b_lower ? min(kt_cnt, max(0, n0 / kOzK - g.kt0)) : 0;
     return true;
   };
 
@@ -1188,11 +1207,11 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
     int it = 0;
     for (int t = blockIdx.x; t < total_tiles && !*abort; t += gridDim.x) {
       OzGemm g;
-      int mt, nt, kt_cnt;
-      if (!tile(t, g, mt, nt, kt_cnt)) continue;
+      int mt, nt, kf, kt_cnt;
+      if (!tile(t, g, mt, nt, kf, kt_cnt)) continue;
       const int n0 = nt * BN, bt = n0 / 128, bhalf = (n0 / 64) & 1;
       bool ok = true;
-      for (int i = 0; i < kt_cnt; ++i, ++it) {
+      for (int i = kf; i < kt_cnt; ++i, ++it) {
         const int kt = g.kt0 + i, s = it % NS;
         if (it >= NS && !mbar_wait(smem_u32(&empty[s]), (unsigned)((it / NS - 1) & 1), abort)) {
           ok = false;
@@ -1221,13 +1240,13 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
     int it = 0, a = 0;
     for (int t = blockIdx.x; t < total_tiles && !*abort; t += gridDim.x) {
       OzGemm g;
-      int mt, nt, kt_cnt;
-      if (!tile(t, g, mt, nt, kt_cnt) || kt_cnt == 0) continue;
+      int mt, nt, kf, kt_cnt;
+      if (!tile(t, g, mt, nt, kf, kt_cnt) || kt_cnt <= kf) continue;
       // the previous tile's accumulators have been read
       if (a > 0 && !mbar_wait(smem_u32(tempty), (unsigned)((a - 1) & 1), abort)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       bool ok = true;
-      for (int i = 0; i < kt_cnt; ++i, ++it) {
+      for (int i = kf; i < kt_cnt; ++i, ++it) {
         const int s = it % NS;
         if (!mbar_wait(smem_u32(&full[s]), (unsigned)((it / NS) & 1), abort)) {
           ok = false;
@@ -1243,7 +1262,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
 #pragma unroll
             for (int q = 0; p + q < S; ++q) {
               const unsigned long long db = oz_desc(base + Cfg::kA + q * BN * kOzK + 256 * j);
-              const unsigned acc = (i > 0 || j > 0 || p > 0) ? 1u : 0u;
+              const unsigned acc = (i > kf || j > 0 || p > 0) ? 1u : 0u;
               const unsigned d = tmem + (unsigned)((p + q) * BN);
               // A slice p is read from shared memory once per 32-k step and kept
               // in the collector buffer for its other slice pairs
@@ -1278,8 +1297,9 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
     int a = 0;
     for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
       OzGemm g;
-      int mt, nt, kt_cnt;
-      if (!tile(t, g, mt, nt, kt_cnt)) continue;
+      int mt, nt, kf, kt_cnt;
+      if (!tile(t, g, mt, nt, kf, kt_cnt)) continue;
+      kt_cnt -= kf;  // k tiles run
       const int gm = mt * 128 + 32 * q4 + lane, n0 = nt * BN;
       bool ok = true;
       if (kt_cnt > 0) {
@@ -1323,13 +1343,29 @@ __global__ void __launch_bounds__(256, 1) k_gemm_oz(const OzGemm* __restrict__ d
           }
         }
         if (gm < g.m) {
+          // 16 columns at a time: their C entries and column exponents are
+          // loaded before any store, so the loads are in flight together (a
+          // load after a store to C would wait for it: the compiler cannot rule
+          // out aliasing)
+          double* crow = g.C + gm;
 #pragma unroll
-          for (int e = 0; e < 64; ++e) {
-            const int gn = n0 + 64 * half + e;
-            if (gn < g.n) {
-              double* cp = g.C + gm + (long long)gn * g.ldc;
-              const double val = g.alpha * ldexp(h[e], ea + max(g.eb[gn], -4096) - 14);
-              *cp = (g.beta == 0.0) ? val : fma(g.beta, *cp, val);
+          for (int e0 = 0; e0 < 64; e0 += 16) {
+            double cv[16];
+            int fe[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              const int gn = n0 + 64 * half + e0 + e;
+              const bool in = gn < g.n;
+              fe[e] = in ? g.eb[gn] : 0;
+              cv[e] = (in && g.beta != 0.0) ? crow[(long long)gn * g.ldc] : 0.0;
+            }
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              const int gn = n0 + 64 * half + e0 + e;
+              if (gn < g.n) {
+                const double val = g.alpha * ldexp(h[e0 + e], ea + max(fe[e], -4096) - 14);
+                crow[(long long)gn * g.ldc] = (g.beta == 0.0) ? val : fma(g.beta, cv[e], val);
+              }
             }
           }
         }

@@ -302,6 +302,7 @@ struct OzGemm {
   double alpha, beta;
   int lower;  // skip the tiles entirely above the diagonal
   int a_lower;  // op(A) lower triangular: a 128-row tile reads no k tile past its last row
+  int b_lower;  // op(B) lower triangular: a column tile reads no k tile before its first column
 };
 // C = alpha op(A) op(B) + beta C from converted operands with `slices` slices
 // (2..kOzMaxS); d_tile_off counts tiles of 128 x oz_tile_n(slices) columns.

@@ -164,6 +164,55 @@ def test_mixed_cholesky_close_to_fp64(N, partition):
     fd.close()
 
 
+def test_mixed_cholesky_int8_factor_products():
+    """HIF_OPT_CHOL_SLICES: the trailing updates of the pivot-block factorization
+    and the products forming L^{-1} from 7 int8 slices against FP64 products (0,
+    the default), at n = 64 where the top blocks span many 128-pivot blocks: the
+    stored factors stay consistent (L lower, L L^{-1} = I to 1e-10), the inverse
+    applies agree to the mixed arithmetic's own level and PCG needs no more
+    iterations."""
+    N = 63
+    ax, ay, az, V = face_inputs(N)
+    fs = {}
+    for slices in (0, 7):
+        f = hb.HIFFactor(N, 4, 1e-6)
+        f.set_option(hb.OPT_PRECISION, hb.PRECISION_MIXED)
+        f.set_option(hb.OPT_ELIMINATION, hb.ELIM_CHOLESKY)
+        f.set_option(hb.OPT_CHOL_SLICES, slices)
+        hb.SetupStencilFaces(f, N, 1.0 / (N + 1), ax, ay, az, V)
+        f.Factor()
+        fs[slices] = f
+    f = fs[7]
+    top = f.num_levels() - 1
+    info = f.block(top, 0, 0)
+    r = info["red"].size
+    assert r > 4 * 128
+    raw = {}
+    for which in (5, 6):
+        buf = np.zeros(r * r)
+        assert hb.lib().hif_block_matrix(f._h, top, 0, 0, which, hb._dptr(buf)) == hb.HIF_OK
+        raw[which] = buf.reshape(r, r).T
+    L, Li = raw[5], raw[6]
+    assert np.all(np.triu(L, 1) == 0) and np.all(np.triu(Li, 1) == 0)
+    assert np.abs(L @ Li - np.eye(r)).max() < 1e-10
+    u = synth.dof_vector(N, 5)
+    y0, y7 = u.copy(), u.copy()
+    fs[0].Apply(y0, True)
+    fs[7].Apply(y7, True)
+    assert rel(y7, y0) < 1e-5
+    _, it0, _ = fs[0].solve_pcg(u, tol=1e-10, maxit=50)
+    _, it7, rr7 = fs[7].solve_pcg(u, tol=1e-10, maxit=50)
+    assert rr7 <= 1e-10 and it7 <= it0
+    for g in fs.values():
+        g.close()
+    with pytest.raises(hb.HIFError):
+        h = hb.HIFFactor(N, 4, 1e-6)
+        try:
+            h.set_option(hb.OPT_CHOL_SLICES, 9)
+        finally:
+            h.close()
+
+
 def test_cholesky_multi_rhs_and_save_load():
     """16+ right-hand sides (gather / GEMM / emit apply) equal the single-RHS apply;
     a saved Cholesky factor reloads bit-identically."""
