@@ -1943,8 +1943,10 @@ class Engine {
       });
     }
     mark("schur cell partition", level);
-    // sizes and device layout
-    std::vector<int> red_all, skel_all;
+    // sizes and device layout (the flat lists reuse the handle's host buffers:
+    // their pages are touched once, not at every factorization)
+    std::vector<int>& red_all = h_red_all;
+    std::vector<int>& skel_all = h_skel_all;
     long long bsz = 0, asz = 0;
     std::vector<long long> o_B(ncell);
     st.o_a22.resize(ncell);
@@ -1953,7 +1955,7 @@ class Engine {
     st.o_w.assign(ncell, 0);
     st.o_red.resize(ncell);
     st.o_skel.resize(ncell);
-    std::vector<int> rows_all;
+    std::vector<int>& rows_all = h_rows_all;
     std::vector<long long> o_rows(ncell);
     long long nred = 0, nskel = 0;
     for (int b = 0; b < ncell; ++b) {
@@ -2134,18 +2136,27 @@ class Engine {
         if (cl.empty()) continue;
         BlockInfo b;
         b.face = face;
-        b.global = cl;
+        b.global = std::move(cl);
         b.cell = idx;
         b.nbr = (nb[0] * cpd + nb[1]) * cpd + nb[2];
         pb[idx].push_back(std::move(b));
-        pr[idx].push_back(rw);
+        pr[idx].push_back(std::move(rw));
+        rw.clear();
+        cl.clear();
       }
     });
-    for (int idx = 0; idx < ncell; ++idx)
+    // cell order, merged in parallel into place
+    std::vector<int> off(ncell + 1, 0);
+    for (int idx = 0; idx < ncell; ++idx) off[idx + 1] = off[idx] + (int)pb[idx].size();
+    const size_t base = blocks.size();
+    blocks.resize(base + off[ncell]);
+    rows_l.resize(base + off[ncell]);
+    parallel_for(ncell, [&](int idx) {
       for (size_t q = 0; q < pb[idx].size(); ++q) {
-        blocks.push_back(std::move(pb[idx][q]));
-        rows_l.push_back(std::move(pr[idx][q]));
+        blocks[base + off[idx] + q] = std::move(pb[idx][q]);
+        rows_l[base + off[idx] + q] = std::move(pr[idx][q]);
       }
+    });
   }
 
   // The face partition of a level depends only on the DOFs left after that
@@ -2482,7 +2493,9 @@ class Engine {
 
     // skeleton / redundant sets (InterpDecomp.cpp:102-110), internal order
     th = wall();
-    std::vector<int> red_all, skel_all, rows2;
+    std::vector<int>& red_all = h_red_all;
+    std::vector<int>& skel_all = h_skel_all;
+    std::vector<int>& rows2 = h_rows_all;
     std::vector<long long> o_B(nf), o_r2(nf);
     long long bsz = 0, asz = 0;
     st.o_a22.resize(nf);
@@ -2496,6 +2509,10 @@ class Engine {
       const int n = b.global.size();
       b.jpvt.assign(h_jp.begin() + o_i[f], h_jp.begin() + o_i[f] + n);
       b.rdiag.assign(h_rd.begin() + o_i[f], h_rd.begin() + o_i[f] + n);
+      int k = 0;
+      for (int i = 0; i < n; ++i) k += h_keep[o_i[f] + i] != 0;
+      b.skel_pos.reserve(k);
+      b.red_pos.reserve(n - k);
       for (int i = 0; i < n; ++i) {
         if (h_keep[o_i[f] + i]) b.skel_pos.push_back(b.jpvt[i]);
         else b.red_pos.push_back(b.jpvt[i]);
@@ -3085,6 +3102,9 @@ class Engine {
   // HIF_PRECISION_MIXED: int8 slices of the Schur products (0: split TF32) and
   // of the X products (0: FP64)
   int schur_slices = 5, x_slices = 7, y_slices = 6, chol_slices = 0;
+  // host index lists of the phase being built, kept across phases and
+  // factorizations
+  std::vector<int> h_red_all, h_skel_all, h_rows_all;
   // HIF_OPT_ELIMINATION, and the choice made for the factorization in progress
   int elimination = HIF_ELIM_AUTO;
   bool use_chol = false;
