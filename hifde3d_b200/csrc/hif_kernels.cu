@@ -3170,6 +3170,10 @@ __device__ __forceinline__ void gemv_emit(const GemvDesc& g, int i, int c, doubl
   else u_out[g.out_idx[i] + (long long)c * ldu] = g.alpha * y;
 }
 
+// RG right-hand sides per pass: 4, or 1 for single-vector launches (fewer
+// registers, so more CTAs and more loads in flight); a column of results is the
+// same sequence of operations either way.
+template <int RG>
 __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
                                           const double* __restrict__ u_in_k,
                                           double* __restrict__ u_out_k, int nrhs_k,
@@ -3180,25 +3184,86 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
   const int nrhs = g.uin ? g.nrhs : nrhs_k;
   const long long ldu = g.uin ? g.ldu : ldu_k;
   const long long contrib_ld = g.uin ? g.cld : contrib_ld_k;
-  __shared__ double xs[kXChunk][kRhsGroup];
+  __shared__ double xs[kXChunk][RG];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if constexpr (RG == 1) {
+    // one vector: x is read where it is used (a broadcast load per column or
+    // row) instead of being staged per chunk, so no barrier interrupts the
+    // stream of M; the columns of each warp and the order of every sum are
+    // those of the staged form, so the results are the same bit for bit
+    if (g.trans == 0) {
+      __shared__ double red1[8][32];
+      const int i = local * 32 + lane;
+      for (int c0 = 0; c0 < nrhs; ++c0) {
+        double acc = 0.0;
+        const int jend = g.tri ? min(g.n, (local + 1) * 32) : g.n;
+        for (int j0 = 0; j0 < jend; j0 += kXChunk) {
+          const int jb = warp * 32, cnt = min(32, min(kXChunk, jend - j0) - jb);
+          if (i < g.m && cnt > 0) {
+            const double* col = g.M + i + (long long)(j0 + jb) * g.ld;
+            const int* idx = g.in_idx + j0 + jb;
+            const double* x = u_in + (long long)c0 * ldu;
+#pragma unroll 16
+            for (int jj = 0; jj < cnt; ++jj)
+              acc = fma(col[(long long)jj * g.ld], x[idx[jj]], acc);
+          }
+        }
+        __syncthreads();  // the previous vector's sums have been read
+        red1[warp][lane] = acc;
+        __syncthreads();
+        if (warp == 0 && i < g.m) {
+          double y = red1[0][lane];
+#pragma unroll
+          for (int w = 1; w < 8; ++w) y += red1[w][lane];
+          gemv_emit(g, i, c0, y, u_out, ldu, contrib_ld);
+        }
+      }
+    } else {
+      const int jw = local * 32 + warp * 4;
+      const int ibeg = g.tri ? ((local * 32) / kXChunk) * kXChunk : 0;
+      for (int c0 = 0; c0 < nrhs; ++c0) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        const double* x = u_in + (long long)c0 * ldu;
+        for (int i0 = ibeg; i0 < g.m; i0 += kXChunk) {
+          const int ni = min(kXChunk, g.m - i0);
+#pragma unroll 2
+          for (int ii = lane; ii < ni; ii += 32) {
+            const double xv = x[g.in_idx[i0 + ii]];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const double mv = jw + q < g.n ? g.M[(long long)(jw + q) * g.ld + i0 + ii] : 0.0;
+              acc[q] = fma(mv, xv, acc[q]);
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double y = warp_sum(acc[q]);
+          if (lane == 0 && jw + q < g.n) gemv_emit(g, jw + q, c0, y, u_out, ldu, contrib_ld);
+        }
+      }
+    }
+    return;
+  }
   if (g.trans == 0) {
     // 32-row strip, lane = row; of every staged chunk of x, warp w takes the
     // 32 columns [32 w, 32 w + 32), so that a warp's loads are whole 256-byte
     // column segments and several are in flight; the eight partial sums are
     // added in warp order
-    __shared__ double red[8][32][kRhsGroup];
+    __shared__ double red[8][32][RG];
     const int i = local * 32 + lane;
-    for (int c0 = 0; c0 < nrhs; c0 += kRhsGroup) {
-      const int nc = min(kRhsGroup, nrhs - c0);
-      double acc[kRhsGroup] = {0.0, 0.0, 0.0, 0.0};
+    for (int c0 = 0; c0 < nrhs; c0 += RG) {
+      const int nc = min(RG, nrhs - c0);
+      double acc[RG];
+#pragma unroll
+      for (int cc = 0; cc < RG; ++cc) acc[cc] = 0.0;
       // lower triangular: this strip's rows need no column right of its last row
       const int jend = g.tri ? min(g.n, (local + 1) * 32) : g.n;
       for (int j0 = 0; j0 < jend; j0 += kXChunk) {
         const int nj = min(kXChunk, jend - j0);
         __syncthreads();
-        for (int e = tid; e < nj * kRhsGroup; e += 256) {
-          const int jj = e / kRhsGroup, cc = e % kRhsGroup;
+        for (int e = tid; e < nj * RG; e += 256) {
+          const int jj = e / RG, cc = e % RG;
           xs[jj][cc] = (cc < nc) ? u_in[g.in_idx[j0 + jj] + (long long)(c0 + cc) * ldu] : 0.0;
         }
         __syncthreads();
@@ -3209,13 +3274,13 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
           for (int jj = 0; jj < cnt; ++jj) {
             const double mv = col[(long long)jj * g.ld];
 #pragma unroll
-            for (int cc = 0; cc < kRhsGroup; ++cc)
+            for (int cc = 0; cc < RG; ++cc)
               acc[cc] = fma(mv, xs[jb + jj][cc], acc[cc]);
           }
         }
       }
 #pragma unroll
-      for (int cc = 0; cc < kRhsGroup; ++cc) red[warp][lane][cc] = acc[cc];
+      for (int cc = 0; cc < RG; ++cc) red[warp][lane][cc] = acc[cc];
       __syncthreads();
       if (warp == 0 && i < g.m) {
         for (int cc = 0; cc < nc; ++cc) {
@@ -3227,21 +3292,21 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
       }
     }
   } else {
-    for (int c0 = 0; c0 < nrhs; c0 += kRhsGroup) {
-      const int nc = min(kRhsGroup, nrhs - c0);
-      double acc[4][kRhsGroup];
+    for (int c0 = 0; c0 < nrhs; c0 += RG) {
+      const int nc = min(RG, nrhs - c0);
+      double acc[4][RG];
 #pragma unroll
       for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int cc = 0; cc < kRhsGroup; ++cc) acc[q][cc] = 0.0;
+        for (int cc = 0; cc < RG; ++cc) acc[q][cc] = 0.0;
       // lower triangular: these columns have no entry above their first column
       const int ibeg = g.tri ? ((local * 32) / kXChunk) * kXChunk : 0;
       const int jw = local * 32 + warp * 4;  // this warp's first column
       for (int i0 = ibeg; i0 < g.m; i0 += kXChunk) {
         const int ni = min(kXChunk, g.m - i0);
         __syncthreads();
-        for (int e = tid; e < ni * kRhsGroup; e += 256) {
-          const int ii = e / kRhsGroup, cc = e % kRhsGroup;
+        for (int e = tid; e < ni * RG; e += 256) {
+          const int ii = e / RG, cc = e % RG;
           xs[ii][cc] = (cc < nc) ? u_in[g.in_idx[i0 + ii] + (long long)(c0 + cc) * ldu] : 0.0;
         }
         __syncthreads();
@@ -3255,14 +3320,14 @@ __device__ __forceinline__ void gemv_tile(const GemvDesc& g0, int local,
 #pragma unroll
           for (int q = 0; q < 4; ++q)
 #pragma unroll
-            for (int cc = 0; cc < kRhsGroup; ++cc) acc[q][cc] = fma(mv[q], xs[ii][cc], acc[q][cc]);
+            for (int cc = 0; cc < RG; ++cc) acc[q][cc] = fma(mv[q], xs[ii][cc], acc[q][cc]);
         }
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int j = jw + q;
 #pragma unroll
-        for (int cc = 0; cc < kRhsGroup; ++cc) {
+        for (int cc = 0; cc < RG; ++cc) {
           const double y = warp_sum(acc[q][cc]);
           if (lane == 0 && j < g.n && cc < nc) gemv_emit(g, j, c0 + cc, y, u_out, ldu, contrib_ld);
         }
@@ -3431,14 +3496,14 @@ __global__ void __launch_bounds__(256, 3) k_gemv_small(const GemvFastSeg* __rest
 // 32-column tiles), located from the unit table (descriptor, tile) rather than
 // a search over tile offsets. Two CTAs per SM: each warp keeps eight column
 // loads in flight, which covers the memory latency at this occupancy.
-__global__ void __launch_bounds__(256, 2) k_gemv_tiles(const GemvFastSeg* __restrict__ segs,
-                                                   const int* __restrict__ seg_off, int nseg,
-                                                   const double* __restrict__ u_in,
-                                                   double* __restrict__ u_out, int nrhs,
-                                                   long long ldu, long long contrib_ld) {
+template <int RG>
+__global__ void __launch_bounds__(256, RG == 1 ? 3 : 2)
+    k_gemv_tiles(const GemvFastSeg* __restrict__ segs, const int* __restrict__ seg_off, int nseg,
+                 const double* __restrict__ u_in, double* __restrict__ u_out, int nrhs,
+                 long long ldu, long long contrib_ld) {
   const int si = find_desc(seg_off, nseg, blockIdx.x);
   const int2 t = segs[si].tab[blockIdx.x - seg_off[si]];
-  gemv_tile(segs[si].desc[t.x], t.y, u_in, u_out, nrhs, ldu, contrib_ld);
+  gemv_tile<RG>(segs[si].desc[t.x], t.y, u_in, u_out, nrhs, ldu, contrib_ld);
 }
 
 int gemv_tile_count(int m, int n, int trans) {
@@ -3454,9 +3519,12 @@ void launch_gemv_fast(const GemvFastSeg* d_segs, const int* d_seg_off, int nseg,
   if (layout == kGemvSmall)
     k_gemv_small<<<(units + 7) / 8, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
                                                  contrib_ld);
-  else
-    k_gemv_tiles<<<units, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
-                                       contrib_ld);
+  else if (nrhs == 1)
+    k_gemv_tiles<1><<<units, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs, ldu,
+                                          contrib_ld);
+  else  // several vectors, or per-descriptor vectors (serving: nrhs 0)
+    k_gemv_tiles<kRhsGroup><<<units, 256, 0, s>>>(d_segs, d_seg_off, nseg, u_in, u_out, nrhs,
+                                                  ldu, contrib_ld);
 }
 
 
