@@ -200,10 +200,14 @@ class HostPool {
       for (int i = i0; i < i1; ++i) (*j.f)(i);
     }
   }
+  // the open job with the fewest workers: concurrent loops (a partition thread's
+  // long one, the factorization thread's short ones) share the pool instead of
+  // the first one taking every worker
   Job* open_job() {
+    Job* best = nullptr;
     for (Job* j : jobs_)
-      if (j->next.load() < j->n) return j;
-    return nullptr;
+      if (j->next.load() < j->n && (!best || j->holders < best->holders)) best = j;
+    return best;
   }
   void loop() {
     std::unique_lock<std::mutex> lk(mu_);
