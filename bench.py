@@ -590,10 +590,17 @@ def run_ours(args, rank: int, world: int):
                 "pcg_relres": rel[-1], "clocks": clk, "kst": kst}
 
     runs = {}
+    fp64_chol = None
     precs = {"fp64": [hb.PRECISION_FP64], "mixed": [hb.PRECISION_MIXED],
              "both": [hb.PRECISION_FP64, hb.PRECISION_MIXED]}[args.precision]
     for prec in precs:
         runs[prec] = measure(prec)
+        if prec == hb.PRECISION_FP64 and not args.no_fp64_cholesky:
+            # FP64 with the Cholesky elimination of the symmetric interiors (the
+            # FP64 default keeps the reference's Gauss-Jordan inverse)
+            f.set_option(hb.OPT_ELIMINATION, hb.ELIM_CHOLESKY)
+            fp64_chol = measure(prec)
+            f.set_option(hb.OPT_ELIMINATION, hb.ELIM_AUTO)
     head_prec = precs[-1]
     head = runs[head_prec]
     ms_total = head["ms_step"] * args.steps
@@ -706,6 +713,19 @@ def run_ours(args, rank: int, world: int):
                 "host": rec_ref.get("host"), "source": os.path.relpath(REF_RECORD, ROOT)}
             for nm in ("fp64", "mixed"):
                 same["n64"][f"{nm}_vs_reference"] = same["n64"][nm]["steps_per_s"] * t64
+    # n = 128 (this workload): the reference's capped run, levels reached so far;
+    # their elapsed time is a lower bound on its factor time
+    r128 = rec_ref.get("n128") if rec_ref else None
+    if r128 and r128.get("per_level") and n == 128:
+        t128 = float(r128["per_level"][-1]["elapsed_s"])
+        same["n128"] = {
+            "reference_1core_lower_bound_s": t128,
+            "levels_completed": len(r128["per_level"]),
+            "status": r128.get("status"),
+            "source": os.path.relpath(REF_RECORD, ROOT)}
+        for nm, prec in (("fp64", hb.PRECISION_FP64), ("mixed", hb.PRECISION_MIXED)):
+            if prec in runs:
+                same["n128"][f"{nm}_vs_reference_at_least"] = t128 / (runs[prec]["ms_step"] * 1e-3)
 
     value = job_value(world, ms_step)
     line = {
@@ -758,6 +778,15 @@ def run_ours(args, rank: int, world: int):
                           "factor_s": r["factor_s"], "solve_ms": r["solve_ms"],
                           "solves_per_s": 1e3 / r["solve_ms"], "pcg_iters": r["pcg_iters"],
                           "pcg_relres": r["pcg_relres"]}
+    if fp64_chol is not None:
+        r = fp64_chol
+        line["fp64_cholesky"] = {
+            "steps_per_s": 1e3 / r["ms_step"], "ms_per_step": r["ms_step"],
+            "factor_s": r["factor_s"], "solve_ms": r["solve_ms"], "pcg_iters": r["pcg_iters"],
+            "pcg_relres": r["pcg_relres"],
+            "arithmetic": ("FP64 throughout, Cholesky elimination of the symmetric interiors "
+                           "(HIF_OPT_ELIMINATION = HIF_ELIM_CHOLESKY); pinned to the reference's "
+                           "F^-1 u at n = 64 by tests/test_gpu_cholesky.py")}
     if len(runs) == 2 and not args.no_level_error:
         # mixed against FP64 per level on the headline operator (the FP64 factor is
         # pinned to the reference's at n = 64 by the parity tests)
@@ -816,6 +845,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="fixed tile rules")
     ap.add_argument("--no-same-size", action="store_true",
                     help="skip the GPU rates at n = 32 and 64 (same-size reference comparison)")
+    ap.add_argument("--no-fp64-cholesky", action="store_true",
+                    help="skip the FP64 run with the Cholesky elimination")
     ap.add_argument("--no-level-error", action="store_true",
                     help="skip the per-level mixed-vs-FP64 error")
     ap.add_argument("--ref-n", type=int, default=REF_N,

@@ -785,9 +785,8 @@ void gemm_batch_int8(const std::vector<GemmDesc>& gin, BufList& tmp, cudaStream_
 // (0) or from `x` int8 slices. The Gauss-Jordan updates of A22^{-1} are rank-128
 // products, bound by the traffic of their target rather than by arithmetic, and
 // stay FP64.
-// chol: in the Cholesky elimination, the trailing updates of the pivot-block
-// factorization and the products forming L^{-1} in FP64 (0) or from `chol`
-// int8 slices.
+// chol: in the Cholesky elimination, the products forming L^{-1} (long k) in
+// FP64 (0) or from `chol` int8 slices; the pivot-block updates stay FP64.
 struct ElimArith {
   int schur = -1;
   int x = 0;
@@ -926,8 +925,8 @@ void chol_blocks(const std::vector<SweepDesc>& descs, BufList& tmp, cudaStream_t
       timed(HIF_KCLASS_COPY, 0, 0, [&] { launch_copy(dq, doq, (int)cq.size(), ocq.back(), stream); });
     }
     gemm_batch(gp, step, stream, HIF_KCLASS_SWEEP_PANEL, timed);
-    if (ar.chol > 0) gemm_batch_int8(gu, step, stream, timed, ar.chol, d_status);
-    else gemm_batch(gu, step, stream, HIF_KCLASS_GEMM, timed, 128);
+    // rank-128 updates: FP64 (from int8 slices they are bound by their C traffic)
+    gemm_batch(gu, step, stream, HIF_KCLASS_GEMM, timed, 128);
     {
       CopyDesc* dc = step.add(upload(cdg, stream));
       int* doc = step.add(upload(ocd, stream));
@@ -2664,7 +2663,7 @@ class Engine {
   static constexpr double kGramMinEps = 1e-7;
   // mixed precision: faces wider than this (and taller than wide) take the
   // Gram-matrix ID; narrower ones the one-CTA pivoted QR (HIF_OPT_GRAM_MIN_N)
-  int gram_min_n = 64;
+  int gram_min_n = 32;
   int gram_slices = 0;  // HIF_OPT_GRAM_SLICES
   void id_cholesky(const std::vector<IdDesc>& v, BufList& tmp) {
     Arena& work = *cur_work;
@@ -3105,7 +3104,7 @@ class Engine {
   bool autotune = false;
   // HIF_PRECISION_MIXED: int8 slices of the Schur products (0: split TF32) and
   // of the X products (0: FP64)
-  int schur_slices = 5, x_slices = 7, y_slices = 6, chol_slices = 0;
+  int schur_slices = 5, x_slices = 7, y_slices = 6, chol_slices = 7;
   // host index lists of the phase being built, kept across phases and
   // factorizations
   std::vector<int> h_red_all, h_skel_all, h_rows_all;

@@ -206,13 +206,13 @@ enum hif_option {
   HIF_OPT_Y_SLICES = 11,      /* MIXED, Cholesky elimination: int8 slices (2..8) of
                                  Y = L^{-1} A21 (default 6); 0: FP64 */
   HIF_OPT_GRAM_MIN_N = 12,    /* MIXED: faces with more columns than this (and more rows
-                                 than columns) take the Gram-matrix ID (default 64) */
+                                 than columns) take the Gram-matrix ID (default 32) */
   HIF_OPT_GRAM_SLICES = 13,   /* MIXED: the Gram matrices M^T M of that ID from int8 slices
                                  (2..8); 0 (default): FP64 products */
   HIF_OPT_CHOL_SLICES = 14    /* MIXED, Cholesky elimination: int8 slices (2..8) of the
-                                 trailing updates of the pivot-block factorization and of
-                                 the products forming L^{-1}; 0 (default): FP64 (the
-                                 rank-128 updates have too short a k for the slices) */
+                                 products forming L^{-1} (default 7); 0: FP64. The
+                                 rank-128 updates of the pivot-block factorization stay
+                                 FP64 (too short a k for the slices) */
 };
 /* Arithmetic of the factorization. MIXED: the long-K products of the eliminations
  * (S = A11 - A12 X, and X or Y) are FP64 products formed from exact int8 slice

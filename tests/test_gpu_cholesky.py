@@ -165,9 +165,9 @@ def test_mixed_cholesky_close_to_fp64(N, partition):
 
 
 def test_mixed_cholesky_int8_factor_products():
-    """HIF_OPT_CHOL_SLICES: the trailing updates of the pivot-block factorization
-    and the products forming L^{-1} from 7 int8 slices against FP64 products (0,
-    the default), at n = 64 where the top blocks span many 128-pivot blocks: the
+    """HIF_OPT_CHOL_SLICES: the products forming L^{-1} from 7 int8 slices (the
+    default) against FP64 products (0), at n = 64 where the top blocks span many
+    128-pivot blocks: the
     stored factors stay consistent (L lower, L L^{-1} = I to 1e-10), the inverse
     applies agree to the mixed arithmetic's own level and PCG needs no more
     iterations."""
