@@ -1552,6 +1552,7 @@ class Engine {
     }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     release_factor();
+    join_reaper();
     release_workspace();
     sync_quiet();
     arena_factor.release();
@@ -1775,9 +1776,21 @@ class Engine {
     dfree(d_contrib, stream);
     d_contrib = nullptr;
     contrib_cap = 0;
-    steps.clear();
+    // the released factor's host structures (some 10^5 small vectors at
+    // n = 128, ~25 ms to free) are destroyed on a thread of their own, off the
+    // next factorization's critical path; they hold no device resources
+    join_reaper();
+    if (!steps.empty()) {
+      auto* old = new std::vector<StepData>(std::move(steps));
+      steps.clear();
+      reaper_ = std::thread([old] { delete old; });
+    }
     arena_factor.reset();
     factored = false;
+  }
+  std::thread reaper_;
+  void join_reaper() {
+    if (reaper_.joinable()) reaper_.join();
   }
 
   int levels_for() const {
@@ -1806,10 +1819,12 @@ class Engine {
   // ---- Initialize (src/Factor.cpp:6-39) -----------------------------------
   void initialize() {
     release_factor();
+    // every DOF with all three indices in [1, NC) remains: one run of NC - 1
+    // bytes per (j, k) row
     rem.assign(n3, 0);
     for (int k = 1; k < NC; ++k)
       for (int j = 1; j < NC; ++j)
-        for (int i = 1; i < NC; ++i) rem[i + (long long)NC * j + (long long)NC * NC * k] = 1;
+        std::memset(rem.data() + 1 + (long long)NC * j + (long long)NC * NC * k, 1, NC - 1);
     L = levels_for();
     initialized = true;
   }
