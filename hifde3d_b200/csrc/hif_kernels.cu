@@ -1724,7 +1724,7 @@ constexpr int kCdP = 32;             // panel width
 constexpr int kCdXs = kCdP + 1;      // padded stride of the diagonal inverses
 constexpr int kCdThreads = 256;
 constexpr size_t kCholDiagSmem =
-    (size_t)(kSweepNB * kSweepNB + 4 * kCdP * kCdXs + 3 * kCdP * kCdXs + kSweepNB) *
+    (size_t)(kSweepNB * kSweepNB + 4 * kCdP * kCdXs + 3 * kCdP * kCdXs + kSweepNB + 2 * kCdP) *
     sizeof(double);
 static_assert(kSweepNB == 4 * kCdP && kCdThreads == 256, "16 x 16 thread grid over 32-row panels");
 
@@ -1741,6 +1741,7 @@ __global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __res
   double* Xd = S + T * T;              // 4 diagonal inverses, [p][c][i] = X_pp(i, c)
   double* Tb = Xd + 4 * kCdP * kCdXs;  // 3 products of the inverse, [jb][c][k]
   double* rd = Tb + 3 * kCdP * kCdXs;  // 1 / L(i, i)
+  double* colk = rd + T;               // 2 x 32: the current pivot column, double-buffered
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tx = tid & 15, ty = tid >> 4;
   // the lower triangle only (the only one read), in whole columns; 16 loads
@@ -1781,11 +1782,17 @@ __global__ void __launch_bounds__(kCdThreads) k_chol_diag(const SweepDesc* __res
           a[k] = q * rk;
           rmine = rk;
         }
-        // D(lane, j) -= L(lane, k) L(j, k), k < j <= lane
+        // D(lane, j) -= L(lane, k) L(j, k), k < j <= lane; the column L(:, k) is
+        // passed through shared memory (one store per lane, broadcast loads)
+        // rather than by a pair of shuffles per entry; the buffer alternates
+        // with k, so one warp barrier per pivot suffices
+        double* ck = colk + (k & 1) * kCdP;
+        ck[lane] = a[k];
+        __syncwarp();
 #pragma unroll
         for (int j = 1; j < kCdP; ++j) {
           if (j > k) {  // fixed trip count: a[] stays in registers
-            const double ljk = __shfl_sync(0xffffffffu, a[k], j);
+            const double ljk = ck[j];
             if (lane >= j) a[j] = fma(-a[k], ljk, a[j]);
           }
         }
