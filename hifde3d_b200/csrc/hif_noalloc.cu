@@ -14,7 +14,8 @@
 //     on the GPU (different streams, or host threads sharing a device) race on
 //     it and must be serialised by the caller;
 //   * the first call on a device looks the array's address up once, with that
-//     device current. The address is kept for the life of the process, so the
+//     device current; that first call should come before any stream capture
+//     begins on the device. The address is kept for the life of the process, so the
 //     library must not be used on a device after cudaDeviceReset has torn its
 //     context down;
 //   * every call ends by copying the pivot status word to the host and

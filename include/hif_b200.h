@@ -139,7 +139,8 @@ int hif_schur_device(const double* dB, int n, int r, double* dA22inv, double* dX
  * so it returns only after its kernels have finished. Every call on a device shares the
  * scratch array: calls whose kernels may overlap on the GPU race and must be
  * serialised by the caller. The first call on a device looks up the array's device
- * address with that device current. The address is kept for the process's life: do
+ * address with that device current; make that first call before any stream capture
+ * begins on the device. The address is kept for the process's life: do
  * not use the library on a device after cudaDeviceReset. n = 0 is a no-op returning
  * HIF_OK. */
 int hif_schur_device_noalloc(const double* dB, int n, int r, double* dA22inv, double* dX,
