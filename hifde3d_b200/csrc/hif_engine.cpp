@@ -1922,6 +1922,14 @@ class Engine {
   }
 
   // ---- Schur phase (LevelFactorSchur, src/Factor.cpp:184-213) ------------
+  struct Cell0Layout {
+    bool cached = false;
+    std::vector<BlockInfo> blocks;
+    std::vector<int> red_all, skel_all, rows_all;
+    std::vector<long long> o_B, o_rows, o_a22, o_inv, o_x, o_red, o_skel;
+    long long bsz = 0, asz = 0;
+  };
+  Cell0Layout cell0;
   void schur_phase(int level, Sources& in, Sources& out) {
     double th = wall();
     const int cpd = cells_per_dir(level);
@@ -1933,23 +1941,40 @@ class Engine {
     st.cpd = cpd;
     Partitioner part{N, P, NC, rem.data()};
     const int ncell = cpd * cpd * cpd;
-    if (take_cell_partition(level, st.blocks)) {
+    // level 0's cells see the initial DOF mask, so their blocks, offsets and
+    // index lists are the grid's alone: kept from the handle's first
+    // factorization (cell0) and reused by the later ones
+    const bool cell0_hit = level == 0 && cell0.cached;
+    if (cell0_hit) {
+      st.blocks.resize(ncell);
+      parallel_for(ncell, [&](int idx) { st.blocks[idx] = cell0.blocks[idx]; });
+    } else if (take_cell_partition(level, st.blocks)) {
       // built before the last skeletonization's DOFs were removed: drop them
-      // (the scan order and the classification of the rest do not change)
+      // (the scan order and the classification of the rest do not change).
+      // Every position is either redundant or skeleton and red_pos ascends,
+      // so one walk compacts the three lists in place (each write index
+      // trails its read index).
       parallel_for(ncell, [&](int idx) {
         BlockInfo& b = st.blocks[idx];
-        std::vector<char> cls(b.global.size(), 0);
-        for (int q : b.red_pos) cls[q] = 1;
-        std::vector<int> g, r, k;
-        g.reserve(b.global.size());
-        for (size_t t = 0; t < b.global.size(); ++t) {
-          if (!rem[b.global[t]]) continue;
-          (cls[t] ? r : k).push_back((int)g.size());
-          g.push_back(b.global[t]);
+        int* gl = b.global.data();
+        int* rp = b.red_pos.data();
+        int* sp = b.skel_pos.data();
+        const size_t ng_in = b.global.size(), nr_in = b.red_pos.size();
+        size_t ri = 0, nr = 0, ns = 0, ng = 0;
+        for (size_t t = 0; t < ng_in; ++t) {
+          const bool is_red = ri < nr_in && rp[ri] == (int)t;
+          ri += is_red;
+          const int gid = gl[t];
+          if (!rem[gid]) continue;
+          if (is_red)
+            rp[nr++] = (int)ng;
+          else
+            sp[ns++] = (int)ng;
+          gl[ng++] = gid;
         }
-        b.global.swap(g);
-        b.red_pos.swap(r);
-        b.skel_pos.swap(k);
+        b.global.resize(ng);
+        b.red_pos.resize(nr);
+        b.skel_pos.resize(ns);
       });
     } else {
       st.blocks.resize(ncell);
@@ -1963,53 +1988,81 @@ class Engine {
     mark("schur cell partition", level);
     // sizes and device layout (the flat lists reuse the handle's host buffers:
     // their pages are touched once, not at every factorization)
-    std::vector<int>& red_all = h_red_all;
-    std::vector<int>& skel_all = h_skel_all;
+    std::vector<int>& red_all = cell0_hit ? cell0.red_all : h_red_all;
+    std::vector<int>& skel_all = cell0_hit ? cell0.skel_all : h_skel_all;
+    std::vector<int>& rows_all = cell0_hit ? cell0.rows_all : h_rows_all;
     long long bsz = 0, asz = 0;
     std::vector<long long> o_B(ncell);
-    st.o_a22.resize(ncell);
-    st.o_inv.resize(ncell);
-    st.o_x.resize(ncell);
-    st.o_w.assign(ncell, 0);
-    st.o_red.resize(ncell);
-    st.o_skel.resize(ncell);
-    std::vector<int>& rows_all = h_rows_all;
     std::vector<long long> o_rows(ncell);
-    long long nred = 0, nskel = 0;
-    for (int b = 0; b < ncell; ++b) {
-      const BlockInfo& bi = st.blocks[b];
-      const long long n = bi.global.size(), r = bi.r(), s = bi.s();
-      o_B[b] = bsz;
-      bsz += n * n;
-      st.o_a22[b] = asz;
-      asz += r * r;
-      st.o_inv[b] = asz;
-      asz += r * r;
-      st.o_x[b] = asz;
-      asz += r * s;
-      st.o_red[b] = nred;
-      st.o_skel[b] = nskel;
-      o_rows[b] = nred + nskel;
-      nred += r;
-      nskel += s;
+    st.o_w.assign(ncell, 0);
+    if (cell0_hit) {
+      bsz = cell0.bsz;
+      asz = cell0.asz;
+      o_B = cell0.o_B;
+      o_rows = cell0.o_rows;
+      st.o_a22 = cell0.o_a22;
+      st.o_inv = cell0.o_inv;
+      st.o_x = cell0.o_x;
+      st.o_red = cell0.o_red;
+      st.o_skel = cell0.o_skel;
+    } else {
+      st.o_a22.resize(ncell);
+      st.o_inv.resize(ncell);
+      st.o_x.resize(ncell);
+      st.o_red.resize(ncell);
+      st.o_skel.resize(ncell);
+      long long nred = 0, nskel = 0;
+      for (int b = 0; b < ncell; ++b) {
+        const BlockInfo& bi = st.blocks[b];
+        const long long n = bi.global.size(), r = bi.r(), s = bi.s();
+        o_B[b] = bsz;
+        bsz += n * n;
+        st.o_a22[b] = asz;
+        asz += r * r;
+        st.o_inv[b] = asz;
+        asz += r * r;
+        st.o_x[b] = asz;
+        asz += r * s;
+        st.o_red[b] = nred;
+        st.o_skel[b] = nskel;
+        o_rows[b] = nred + nskel;
+        nred += r;
+        nskel += s;
+      }
+      red_all.resize(nred);
+      skel_all.resize(nskel);
+      rows_all.resize(nred + nskel);
+      parallel_for(ncell, [&](int b) {
+        const BlockInfo& bi = st.blocks[b];
+        long long q = o_rows[b];
+        for (size_t t = 0; t < bi.red_pos.size(); ++t) {
+          const int g = bi.global[bi.red_pos[t]];
+          red_all[st.o_red[b] + t] = g;
+          rows_all[q++] = g;
+        }
+        for (size_t t = 0; t < bi.skel_pos.size(); ++t) {
+          const int g = bi.global[bi.skel_pos[t]];
+          skel_all[st.o_skel[b] + t] = g;
+          rows_all[q++] = g;
+        }
+      });
+      if (level == 0) {
+        cell0.blocks = st.blocks;
+        cell0.red_all = red_all;
+        cell0.skel_all = skel_all;
+        cell0.rows_all = rows_all;
+        cell0.o_B = o_B;
+        cell0.o_rows = o_rows;
+        cell0.o_a22 = st.o_a22;
+        cell0.o_inv = st.o_inv;
+        cell0.o_x = st.o_x;
+        cell0.o_red = st.o_red;
+        cell0.o_skel = st.o_skel;
+        cell0.bsz = bsz;
+        cell0.asz = asz;
+        cell0.cached = true;
+      }
     }
-    red_all.resize(nred);
-    skel_all.resize(nskel);
-    rows_all.resize(nred + nskel);
-    parallel_for(ncell, [&](int b) {
-      const BlockInfo& bi = st.blocks[b];
-      long long q = o_rows[b];
-      for (size_t t = 0; t < bi.red_pos.size(); ++t) {
-        const int g = bi.global[bi.red_pos[t]];
-        red_all[st.o_red[b] + t] = g;
-        rows_all[q++] = g;
-      }
-      for (size_t t = 0; t < bi.skel_pos.size(); ++t) {
-        const int g = bi.global[bi.skel_pos[t]];
-        skel_all[st.o_skel[b] + t] = g;
-        rows_all[q++] = g;
-      }
-    });
     st.n_red = red_all.size();
     st.n_skel = skel_all.size();
     if (level > 0) start_face_partition(level, red_all);
@@ -2259,11 +2312,19 @@ class Engine {
   // coordinates interior to the cell width, src/Factor.cpp:314-320), which is
   // exactly what level 0's cell phase eliminates. It starts at once, so the
   // host thread builds it while the cell phase is assembled and eliminated.
+  // Being the grid's alone, it is built once per handle: the first
+  // factorization keeps it (face0_*), later ones copy the blocks from there and
+  // read the row lists in place, so no partition thread competes with level 0's
+  // host work for the worker pool.
+  std::vector<BlockInfo> face0_blocks;
+  std::vector<std::vector<int>> face0_rows;
+  bool face0_cached = false;
   void start_face_partition0() {
     join_face_partition();
     if (L <= 1) return;
     face_pre = FacePartition{};
     face_pre.level = 0;
+    if (face0_cached) return;
     face_pre.mask = rem;
     face_thread = std::thread([this] {
       try {
@@ -2284,14 +2345,28 @@ class Engine {
       }
     });
   }
+  // rows: set to the row lists to read (rows_l, or level 0's kept lists).
   bool take_face_partition(int level, std::vector<BlockInfo>& blocks,
-                           std::vector<std::vector<int>>& rows_l) {
+                           std::vector<std::vector<int>>& rows_l,
+                           const std::vector<std::vector<int>>** rows) {
     join_face_partition();
     if (face_pre.level != level) return false;
     face_pre.level = -1;
     if (face_pre.err) std::rethrow_exception(face_pre.err);
+    if (level == 0) {
+      if (!face0_cached) {
+        face0_blocks = std::move(face_pre.blocks);
+        face0_rows = std::move(face_pre.rows_l);
+        face0_cached = true;
+      }
+      blocks.resize(face0_blocks.size());
+      parallel_for((int)face0_blocks.size(), [&](int f) { blocks[f] = face0_blocks[f]; });
+      *rows = &face0_rows;
+      return true;
+    }
     blocks = std::move(face_pre.blocks);
     rows_l = std::move(face_pre.rows_l);
+    *rows = &rows_l;
     return true;
   }
 
@@ -2303,10 +2378,12 @@ class Engine {
     st.skel = true;
     st.chol = use_chol;
     st.cpd = cpd;
-    std::vector<std::vector<int>> rows_l;
+    std::vector<std::vector<int>> rows_own;
+    const std::vector<std::vector<int>>* rows_p = &rows_own;
     std::vector<BlockInfo>& blocks = st.blocks;
-    if (!take_face_partition(level, blocks, rows_l))
-      partition_faces(level, rem.data(), blocks, rows_l);
+    if (!take_face_partition(level, blocks, rows_own, &rows_p))
+      partition_faces(level, rem.data(), blocks, rows_own);
+    const std::vector<std::vector<int>>& rows_l = *rows_p;
     start_cell_partition(level + 1);
     mark("skel face partition", level);
     const int nf = (int)blocks.size();
@@ -2500,11 +2577,15 @@ class Engine {
         throw Error{HIF_ERR_CUDA, std::string("grouped ID launch: ") + cudaGetErrorString(le)};
     }
     HIF_CK(cudaGetLastError());
-    std::vector<int> h_jp(isz + 1), h_keep(isz + 1);
-    std::vector<double> h_rd(isz + 1);
-    HIF_CK(cudaMemcpyAsync(h_jp.data(), d_jp, isz * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    HIF_CK(cudaMemcpyAsync(h_keep.data(), d_keep, isz * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    HIF_CK(cudaMemcpyAsync(h_rd.data(), d_rd, isz * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    // pivots, kept flags and |R_ii| read back into pinned staging: the copies
+    // run at full link speed right after the IDs, and no host array is
+    // zero-filled first
+    int* h_jp = static_cast<int*>(stage.get((isz + 1) * sizeof(int)));
+    int* h_keep = static_cast<int*>(stage.get((isz + 1) * sizeof(int)));
+    double* h_rd = static_cast<double*>(stage.get((isz + 1) * sizeof(double)));
+    HIF_CK(cudaMemcpyAsync(h_jp, d_jp, isz * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    HIF_CK(cudaMemcpyAsync(h_keep, d_keep, isz * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    HIF_CK(cudaMemcpyAsync(h_rd, d_rd, isz * sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();
     t_id += wall() - ti0;
     mark("skel pivoted QR", level);
@@ -2525,8 +2606,8 @@ class Engine {
     parallel_for(nf, [&](int f) {
       BlockInfo& b = blocks[f];
       const int n = b.global.size();
-      b.jpvt.assign(h_jp.begin() + o_i[f], h_jp.begin() + o_i[f] + n);
-      b.rdiag.assign(h_rd.begin() + o_i[f], h_rd.begin() + o_i[f] + n);
+      b.jpvt.assign(h_jp + o_i[f], h_jp + o_i[f] + n);
+      b.rdiag.assign(h_rd + o_i[f], h_rd + o_i[f] + n);
       int k = 0;
       for (int i = 0; i < n; ++i) k += h_keep[o_i[f] + i] != 0;
       b.skel_pos.reserve(k);
