@@ -1559,6 +1559,10 @@ class Engine {
     arena_work[0].release();
     arena_work[1].release();
     arena_desc.release();
+    dfree(cell0.d_red, stream);
+    dfree(cell0.d_skel, stream);
+    dfree(cell0.d_rows, stream);
+    dfree(face0_didx, stream);
     dfree(d_band, stream);
     dfree(d_status, stream);
     dfree(d_dof_src, stream);
@@ -1928,7 +1932,19 @@ class Engine {
     std::vector<int> red_all, skel_all, rows_all;
     std::vector<long long> o_B, o_rows, o_a22, o_inv, o_x, o_red, o_skel;
     long long bsz = 0, asz = 0;
+    // device copies of red_all / skel_all / rows_all, made by the second
+    // factorization (the first one's uploads live in its arenas); read-only
+    int* d_red = nullptr;
+    int* d_skel = nullptr;
+    int* d_rows = nullptr;
   };
+  // A device copy of `count` ints at src that lives with the handle.
+  int* keep_on_device(const int* src, size_t count) {
+    int* d = dalloc<int>(std::max<size_t>(count, 1), stream);
+    if (count)
+      HIF_CK(cudaMemcpyAsync(d, src, count * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    return d;
+  }
   Cell0Layout cell0;
   void schur_phase(int level, Sources& in, Sources& out) {
     double th = wall();
@@ -2077,10 +2093,22 @@ class Engine {
     t_scratch = &work;
     double* dB = work.alloc<double>(bsz);
     st.arena = arena_factor.alloc<double>(asz);
-    st.d_red = arena_factor.upload(red_all, stream);
-    st.d_skel = arena_factor.upload(skel_all, stream);
     BufList tmp;
-    int* drows = work.upload(rows_all, stream);
+    int* drows;
+    if (cell0_hit && cell0.d_rows) {
+      st.d_red = cell0.d_red;
+      st.d_skel = cell0.d_skel;
+      drows = cell0.d_rows;
+    } else {
+      st.d_red = arena_factor.upload(red_all, stream);
+      st.d_skel = arena_factor.upload(skel_all, stream);
+      drows = work.upload(rows_all, stream);
+      if (cell0_hit) {
+        cell0.d_red = keep_on_device(st.d_red, red_all.size());
+        cell0.d_skel = keep_on_device(st.d_skel, skel_all.size());
+        cell0.d_rows = keep_on_device(drows, rows_all.size());
+      }
+    }
 
     // gather every cell block
     double tg0 = wall();
@@ -2319,6 +2347,7 @@ class Engine {
   std::vector<BlockInfo> face0_blocks;
   std::vector<std::vector<int>> face0_rows;
   bool face0_cached = false;
+  int* face0_didx = nullptr;  // its row and column lists on the device (read-only)
   void start_face_partition0() {
     join_face_partition();
     if (L <= 1) return;
@@ -2407,12 +2436,19 @@ class Engine {
     }
     // row and column lists of every face, filled in parallel
     // written straight into pinned staging memory: no host array to zero-fill
-    // and page in, and no second copy before the upload
-    int* idx_all = static_cast<int*>(stage.get(std::max<long long>(xsz, 1) * sizeof(int)));
-    parallel_for(nf, [&](int f) {
-      std::copy(rows_l[f].begin(), rows_l[f].end(), idx_all + o_rows[f]);
-      std::copy(blocks[f].global.begin(), blocks[f].global.end(), idx_all + o_cols[f]);
-    });
+    // and page in, and no second copy before the upload. Level 0's are the
+    // grid's alone: from a handle's second factorization on, the device copy
+    // it keeps is read instead
+    const bool face0_hit = rows_p == &face0_rows;
+    const bool idx_kept = face0_hit && face0_didx != nullptr;
+    int* idx_all = nullptr;
+    if (!idx_kept) {
+      idx_all = static_cast<int*>(stage.get(std::max<long long>(xsz, 1) * sizeof(int)));
+      parallel_for(nf, [&](int f) {
+        std::copy(rows_l[f].begin(), rows_l[f].end(), idx_all + o_rows[f]);
+        std::copy(blocks[f].global.begin(), blocks[f].global.end(), idx_all + o_cols[f]);
+      });
+    }
     mark("skel index lists", level);
     t_host += wall() - th;
 
@@ -2423,8 +2459,15 @@ class Engine {
     t_scratch = &work;
     double* dM = work.alloc<double>(msz);
     double* dWs = work.alloc<double>(wsz);
-    int* didx = tmp.add(desc_alloc<int>(xsz, stream));
-    if (xsz) HIF_CK(cudaMemcpyAsync(didx, idx_all, xsz * sizeof(int), cudaMemcpyHostToDevice, stream));
+    int* didx;
+    if (idx_kept) {
+      didx = face0_didx;
+    } else {
+      didx = tmp.add(desc_alloc<int>(xsz, stream));
+      if (xsz)
+        HIF_CK(cudaMemcpyAsync(didx, idx_all, xsz * sizeof(int), cudaMemcpyHostToDevice, stream));
+      if (face0_hit) face0_didx = keep_on_device(didx, xsz);
+    }
     int* d_jp = tmp.add(dalloc<int>(isz + 1, stream));
     int* d_keep = tmp.add(dalloc<int>(isz + 1, stream));
     int* d_rank = tmp.add(dalloc<int>(nf + 1, stream));
