@@ -2353,7 +2353,20 @@ class Engine {
     if (L <= 1) return;
     face_pre = FacePartition{};
     face_pre.level = 0;
-    if (face0_cached) return;
+    if (face0_cached) {
+      // the factor keeps its own copy of the blocks (pivots and index sets are
+      // added to them): made here, while level 0's cell phase runs
+      face_thread = std::thread([this] {
+        try {
+          face_pre.blocks.resize(face0_blocks.size());
+          parallel_for((int)face0_blocks.size(),
+                       [&](int f) { face_pre.blocks[f] = face0_blocks[f]; });
+        } catch (...) {
+          face_pre.err = std::current_exception();
+        }
+      });
+      return;
+    }
     face_pre.mask = rem;
     face_thread = std::thread([this] {
       try {
@@ -2383,13 +2396,15 @@ class Engine {
     face_pre.level = -1;
     if (face_pre.err) std::rethrow_exception(face_pre.err);
     if (level == 0) {
-      if (!face0_cached) {
+      if (face0_cached) {
+        blocks = std::move(face_pre.blocks);
+      } else {
         face0_blocks = std::move(face_pre.blocks);
         face0_rows = std::move(face_pre.rows_l);
         face0_cached = true;
+        blocks.resize(face0_blocks.size());
+        parallel_for((int)face0_blocks.size(), [&](int f) { blocks[f] = face0_blocks[f]; });
       }
-      blocks.resize(face0_blocks.size());
-      parallel_for((int)face0_blocks.size(), [&](int f) { blocks[f] = face0_blocks[f]; });
       *rows = &face0_rows;
       return true;
     }
