@@ -2341,8 +2341,9 @@ class Engine {
   // exactly what level 0's cell phase eliminates. It starts at once, so the
   // host thread builds it while the cell phase is assembled and eliminated.
   // Being the grid's alone, it is built once per handle: the first
-  // factorization keeps it (face0_*), later ones copy the blocks from there and
-  // read the row lists in place, so no partition thread competes with level 0's
+  // factorization keeps it (face0_*); later ones copy its blocks on a host
+  // thread while level 0's cell phase runs and read its row lists in place, so
+  // the partition is not rebuilt and no partition loop competes with level 0's
   // host work for the worker pool.
   std::vector<BlockInfo> face0_blocks;
   std::vector<std::vector<int>> face0_rows;
