@@ -613,10 +613,13 @@ def run_ours(args, rank: int, world: int):
     # end to end through the public API with host buffers
     e2e_s, it_e2e, rr_e2e = float("nan"), None, None
     if not args.no_e2e:
+        # host buffers in the reference's layout (NumTns: i fastest), which the
+        # API takes without a host-side transpose
+        hx = [np.asfortranarray(x) for x in (ax, ay, az, V)]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            hb.SetupStencilFaces(f, N, h, ax, ay, az, V)
+            hb.SetupStencilFaces(f, N, h, *hx)
             f.Factor()
             _xh, it_e2e, rr_e2e = f.solve_pcg(b, 1e-10, 100)
         torch.cuda.synchronize()

@@ -155,6 +155,17 @@ T* upload(const std::vector<T>& v, cudaStream_t s) {
   return d;
 }
 
+// A caller's host array copied straight to a new stream-ordered device buffer
+// (freed with dfree): no intermediate host copy. The runtime stages a pageable
+// source itself, so the array may be reused once the copy call has returned.
+template <class T>
+T* upload_host(const T* src, long long count, cudaStream_t s) {
+  T* d = dalloc<T>((size_t)count, s);
+  if (count > 0)
+    HIF_CK(cudaMemcpyAsync(d, src, (size_t)count * sizeof(T), cudaMemcpyHostToDevice, s));
+  return d;
+}
+
 // Host worker pool for parallel_for, started on first use and kept for the
 // process (several host threads run parallel loops at once: a factorization's
 // partition threads, the serving loop's factor workers). A loop is a job on
@@ -3996,9 +4007,8 @@ int hif_setup_stencil(hif_handle h, int N, double hstep, const double* A, const 
   return guarded([&] {
     hif::Engine& e = *h->e;
     const long long nt = (long long)(N + 2) * (N + 2) * (N + 2);
-    std::vector<double> a(A, A + nt), v(V, V + nt);
-    double* dA = hif::upload(a, e.stream);
-    double* dV = hif::upload(v, e.stream);
+    double* dA = hif::upload_host(A, nt, e.stream);
+    double* dV = hif::upload_host(V, nt, e.stream);
     e.setup_node_device(dA, dV, hstep);
     hif::dfree(dA, e.stream);
     hif::dfree(dV, e.stream);
@@ -4012,11 +4022,10 @@ int hif_setup_stencil_faces(hif_handle h, int N, double hstep, const double* ax,
   return guarded([&] {
     hif::Engine& e = *h->e;
     const long long nt = (long long)(N + 2) * (N + 2) * (N + 2);
-    std::vector<double> hx(ax, ax + nt), hy(ay, ay + nt), hz(az, az + nt), hv(V, V + nt);
-    double* dx = hif::upload(hx, e.stream);
-    double* dy = hif::upload(hy, e.stream);
-    double* dz = hif::upload(hz, e.stream);
-    double* dv = hif::upload(hv, e.stream);
+    double* dx = hif::upload_host(ax, nt, e.stream);
+    double* dy = hif::upload_host(ay, nt, e.stream);
+    double* dz = hif::upload_host(az, nt, e.stream);
+    double* dv = hif::upload_host(V, nt, e.stream);
     hif::launch_setup_faces(dx, dy, dz, dv, N, hstep, e.d_band, e.stream);
     HIF_CK(cudaGetLastError());
     hif::dfree(dx, e.stream);
